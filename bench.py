@@ -1,0 +1,313 @@
+"""f2 block-tensor extraction benchmark (one JSON line on rank 0).
+
+Metric: f2 SNP-pop-pairs/s = M * P*(P-1)/2 per extraction pass, per second. A step is one
+pass of the hot path (ploidy -> decode -> per-block contraction -> FP64 f2/vpair) over
+one synthetic panel already resident in HBM. Workload (default): 1,000 populations x 10
+samples (10,000 total), 1,150,000 SNPs on 22 chromosomes, 5 cM blocks (~700), split-BF16
+tensor-core contraction. The panel (2.9 GB of genotypes, ~12 GB of operands) is far larger
+than L2, so no flush is needed between steps.
+
+`e2e` times the same extraction through the C ABI with host buffers: pinned genotypes in,
+H2D copy, extraction, D2H of the FP64 f2 and vpair tensors, every step.
+
+`--impl reference` times the reference's own CpuBackend (oracle/_ref, built from the
+reference sources; the C restatement when that is absent) on the host cores, one
+jackknife block per thread, on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): blocks are independent, so every rank extracts its own panel (a
+different genome segment of the same shape): weak scaling, no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+METRIC = "f2 SNP·pop-pairs/s: split-BF16 TC vs plain FP32 on 1 B200, rel err ≤1e-6 vs FP64"
+UNIT = "SNP·pop-pairs/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling (every 200 ms) during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        try:
+            rows = [ln.split(",") for ln in Path(self.f.name).read_text().splitlines() if ln.strip()]
+        except OSError:
+            rows = []
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+            except (ValueError, IndexError):
+                continue
+            for name, val in zip(names, r[4:8]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def units(P: int, M: int) -> float:
+    return float(M) * P * (P - 1) / 2.0
+
+
+def make_panel(workload: str, rank: int, device: str, n_snp: int | None = None):
+    from steppecu_b200 import synth
+
+    return synth.generate(workload, seed=20261203 + 1000 * rank, device=device, n_snp=n_snp)
+
+
+def cpu_sample(workload: str, threads: int, seed_rank: int = 0):
+    """Bounded CPU sample: `threads` blocks of the workload's panel model (one per thread),
+    decoded and reduced by the CPU implementation. Returns (units, seconds, kind, desc)."""
+    import numpy as np
+
+    import oracle
+    from steppecu_b200 import synth
+
+    wl = synth.WORKLOADS[workload]
+    per_block = max(1, wl.n_snp // 700)
+    n_snp = per_block * threads
+    p = synth.generate(workload, seed=20261203 + 17 + seed_rank, device="cpu", n_snp=n_snp)
+    sel, po = p.selection()
+    rec = p.records_numpy()
+    bid = np.minimum(np.arange(n_snp) // per_block, threads - 1).astype(np.int32)
+    kind = "reference" if oracle.ref_available() else "port"
+    lib = "ref" if kind == "reference" else "port"
+    t0 = time.perf_counter()
+    pl = oracle.detect_ploidy_pa(rec, sel)
+    ac2, n = oracle.decode_counts_pa(rec, sel, po, pl)
+    q, v, nd = oracle.counts_to_qvn(ac2, n)
+    oracle.compute_f2_blocks_sharded(q, v, nd, p.n_pop, bid, threads, threads=threads, lib=lib)
+    dt = time.perf_counter() - t0
+    desc = (f"{threads} blocks x {per_block} SNPs of the {workload} panel model (P={p.n_pop}, "
+            f"N={p.n_ind}), decode + f2 on {threads} threads, one block per thread")
+    return units(p.n_pop, n_snp), dt, kind, desc
+
+
+def run_reference(args, rank: int, world: int):
+    threads = os.cpu_count() or 1
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_sample(args.workload, threads)
+    tot_u, tot_t = 0.0, 0.0
+    kind, desc = "port", ""
+    for _ in range(args.steps):
+        u, t, kind, desc = cpu_sample(args.workload, threads)
+        tot_u += u
+        tot_t += t
+    val = tot_u / tot_t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * tot_t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "sample": desc},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--precision", default="split_bf16")
+    ap.add_argument("--compare-simt", action="store_true", default=True)
+    ap.add_argument("--no-compare-simt", dest="compare_simt", action="store_false")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--cpu-threads", type=int, default=None)
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    args.warmup = max(3, args.warmup)
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+
+    import steppecu_b200 as sb
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    dev = f"cuda:{local}"
+    panel = make_panel(args.workload, rank, dev)
+    sel, po = panel.selection()
+    P, M, B = panel.n_pop, panel.n_snp, panel.n_block
+    ctx = sb.Context(local)
+    rec = panel.records  # device-resident [M, bpr] uint8
+    n_out = P * P * B
+    f2 = torch.empty(n_out, dtype=torch.float64, device=dev)
+    vp = torch.empty_like(f2)
+    stream = torch.cuda.current_stream()
+    plan = ctx.plan(rec, panel.n_ind, sel, po, panel.block_id, B, precision=args.precision)
+
+    def timed(pl, steps, warm):
+        for _ in range(warm):
+            pl.run(rec, f2, vp, stream.cuda_stream)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        pl.set_timing(True)
+        l0 = ctx.launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            pl.run(rec, f2, vp, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = ctx.launches - l0
+        ms = e0.elapsed_time(e1) / steps
+        dec, con = pl.last_times()
+        pl.set_timing(False)
+        barrier()
+        return ms, dec, con, launches
+
+    with Clocks(local) as clk:
+        ms, dec_ms, con_ms, launches = timed(plan, args.steps, args.warmup)
+    clocks = clk.summary()
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = units(P, M) * world / (ms / 1000.0)
+
+    # Plain FP32 SIMT form on the same panel (the comparison arithmetic).
+    simt = None
+    if args.compare_simt and args.precision != "fp32":
+        plan_s = ctx.plan(rec, panel.n_ind, sel, po, panel.block_id, B, precision="fp32")
+        s_steps = max(1, min(args.steps, 3))
+        ms_s, dec_s, con_s, _ = timed(plan_s, s_steps, 1)
+        simt = {"value": units(P, M) / (ms_s / 1000.0), "ms_per_step": ms_s, "contract_ms": con_s,
+                "decode_ms": dec_s}
+        plan_s.close()
+
+    # End to end through the C ABI with pinned host buffers.
+    rec_h = torch.empty(rec.shape, dtype=torch.uint8, pin_memory=True)
+    rec_h.copy_(rec)
+    f2_h = torch.empty(n_out, dtype=torch.float64, pin_memory=True)
+    vp_h = torch.empty(n_out, dtype=torch.float64, pin_memory=True)
+    rec_np, f2_np, vp_np = rec_h.numpy(), f2_h.numpy(), vp_h.numpy()
+    e2e_steps = args.e2e_steps or max(1, min(args.steps, 5))
+    ctx.extract_blocks(rec_np, panel.n_ind, sel, po, panel.block_id, B, precision=args.precision,
+                       out=(f2_np, vp_np))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.extract_blocks(rec_np, panel.n_ind, sel, po, panel.block_id, B, precision=args.precision,
+                           out=(f2_np, vp_np))
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": units(P, M) * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(rec.numel()),
+           "d2h_bytes_per_step": int(2 * n_out * 8), "ms_per_step": 1000.0 * e2e_s, "steps": e2e_steps}
+
+    # Roofline of the dominant kernel (the contraction): algorithmic flops per launch =
+    # 3 contractions x 2 * P^2 * M (SNP-padded work excluded) over the measured launch time.
+    peaks, peak_kind = load_peaks()
+    flops = 6.0 * P * P * M
+    achieved = flops / (con_ms / 1000.0) / 1e12
+    peak = float(peaks.get("bf16_tflops", PEAKS_FALLBACK["bf16_tflops"]))
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                "kernel_ms": con_ms, "decode_ms": dec_ms,
+                "decode_hbm_gbs": (M * panel.bytes_per_record + 11 * P * M) / (dec_ms / 1000.0) / 1e9}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = args.cpu_threads or (os.cpu_count() or 1)
+        u, t, kind, desc = cpu_sample(args.workload, threads)
+        cpu = {"value": u / t, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"split_bf16": "bf16x3", "split_f16": "f16x3"}.get(args.precision, "f32"),
+            "data": "synthetic",
+            "config": {"workload": args.workload, "populations": P, "samples": panel.n_ind, "snps": M,
+                       "blocks": B, "precision": args.precision, "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"block-sharded x{world}" if world > 1 else "1 GPU"},
+            "gpu_launches": int(launches), "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+            "plain_fp32_simt": simt,
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

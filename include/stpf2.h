@@ -1,0 +1,174 @@
+/* include/stpf2.h — C ABI of libstpf2.so, the B200 (sm_100a) f2 block-tensor extraction.
+ *
+ * One streaming pass turns 2-bit PACKEDANCESTRYMAP genotypes into the reference's
+ * F2BlockTensor: per-jackknife-block f2 means and both-present SNP counts, FP64,
+ * element (i, j, b) at i + P*j + P*P*b (include/steppe/fstats.hpp:19-59 in the
+ * reference). Plain pointers and sizes only; no C++ or torch types cross this line.
+ *
+ * Each entry point names the reference interface it replaces. Errors come back as an
+ * stp_status; stp_last_error() gives the message of the calling thread's last failure.
+ * Degenerate extents (P <= 0, M <= 0, n_block <= 0) give empty/zero results, not errors,
+ * as in the reference (src/device/cpu/cpu_backend.cpp:234).
+ */
+#ifndef STPF2_H
+#define STPF2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STPF2_ABI_VERSION 1
+
+/* Status codes. 0..5 keep the numbering of steppe::Status (include/steppe/error.hpp:14-26);
+ * the rest stand for the reference's exception types (std::invalid_argument /
+ * std::runtime_error / CudaError in src/device/cuda/check.cuh:34-60). */
+typedef enum stp_status {
+    STP_OK = 0,
+    STP_DEVICE_OOM = 1,
+    STP_INVALID_CONFIG = 5,
+    STP_INVALID_ARGUMENT = 100, /* std::invalid_argument: bad sizes, null pointers */
+    STP_RUNTIME_ERROR = 101,    /* std::runtime_error: malformed partition, M > INT_MAX */
+    STP_CUDA_ERROR = 102,       /* CudaError: a CUDA runtime/driver call failed */
+    STP_NO_DEVICE = 103,        /* no CUDA device (the reference's "GPU product" error) */
+    STP_DEVICE_TIMEOUT = 104    /* a bounded device-side wait ran out; results invalid */
+} stp_status;
+
+/* Contraction arithmetic. The reference's Precision (include/steppe/config.hpp:74-95)
+ * selects FP64 / emulated FP64 cuBLAS; this build's modes are: */
+typedef enum stp_precision {
+    STP_PREC_FP32_SIMT = 0,  /* plain FP32 CUDA-core contraction, FP64 combine */
+    STP_PREC_SPLIT_BF16 = 1, /* tcgen05 split-BF16 (hi+lo, 3 products), FP32 TMEM, FP64 drain */
+    STP_PREC_SPLIT_F16 = 2   /* tcgen05 split-FP16 (scaled hi+lo, 3 products), same pipeline */
+} stp_precision;
+
+/* steppe::ExtractPloidy (include/steppe/extract.hpp) */
+typedef enum stp_ploidy_mode {
+    STP_PLOIDY_AUTO = 0,   /* per-sample detection over the first min(1000, M) SNPs */
+    STP_PLOIDY_PSEUDO = 1, /* every sample pseudo-haploid */
+    STP_PLOIDY_DIPLOID = 2 /* every sample diploid */
+} stp_ploidy_mode;
+
+typedef struct stp_ctx stp_ctx;
+typedef struct stp_plan stp_plan;
+
+/* SNP-major PACKEDANCESTRYMAP records (the .geno payload after its header record):
+ * record s holds individual r's code at byte r/4, MSB-first (src/io/eigenstrat_format.cpp
+ * :17-85, src/io/geno_reader.cpp:465-514). */
+typedef struct stp_geno_view {
+    const uint8_t* records;    /* n_snp records, `pitch` bytes apart */
+    uint64_t bytes_per_record; /* max(48, ceil(n_ind/4)) */
+    uint64_t pitch;            /* distance between records in bytes (>= bytes_per_record) */
+    int64_t n_snp;
+    int64_t n_ind;             /* individuals in the file (.ind rows) */
+    int32_t on_device;         /* records is a device pointer (DecodeTileView::packed_on_device) */
+} stp_geno_view;
+
+/* One extraction request (the inputs of steppe::run_extract_f2 after the front end:
+ * src/app/extract_f2_core.cpp:93-407). Host pointers unless stated. */
+typedef struct stp_f2_request {
+    stp_geno_view geno;
+    const int64_t* sel_rows;      /* [n_sel] file rows of the selected samples, pop-contiguous */
+    const int64_t* pop_offsets;   /* [n_pop+1] into sel_rows (io::GenoReader::build_selection) */
+    int32_t n_pop;
+    const int32_t* sample_ploidy; /* [n_sel] 1/2, or NULL to use ploidy_mode */
+    int32_t ploidy_mode;          /* stp_ploidy_mode, used when sample_ploidy is NULL */
+    const int32_t* block_id;      /* [n_snp] non-decreasing in [0, n_block) (core::assign_blocks) */
+    int32_t n_block;
+    int32_t precision;            /* stp_precision */
+} stp_f2_request;
+
+/* Caller-owned result buffers in F2BlockTensor layout. */
+typedef struct stp_f2_output {
+    double* f2;            /* [P*P*n_block] per-block f2 means */
+    double* vpair;         /* [P*P*n_block] both-present SNP counts */
+    int32_t* block_sizes;  /* [n_block] host */
+    int32_t on_device;     /* f2 / vpair are device pointers */
+    int32_t* ploidy_out;   /* optional [n_sel] host: the ploidy used per selected sample */
+} stp_f2_output;
+
+/* ---- context ------------------------------------------------------------------------ */
+
+/* make_cuda_backend(device) (src/device/backend_factory.hpp:18-21). */
+stp_ctx* stp_create(int device, stp_status* status);
+void stp_destroy(stp_ctx* ctx);
+/* Message of the calling thread's last failed call ("" if none). */
+const char* stp_last_error(void);
+int stp_abi_version(void);
+/* Kernel launches issued by this context since creation (every kernel of this library). */
+uint64_t stp_launch_count(const stp_ctx* ctx);
+
+/* ---- decode ------------------------------------------------------------------------- */
+
+/* ComputeBackend::detect_sample_ploidy_device (src/device/backend.hpp:765) on SNP-major
+ * records: ploidy[g] = 2 if selected sample g has a het within the first min(1000, n_snp)
+ * SNPs, else 1. */
+stp_status stp_detect_ploidy(stp_ctx* ctx, const stp_geno_view* geno, const int64_t* sel_rows,
+                             int64_t n_sel, int32_t* ploidy);
+
+/* Integer decode (decode_af.hpp:58-65): ac2 = 2*ac and n per (pop, SNP), column-major
+ * [P x n_snp] host arrays. The bit-exact form of ComputeBackend::decode_af. */
+stp_status stp_decode_counts(stp_ctx* ctx, const stp_geno_view* geno, const int64_t* sel_rows,
+                             const int64_t* pop_offsets, int32_t n_pop,
+                             const int32_t* sample_ploidy, int32_t ploidy_mode,
+                             int32_t* ac2, int32_t* n);
+
+/* ComputeBackend::decode_af(DecodeTileView) (src/device/backend.hpp:736) on the canonical
+ * individual-major tile: record g (bytes_per_record >= ceil(n_snp/4)) holds selected
+ * sample g's SNP codes MSB-first; pop_offsets[P+1] index records. sample_ploidy NULL with
+ * detect != 0 detects ploidy; NULL with detect == 0 uses `ploidy`. Out: q, v, n host
+ * [P x n_snp] column-major FP64. */
+stp_status stp_decode_af(stp_ctx* ctx, const uint8_t* packed, uint64_t bytes_per_record,
+                         int64_t n_snp, int64_t n_ind, const int64_t* pop_offsets, int32_t n_pop,
+                         const int32_t* sample_ploidy, int32_t ploidy, int32_t detect,
+                         int32_t packed_on_device, double* q, double* v, double* n);
+
+/* ---- f2 ------------------------------------------------------------------------------ */
+
+/* ComputeBackend::compute_f2_blocks(MatView Q, V, N, block_id, n_block, Precision)
+ * (src/device/backend.hpp:687-692). Q/V/N host [P x M] column-major. */
+stp_status stp_f2_from_qvn(stp_ctx* ctx, const double* Q, const double* V, const double* N,
+                           int32_t P, int64_t M, const int32_t* block_id, int32_t n_block,
+                           int32_t precision, double* f2, double* vpair, int32_t* block_sizes);
+
+/* The extract-f2 hot path: packed genotypes -> ploidy -> decode -> per-block contraction
+ * -> FP64 F2BlockTensor (src/app/extract_f2_core.cpp:93-407, Resident tier). */
+stp_status stp_f2_extract_blocks(stp_ctx* ctx, const stp_f2_request* req, stp_f2_output* out);
+
+/* Many independent requests (each its own populations and block map) over shared or
+ * separate genotype matrices, batched into one grouped decode and one grouped contraction. */
+stp_status stp_f2_extract_batch(stp_ctx* ctx, const stp_f2_request* reqs, int32_t n_req,
+                                stp_f2_output* outs);
+
+/* Block jackknife over per-block values (cpu_backend.cpp:2674-2720, :2273-2306), FP64 on
+ * the device: x[k + m*b] with m = P*P -> est[m], var[m]. Host pointers. */
+stp_status stp_f2_jackknife(stp_ctx* ctx, const double* x, const int32_t* block_sizes, int64_t m,
+                            int32_t n_block, double* est, double* var);
+
+/* ---- plans: device-resident repeated extraction --------------------------------------- */
+
+/* Builds everything a request needs once (operand buffers, block layout, work list,
+ * tensor maps, ploidy) so stp_plan_run only launches kernels. The request's genotype
+ * records must be on the device; the plan keeps no reference to host arrays. */
+stp_plan* stp_plan_create(stp_ctx* ctx, const stp_f2_request* req, stp_status* status);
+/* Enqueues decode + contraction on `stream` (a cudaStream_t, NULL = the context stream);
+ * d_f2/d_vpair are device buffers of P*P*n_block doubles. Asynchronous. */
+stp_status stp_plan_run(stp_plan* plan, const uint8_t* d_records, double* d_f2, double* d_vpair,
+                        void* stream);
+/* Kernel launches one stp_plan_run issues. */
+int32_t stp_plan_launches(const stp_plan* plan);
+/* Timing: with timing enabled, every stp_plan_run records CUDA events on its stream around
+ * the decode (ploidy + decode kernels) and the contraction kernel. stp_plan_last_times
+ * returns the mean device time of each, in ms, over all runs since timing was (re-)enabled
+ * (0 if none). Enabling resets the set of timed runs. */
+stp_status stp_plan_set_timing(stp_plan* plan, int32_t enable);
+stp_status stp_plan_last_times(const stp_plan* plan, float* decode_ms, float* contract_ms);
+void stp_plan_destroy(stp_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STPF2_H */

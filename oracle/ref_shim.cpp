@@ -1,0 +1,146 @@
+// oracle/ref_shim.cpp
+//
+// TEST INFRASTRUCTURE ONLY. A C-ABI shim over the reference's own CpuBackend
+// (src/device/cpu/cpu_backend.cpp), compiled in place from the reference sources by
+// oracle/Makefile into oracle/_ref/libref_oracle.so. Tests use it to pin the C
+// restatement in f2_oracle.c, and bench.py's reference arm times it as the
+// reference's CPU implementation. It is never linked into the product.
+//
+// Each entry point forwards to the reference interface named beside it and copies the
+// result into caller-owned buffers with the reference's own layouts.
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <span>
+#include <vector>
+
+#include "core/domain/block_partition_rule.hpp"
+#include "device/backend.hpp"
+#include "device/backend_factory.hpp"
+
+namespace {
+
+std::unique_ptr<steppe::ComputeBackend>& backend() {
+    thread_local std::unique_ptr<steppe::ComputeBackend> be = steppe::device::make_cpu_backend();
+    return be;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ComputeBackend::compute_f2_blocks (src/device/backend.hpp:687-692).
+int ref_compute_f2_blocks(const double* Q, const double* V, const double* N, int P, long M,
+                          const int* block_id, int n_block, double* f2, double* vpair,
+                          int* block_sizes) {
+    try {
+        const steppe::core::MatView q{Q, P, M}, v{V, P, M}, n{N, P, M};
+        const steppe::F2BlockTensor t =
+            backend()->compute_f2_blocks(q, v, n, block_id, n_block, steppe::Precision::fp64());
+        std::memcpy(f2, t.f2.data(), t.f2.size() * sizeof(double));
+        std::memcpy(vpair, t.vpair.data(), t.vpair.size() * sizeof(double));
+        for (std::size_t b = 0; b < t.block_sizes.size(); ++b) block_sizes[b] = t.block_sizes[b];
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// ComputeBackend::decode_af (src/device/backend.hpp:736) on the canonical tile.
+int ref_decode_af(const std::uint8_t* packed, std::size_t bytes_per_record, std::size_t n_snp,
+                  std::size_t n_ind, const std::size_t* pop_offsets, int P,
+                  const int* sample_ploidy, int ploidy, int detect, double* q, double* v,
+                  double* n) {
+    try {
+        steppe::DecodeTileView view;
+        view.packed = packed;
+        view.bytes_per_record = bytes_per_record;
+        view.n_snp = n_snp;
+        view.n_individuals = n_ind;
+        view.pop_offsets = pop_offsets;
+        view.n_pop = P;
+        view.sample_ploidy = sample_ploidy;
+        view.ploidy = ploidy;
+        view.detect_ploidy_on_device = detect != 0;
+        const steppe::DecodeResult r = backend()->decode_af(view);
+        std::memcpy(q, r.q.data(), r.q.size() * sizeof(double));
+        std::memcpy(v, r.v.data(), r.v.size() * sizeof(double));
+        std::memcpy(n, r.n.data(), r.n.size() * sizeof(double));
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// ComputeBackend::detect_sample_ploidy_device (src/device/backend.hpp:765), host default.
+int ref_detect_ploidy(const std::uint8_t* packed, std::size_t bytes_per_record,
+                      std::size_t n_snp, std::size_t n_ind, int* ploidy) {
+    try {
+        steppe::DecodeTileView view;
+        view.packed = packed;
+        view.bytes_per_record = bytes_per_record;
+        view.n_snp = n_snp;
+        view.n_individuals = n_ind;
+        const std::vector<int> r = backend()->detect_sample_ploidy_device(view);
+        for (std::size_t g = 0; g < r.size(); ++g) ploidy[g] = r[g];
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// core::assign_blocks (src/core/domain/block_partition_rule.cpp:57-85).
+int ref_assign_blocks(const int* chrom, const double* genpos, long M, double blgsize,
+                      const double* physpos, double bp_window, int* block_id) {
+    const std::span<const int> c(chrom, static_cast<std::size_t>(M));
+    const std::span<const double> g(genpos, static_cast<std::size_t>(M));
+    const std::span<const double> p =
+        physpos ? std::span<const double>(physpos, static_cast<std::size_t>(M))
+                : std::span<const double>{};
+    const steppe::core::BlockPartition bp = steppe::core::assign_blocks(c, g, blgsize, p, bp_window);
+    for (std::size_t s = 0; s < bp.block_id.size(); ++s) block_id[s] = bp.block_id[s];
+    return bp.n_block;
+}
+
+// The reference's block jackknife (cpu_backend.cpp:2674-2720 and :2273-2306) reached
+// through its public surface: per-item block values x[k + m*b] are placed as f2(0, k+1, b)
+// of a zero-diagonal tensor, assemble_f3_triples((0, k+1, k+1)) returns exactly those
+// values with their leave-one-out totals, and jackknife_diag gives the variance.
+int ref_block_jackknife(const double* x, const int* block_sizes, long m, int nb, double* est,
+                        double* var) {
+    try {
+        const int P = static_cast<int>(m) + 1;
+        steppe::F2BlockTensor t;
+        t.P = P;
+        t.n_block = nb;
+        t.block_sizes.assign(block_sizes, block_sizes + nb);
+        const std::size_t slab = static_cast<std::size_t>(P) * static_cast<std::size_t>(P);
+        t.f2.assign(slab * static_cast<std::size_t>(nb), 0.0);
+        t.vpair.assign(slab * static_cast<std::size_t>(nb), 1.0);
+        std::vector<int> triples;
+        for (long k = 0; k < m; ++k) {
+            for (int b = 0; b < nb; ++b) {
+                const double val = x[static_cast<std::size_t>(k) + static_cast<std::size_t>(m) * b];
+                const std::size_t a = static_cast<std::size_t>(k + 1);
+                t.f2[0 + P * a + slab * b] = val;
+                t.f2[a + 0 + slab * b] = val;
+            }
+            triples.push_back(0);
+            triples.push_back(static_cast<int>(k + 1));
+            triples.push_back(static_cast<int>(k + 1));
+        }
+        auto& be = backend();
+        const steppe::F4Blocks f = be->assemble_f3_triples(t, triples, steppe::Precision::fp64());
+        const steppe::JackknifeDiag d = be->jackknife_diag(f, f.block_sizes, steppe::Precision::fp64());
+        for (long k = 0; k < m; ++k) {
+            est[k] = f.x_total[static_cast<std::size_t>(k)];
+            var[k] = d.var[static_cast<std::size_t>(k)];
+        }
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,359 @@
+"""Python surface of the B200 f2 extraction, mirroring the reference's bindings.
+
+``extract_f2`` / ``read_f2`` / ``F2Blocks`` follow ``steppe.extract_f2``, ``steppe.read_f2``
+and the ``F2Handle`` opaque type (bindings/steppe/__init__.py:493-560,
+bindings/bind_f2handle.cpp:26-47, bindings/bind_fstats.cpp:130-224 in the reference).
+``Context`` exposes the C-ABI entry points that stand in for the ComputeBackend
+f2/decode virtuals. Every computation runs in libstpf2.so on the GPU; without a CUDA
+device the calls raise, as the reference does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib as L
+from .blocks import assign_blocks
+from .eigenstrat import read_geno, read_ind, read_snp, select_pops
+from .f2dir import F2Tensor, read_f2_dir, write_f2_dir
+
+PRECISIONS = {
+    "fp32": L.PREC_FP32_SIMT, "fp32_simt": L.PREC_FP32_SIMT, "simt": L.PREC_FP32_SIMT,
+    "bf16x3": L.PREC_SPLIT_BF16, "split_bf16": L.PREC_SPLIT_BF16, "bf16": L.PREC_SPLIT_BF16,
+    "f16x3": L.PREC_SPLIT_F16, "split_f16": L.PREC_SPLIT_F16, "fp16": L.PREC_SPLIT_F16,
+}
+PRECISION_TAGS = {L.PREC_FP32_SIMT: "fp32_simt", L.PREC_SPLIT_BF16: "split_bf16", L.PREC_SPLIT_F16: "split_f16"}
+DEFAULT_PRECISION = "split_bf16"
+
+PLOIDY = {"auto": L.PLOIDY_AUTO, "1": L.PLOIDY_PSEUDO, "pseudo": L.PLOIDY_PSEUDO,
+          "pseudo_haploid": L.PLOIDY_PSEUDO, "2": L.PLOIDY_DIPLOID, "diploid": L.PLOIDY_DIPLOID}
+
+
+def parse_precision(precision) -> int:
+    if precision is None:
+        precision = DEFAULT_PRECISION
+    if isinstance(precision, int):
+        return precision
+    try:
+        return PRECISIONS[str(precision)]
+    except KeyError:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)} (got {precision!r})") from None
+
+
+def _i64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _is_torch_cuda(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(x.is_cuda)
+
+
+def _data_ptr(x) -> int:
+    return int(x.data_ptr()) if hasattr(x, "data_ptr") else int(x.ctypes.data)
+
+
+class Context:
+    """One libstpf2 context (make_cuda_backend(device)): a device and a CUDA stream."""
+
+    def __init__(self, device: int = 0):
+        st = C.c_int(0)
+        self._h = L.lib().stp_create(device, C.byref(st))
+        if not self._h:
+            raise L.StpError(st.value, L.lib().stp_last_error().decode())
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().stp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def launches(self) -> int:
+        return int(L.lib().stp_launch_count(self._h))
+
+    # -- genotype views ---------------------------------------------------------------
+    @staticmethod
+    def geno_view(records, n_ind: int, bytes_per_record: int | None = None) -> L.GenoView:
+        """records: numpy uint8 [n_snp, pitch] (host) or a torch CUDA uint8 tensor."""
+        n_snp = int(records.shape[0])
+        pitch = int(records.shape[1]) if records.ndim == 2 else 0
+        bpr = bytes_per_record or max(48, (n_ind + 3) // 4)
+        if not _is_torch_cuda(records):
+            records = np.ascontiguousarray(records)
+        v = L.GenoView(_data_ptr(records), bpr, pitch, n_snp, n_ind, 1 if _is_torch_cuda(records) else 0)
+        v._keep = records
+        return v
+
+    # -- decode ---------------------------------------------------------------------------
+    def detect_ploidy(self, records, n_ind: int, sel_rows) -> np.ndarray:
+        v = self.geno_view(records, n_ind)
+        sel = _i64(sel_rows)
+        out = np.zeros(sel.size, np.int32)
+        L.check(L.lib().stp_detect_ploidy(self._h, C.byref(v), L.ptr(sel), sel.size, L.ptr(out)))
+        return out
+
+    def decode_counts(self, records, n_ind: int, sel_rows, pop_offsets, sample_ploidy=None,
+                      ploidy: str | int = "auto") -> tuple[np.ndarray, np.ndarray]:
+        """(ac2, n) int32 [P, M] C-order views of the column-major [P x M] counts."""
+        v = self.geno_view(records, n_ind)
+        sel, po = _i64(sel_rows), _i64(pop_offsets)
+        P = po.size - 1
+        M = v.n_snp
+        ac2 = np.zeros(P * M, np.int32)
+        n = np.zeros(P * M, np.int32)
+        sp = None if sample_ploidy is None else _i32(sample_ploidy)
+        mode = PLOIDY[str(ploidy)] if not isinstance(ploidy, int) else ploidy
+        L.check(L.lib().stp_decode_counts(self._h, C.byref(v), L.ptr(sel), L.ptr(po), P, L.ptr(sp), mode,
+                                          L.ptr(ac2), L.ptr(n)))
+        return ac2.reshape(M, P).T, n.reshape(M, P).T
+
+    def decode_af(self, packed, bytes_per_record: int, n_snp: int, pop_offsets, sample_ploidy=None,
+                  ploidy: int = 2, detect: bool = False):
+        """ComputeBackend::decode_af on the canonical individual-major tile. Returns flat
+        column-major [P x M] q, v, n (FP64), index i + P*s."""
+        po = _i64(pop_offsets)
+        P = po.size - 1
+        pk = np.ascontiguousarray(packed, dtype=np.uint8)
+        n_ind = pk.size // bytes_per_record if bytes_per_record else 0
+        q = np.zeros(P * n_snp)
+        v = np.zeros(P * n_snp)
+        n = np.zeros(P * n_snp)
+        sp = None if sample_ploidy is None else _i32(sample_ploidy)
+        L.check(L.lib().stp_decode_af(self._h, L.ptr(pk), bytes_per_record, n_snp, n_ind, L.ptr(po), P,
+                                      L.ptr(sp), ploidy, 1 if detect else 0, 0, L.ptr(q), L.ptr(v), L.ptr(n)))
+        return q, v, n
+
+    # -- f2 ---------------------------------------------------------------------------------
+    def f2_from_qvn(self, Q, V, N, P: int, block_id, n_block: int, precision=None) -> F2Tensor:
+        """ComputeBackend::compute_f2_blocks(MatView Q, V, N, ...): flat [P x M] inputs."""
+        Q, V, N = (np.ascontiguousarray(x, dtype=np.float64) for x in (Q, V, N))
+        M = Q.size // P if P > 0 else 0
+        bid = _i32(block_id)
+        n = P * P * n_block
+        f2 = np.zeros(n)
+        vp = np.zeros(n)
+        bs = np.zeros(max(n_block, 0), np.int32)
+        L.check(L.lib().stp_f2_from_qvn(self._h, L.ptr(Q), L.ptr(V), L.ptr(N), P, M, L.ptr(bid), n_block,
+                                        parse_precision(precision), L.ptr(f2), L.ptr(vp), L.ptr(bs)))
+        return F2Tensor(f2, vp, bs, P, n_block)
+
+    def _request(self, records, n_ind, sel_rows, pop_offsets, block_id, n_block, precision,
+                 sample_ploidy=None, ploidy="auto"):
+        v = self.geno_view(records, n_ind)
+        sel, po, bid = _i64(sel_rows), _i64(pop_offsets), _i32(block_id)
+        sp = None if sample_ploidy is None else _i32(sample_ploidy)
+        mode = PLOIDY[str(ploidy)] if not isinstance(ploidy, int) else ploidy
+        r = L.F2Request(v, L.ptr(sel), L.ptr(po), po.size - 1, L.ptr(sp), mode, L.ptr(bid), n_block,
+                        parse_precision(precision))
+        r._keep = (v, sel, po, bid, sp)
+        return r
+
+    def extract_blocks(self, records, n_ind: int, sel_rows, pop_offsets, block_id, n_block: int,
+                       precision=None, sample_ploidy=None, ploidy="auto", out=None,
+                       return_ploidy: bool = False):
+        """The extract-f2 hot path on one request. records: host numpy [M, bpr] or a torch
+        CUDA tensor. out: optional (f2, vpair) buffers (numpy host or torch CUDA)."""
+        r = self._request(records, n_ind, sel_rows, pop_offsets, block_id, n_block, precision,
+                          sample_ploidy, ploidy)
+        P = r.n_pop
+        n = P * P * n_block
+        if out is None:
+            f2, vp = np.zeros(n), np.zeros(n)
+        else:
+            f2, vp = out
+        on_dev = _is_torch_cuda(f2)
+        bs = np.zeros(max(n_block, 0), np.int32)
+        ploidy_out = np.zeros(int(r._keep[1].size), np.int32) if return_ploidy else None
+        o = L.F2Output(_data_ptr(f2), _data_ptr(vp), L.ptr(bs), 1 if on_dev else 0, L.ptr(ploidy_out))
+        L.check(L.lib().stp_f2_extract_blocks(self._h, C.byref(r), C.byref(o)))
+        t = F2Tensor(f2, vp, bs, P, n_block) if not on_dev else (f2, vp, bs)
+        return (t, ploidy_out) if return_ploidy else t
+
+    def jackknife(self, x, block_sizes, m: int, n_block: int) -> tuple[np.ndarray, np.ndarray]:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        bs = _i32(block_sizes)
+        est, var = np.zeros(m), np.zeros(m)
+        L.check(L.lib().stp_f2_jackknife(self._h, L.ptr(x), L.ptr(bs), m, n_block, L.ptr(est), L.ptr(var)))
+        return est, var
+
+    def plan(self, records, n_ind: int, sel_rows, pop_offsets, block_id, n_block: int, precision=None,
+             sample_ploidy=None, ploidy="auto") -> "Plan":
+        return Plan(self, self._request(records, n_ind, sel_rows, pop_offsets, block_id, n_block, precision,
+                                        sample_ploidy, ploidy))
+
+
+class Plan:
+    """Device-resident repeated extraction (stp_plan_*): inputs and outputs stay in HBM."""
+
+    def __init__(self, ctx: Context, req: L.F2Request):
+        st = C.c_int(0)
+        self._ctx = ctx
+        self._h = L.lib().stp_plan_create(ctx._h, C.byref(req), C.byref(st))
+        if not self._h:
+            raise L.StpError(st.value, L.lib().stp_last_error().decode())
+        self.P = req.n_pop
+        self.n_block = req.n_block
+
+    def run(self, records, f2, vpair, stream: int = 0) -> None:
+        L.check(L.lib().stp_plan_run(self._h, _data_ptr(records), _data_ptr(f2), _data_ptr(vpair),
+                                     stream or None))
+
+    @property
+    def launches(self) -> int:
+        return int(L.lib().stp_plan_launches(self._h))
+
+    def set_timing(self, on: bool = True) -> None:
+        L.check(L.lib().stp_plan_set_timing(self._h, 1 if on else 0))
+
+    def last_times(self) -> tuple[float, float]:
+        a, b = C.c_float(0), C.c_float(0)
+        L.check(L.lib().stp_plan_last_times(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().stp_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- the reference's Python surface ---------------------------------------------------------
+
+class F2Blocks:
+    """Opaque f2 handle (F2Handle): the host f2 tensor plus population labels."""
+
+    def __init__(self, tensor: F2Tensor, pops: list[str], device: int = 0):
+        self._t = tensor
+        self._pops = list(pops)
+        self._device = device
+
+    @property
+    def pops(self) -> list[str]:
+        return list(self._pops)
+
+    @property
+    def P(self) -> int:
+        return self._t.P
+
+    @property
+    def n_block(self) -> int:
+        return self._t.n_block
+
+    @property
+    def block_sizes(self) -> list[int]:
+        return [int(x) for x in self._t.block_sizes]
+
+    @property
+    def device(self) -> int:
+        return self._device
+
+    @property
+    def tensor(self) -> F2Tensor:
+        return self._t
+
+    def to_numpy(self) -> np.ndarray:
+        """f2 as float64, F-contiguous (P, P, n_block). A copy."""
+        return np.array(self._t.cube("f2"), order="F", copy=True)
+
+    def vpair_to_numpy(self) -> np.ndarray:
+        return np.array(self._t.cube("vpair"), order="F", copy=True)
+
+    def __repr__(self) -> str:
+        return f"F2Blocks(P={self.P}, n_block={self.n_block}, device={self.device})"
+
+
+def read_f2(directory, *, device: int = 0) -> F2Blocks:
+    """Loads an f2 directory (f2.bin STPF2BK1 + pops.txt) into an F2Blocks handle."""
+    t, pops = read_f2_dir(directory)
+    return F2Blocks(t, pops, device)
+
+
+_CTX: dict[int, Context] = {}
+
+
+def context(device: int = 0) -> Context:
+    if device not in _CTX:
+        _CTX[device] = Context(device)
+    return _CTX[device]
+
+
+def extract_f2(prefix, *, pops: list[str], out: str | None = None, device: int = 0, blgsize: float = 0.05,
+               maf: float = 0.0, maxmiss: float = 0.0, autosomes_only: bool = True,
+               drop_monomorphic: bool = False, transversions_only: bool = False, ploidy: str = "auto",
+               strand_mode: str = "drop", precision: str | None = None):
+    """Builds an f2_blocks tensor from <prefix>.{geno,snp,ind} on the GPU.
+
+    The P axis is the selection sorted ascending by label (pops.txt order). Returns an
+    F2Blocks handle, or writes an STPF2BK1 directory to ``out`` and returns its path.
+    SNP filters (maxmiss, maf, monomorphic, autosomes, transversions, strand) are
+    applied before the block walk, from the GPU's exact per-population counts.
+    """
+    if not pops:
+        raise ValueError("extract_f2: pops needs at least one population name")
+    if ploidy not in PLOIDY:
+        raise ValueError("extract_f2: ploidy must be one of 'auto', '1'/'pseudo', '2'/'diploid'")
+    if strand_mode not in ("drop", "keep", "flip"):
+        raise ValueError("extract_f2: strand_mode must be one of 'drop', 'keep', 'flip'")
+    prec = parse_precision(precision)
+    prefix = str(prefix)
+    h, rec = read_geno(prefix + ".geno")
+    snp = read_snp(prefix + ".snp")
+    ind = read_ind(prefix + ".ind")
+    if len(ind) < h.n_ind:
+        raise ValueError(f"extract_f2: .ind has {len(ind)} rows but .geno has {h.n_ind} individuals")
+    if snp.chrom.size < h.n_snp:
+        raise ValueError(f"extract_f2: .snp has {snp.chrom.size} rows but the tile spans {h.n_snp} SNPs")
+    labels, sel, po = select_pops(ind, pops)
+    ctx = context(device)
+    from .filters import snp_keep_mask
+    keep = snp_keep_mask(ctx, rec, h, snp, sel, po, ploidy=ploidy, maf=maf, maxmiss=maxmiss,
+                         autosomes_only=autosomes_only, drop_monomorphic=drop_monomorphic,
+                         transversions_only=transversions_only, strand_mode=strand_mode)
+    idx = np.flatnonzero(keep)
+    if idx.size == 0:
+        raise ValueError(f"extract_f2: every SNP was filtered out (0 of {h.n_snp} kept) — relax the filters")
+    # Ploidy is detected on the unfiltered tile's first min(1000, M) SNPs (extract_f2_core.cpp:145-166).
+    sample_ploidy = None
+    if ploidy == "auto":
+        sample_ploidy = ctx.detect_ploidy(rec, h.n_ind, sel)
+    kept = rec if idx.size == h.n_snp else np.ascontiguousarray(rec[idx])
+    bid, nb = assign_blocks(snp.chrom[idx], snp.genpos[idx], blgsize, snp.physpos[idx])
+    if nb <= 0:
+        raise ValueError("extract_f2: assign_blocks produced 0 blocks (check blgsize and the .snp genetic positions)")
+    t = ctx.extract_blocks(kept, h.n_ind, sel, po, bid, nb, precision=prec, sample_ploidy=sample_ploidy,
+                           ploidy=ploidy)
+    if out is None:
+        return F2Blocks(t, labels, device)
+    meta = {
+        "precision_tag": PRECISION_TAGS.get(prec, ""), "blgsize_cm": blgsize * 100.0,
+        "n_snp_total": h.n_snp, "n_snp_kept": int(idx.size),
+        "filters": {"maf_min": maf, "maxmiss": maxmiss, "autosomes_only": autosomes_only,
+                    "drop_monomorphic": drop_monomorphic, "transversions_only": transversions_only},
+        "pop_selection": "explicit:" + ",".join(pops),
+        "geno": prefix + ".geno", "snp": prefix + ".snp", "ind": prefix + ".ind",
+    }
+    write_f2_dir(out, t, labels, meta)
+    return str(out)

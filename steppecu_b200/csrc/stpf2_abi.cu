@@ -1,0 +1,686 @@
+// steppecu_b200/csrc/stpf2_abi.cu
+//
+// The C ABI of libstpf2.so (include/stpf2.h): contexts, plans, and the entry points that
+// stand in for the reference's ComputeBackend f2/decode virtuals (src/device/backend.hpp
+// :673-765) and its extract-f2 hot path (src/app/extract_f2_core.cpp:93-407). Host code
+// only: it validates arguments, builds the block layout and work lists, moves data and
+// launches the kernels in decode.cu, f2_simt.cu, f2_umma.cu and jackknife.cu. There is
+// no CPU fallback: without a CUDA device every entry point returns STP_NO_DEVICE.
+#include <algorithm>
+#include <array>
+#include <climits>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "stpf2_internal.cuh"
+
+struct stp_ctx : stpf2::Ctx {};
+
+namespace stpf2 {
+
+int decode_center_count(int64_t n_sel);
+int simt_tile();
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+stp_status guarded(F&& f) {
+    try {
+        f();
+        return STP_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host out of memory";
+        return STP_RUNTIME_ERROR;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return STP_RUNTIME_ERROR;
+    }
+}
+
+void need(bool ok, const char* what) {
+    if (!ok) fail(STP_INVALID_ARGUMENT, what);
+}
+
+void use_device(const Ctx& c) { STPF2_CUDA(cudaSetDevice(c.device)); }
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+template <class T>
+void upload(DevBuf& b, const std::vector<T>& h, cudaStream_t s) {
+    b.reserve(std::max<size_t>(h.size() * sizeof(T), 16));
+    if (!h.empty())
+        STPF2_CUDA(cudaMemcpyAsync(b.ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+}  // namespace
+
+// ---- layout ---------------------------------------------------------------------------
+
+BlockLayout make_block_layout(const int32_t* block_id, int64_t n_snp, int n_block) {
+    BlockLayout L;
+    L.n_block = n_block;
+    L.n_snp = n_snp;
+    std::vector<int64_t> beg(static_cast<size_t>(n_block), 0), end(static_cast<size_t>(n_block), 0);
+    int prev = -1;
+    for (int64_t s = 0; s < n_snp;) {
+        const int b = block_id[s];
+        if (b < 0 || b >= n_block)
+            fail(STP_RUNTIME_ERROR, "block_id[" + std::to_string(s) + "] = " + std::to_string(b) +
+                                        " is out of range [0, " + std::to_string(n_block) + ")");
+        if (b < prev)
+            fail(STP_RUNTIME_ERROR, "block_id is not non-decreasing at column " + std::to_string(s) +
+                                        "; the partition is not contiguous");
+        int64_t e = s;
+        while (e < n_snp && block_id[e] == b) ++e;
+        beg[b] = s;
+        end[b] = e;
+        prev = b;
+        s = e;
+    }
+    L.blocks.resize(static_cast<size_t>(n_block));
+    L.snp_begin = beg;
+    int64_t col = 0;
+    for (int b = 0; b < n_block; ++b) {
+        const int64_t k = end[b] - beg[b];
+        if (k > INT_MAX) fail(STP_RUNTIME_ERROR, "block larger than INT_MAX SNPs");
+        L.blocks[b] = BlockInfo{col, static_cast<int32_t>(k), b};
+        col += (k + kColAlign - 1) / kColAlign * kColAlign;
+    }
+    L.ld = std::max<int64_t>(col, kColAlign);
+    if (L.ld > INT_MAX)
+        fail(STP_RUNTIME_ERROR, "padded SNP axis exceeds INT_MAX columns (M > INT_MAX)");
+    L.snp_col.resize(static_cast<size_t>(n_snp));
+    for (int64_t s = 0; s < n_snp; ++s) {
+        const int b = block_id[s];
+        L.snp_col[s] = static_cast<int32_t>(L.blocks[b].col + (s - beg[b]));
+    }
+    return L;
+}
+
+std::vector<WorkItem> make_work_items(const BlockLayout& L, int P, int tile) {
+    const int T = (P + tile - 1) / tile;
+    std::vector<WorkItem> items;
+    items.reserve(static_cast<size_t>(L.n_block) * T * (T + 1) / 2);
+    for (int b = 0; b < L.n_block; ++b)
+        for (int ti = 0; ti < T; ++ti)
+            for (int tj = ti; tj < T; ++tj) items.push_back(WorkItem{b, static_cast<int16_t>(ti), static_cast<int16_t>(tj)});
+    std::stable_sort(items.begin(), items.end(), [&](const WorkItem& a, const WorkItem& b) {
+        return L.blocks[a.blk].k > L.blocks[b.blk].k;
+    });
+    return items;
+}
+
+size_t operand_plane_bytes(OpFmt f, int P, int64_t ld) {
+    const size_t pl = static_cast<size_t>(P) * static_cast<size_t>(ld);
+    const size_t main = (f == OpFmt::F32) ? 2 * pl * 4 : 5 * pl * 2;
+    return align256(main) + align256(pl);
+}
+
+void bind_operand_planes(OperandPlanes& op, OpFmt f, int P, int64_t ld, void* base) {
+    const size_t pl = static_cast<size_t>(P) * static_cast<size_t>(ld);
+    const size_t main = (f == OpFmt::F32) ? 2 * pl * 4 : 5 * pl * 2;
+    op.fmt = f;
+    op.P = P;
+    op.ld = ld;
+    op.planes = base;
+    op.m_u8 = static_cast<uint8_t*>(base) + align256(main);
+    op.scale_inv = (f == OpFmt::F16) ? 1.0 / double(1 << (2 * kF16PtShift)) : 1.0;
+}
+
+// ---- plan ------------------------------------------------------------------------------
+
+struct Plan {
+    Ctx* ctx = nullptr;
+    int P = 0;
+    int64_t n_sel = 0, n_snp = 0;
+    uint64_t pitch = 0;
+    int precision = 0;
+    bool detect = false;
+    BlockLayout L;
+    DevBuf sel, pop_off, center_idx, snp_col, blocks, items, own_planes;
+    int n_center = 0, n_items = 0;
+    OperandPlanes op;
+    UmmaPlan* umma = nullptr;
+    // Timing: three events per run (start, after decode, after contraction), one set per
+    // run since timing was (re-)enabled, so a timed region of many runs is averaged.
+    bool timing = false;
+    std::vector<std::array<cudaEvent_t, 3>> ev;
+    size_t n_timed = 0;
+
+    ~Plan() {
+        if (umma) umma_plan_destroy(umma);
+        for (auto& t : ev)
+            for (auto e : t)
+                if (e) cudaEventDestroy(e);
+    }
+
+    int launches() const { return (detect ? 1 : 0) + 1 + 1; }
+};
+
+namespace {
+
+// Validates a request and builds its plan. planes_base != nullptr borrows operand
+// storage (at least operand_plane_bytes) instead of allocating it.
+std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch, void* planes_base) {
+    need(r.n_pop >= 0 && r.geno.n_snp >= 0 && r.n_block >= 0, "negative extent");
+    need(r.geno.bytes_per_record > 0 || r.geno.n_snp == 0, "bytes_per_record is 0");
+    need(r.pop_offsets != nullptr || r.n_pop == 0, "pop_offsets is NULL");
+    auto p = std::make_unique<Plan>();
+    p->ctx = &c;
+    p->P = r.n_pop;
+    p->n_snp = r.geno.n_snp;
+    p->pitch = pitch;
+    p->precision = r.precision;
+    const OpFmt fmt = fmt_of(r.precision);
+    const int64_t n_sel = r.n_pop > 0 ? r.pop_offsets[r.n_pop] : 0;
+    p->n_sel = n_sel;
+    need(r.n_pop == 0 || r.pop_offsets[0] == 0, "pop_offsets[0] must be 0");
+    for (int i = 0; i < r.n_pop; ++i)
+        need(r.pop_offsets[i + 1] >= r.pop_offsets[i], "pop_offsets must be non-decreasing");
+    need(n_sel == 0 || r.sel_rows != nullptr, "sel_rows is NULL");
+    need(n_sel < INT_MAX, "too many selected samples");
+    need(r.block_id != nullptr || r.geno.n_snp == 0, "block_id is NULL");
+
+    cudaStream_t s = c.stream;
+    std::vector<uint32_t> sel(static_cast<size_t>(n_sel));
+    const bool auto_ploidy = r.sample_ploidy == nullptr && r.ploidy_mode == STP_PLOIDY_AUTO;
+    for (int64_t g = 0; g < n_sel; ++g) {
+        const int64_t row = r.sel_rows[g];
+        need(row >= 0 && row < r.geno.n_ind, "sel_rows entry outside [0, n_ind)");
+        need(static_cast<uint64_t>(row / 4) < r.geno.bytes_per_record, "sel_rows entry beyond the record");
+        int pl = 0;
+        if (r.sample_ploidy) pl = r.sample_ploidy[g];
+        else if (r.ploidy_mode == STP_PLOIDY_PSEUDO) pl = 1;
+        else if (r.ploidy_mode == STP_PLOIDY_DIPLOID) pl = 2;
+        else need(auto_ploidy, "unknown ploidy_mode");
+        if (pl != 1 && pl != 2) pl = 0;  // a bad ploidy contributes nothing (decode_af.hpp:58-65)
+        sel[g] = pack_sel(row, pl);
+    }
+    p->detect = auto_ploidy;
+    upload(p->sel, sel, s);
+
+    std::vector<int32_t> po(static_cast<size_t>(r.n_pop) + 1, 0);
+    for (int i = 0; i <= r.n_pop && r.n_pop > 0; ++i) po[i] = static_cast<int32_t>(r.pop_offsets[i]);
+    upload(p->pop_off, po, s);
+
+    p->n_center = decode_center_count(n_sel);
+    std::vector<int32_t> ci(static_cast<size_t>(p->n_center));
+    for (int k = 0; k < p->n_center; ++k) ci[k] = static_cast<int32_t>((static_cast<int64_t>(k) * n_sel) / p->n_center);
+    upload(p->center_idx, ci, s);
+
+    p->L = make_block_layout(r.block_id, r.geno.n_snp, r.n_block);
+    upload(p->snp_col, p->L.snp_col, s);
+    upload(p->blocks, p->L.blocks, s);
+
+    const size_t ob = operand_plane_bytes(fmt, std::max(r.n_pop, 1), p->L.ld);
+    if (!planes_base) {
+        p->own_planes.reserve(ob);
+        planes_base = p->own_planes.ptr;
+    }
+    // Padding columns must read as zero; decode only ever writes real SNP columns.
+    STPF2_CUDA(cudaMemsetAsync(planes_base, 0, ob, s));
+    bind_operand_planes(p->op, fmt, r.n_pop, p->L.ld, planes_base);
+
+    if (r.precision == STP_PREC_FP32_SIMT) {
+        const std::vector<WorkItem> items = make_work_items(p->L, r.n_pop, simt_tile());
+        p->n_items = static_cast<int>(items.size());
+        upload(p->items, items, s);
+    } else if (r.n_pop > 0 && r.n_block > 0) {
+        p->umma = umma_plan_create(c, p->op, p->L);
+    }
+    return p;
+}
+
+void run_plan(Plan& p, const uint8_t* d_records, double* d_f2, double* d_vpair, cudaStream_t s) {
+    Ctx& c = *p.ctx;
+    const size_t out_elems = static_cast<size_t>(p.P) * p.P * p.L.n_block;
+    if (p.P <= 0 || p.L.n_block <= 0) return;
+    if (p.n_snp <= 0) {  // no SNPs: every block is empty -> zeros (cpu_backend.cpp:234)
+        STPF2_CUDA(cudaMemsetAsync(d_f2, 0, out_elems * sizeof(double), s));
+        STPF2_CUDA(cudaMemsetAsync(d_vpair, 0, out_elems * sizeof(double), s));
+        return;
+    }
+    std::array<cudaEvent_t, 3>* tev = nullptr;
+    if (p.timing) {
+        if (p.n_timed == p.ev.size()) {
+            std::array<cudaEvent_t, 3> t{};
+            for (auto& e : t) STPF2_CUDA(cudaEventCreate(&e));
+            p.ev.push_back(t);
+        }
+        tev = &p.ev[p.n_timed++];
+        STPF2_CUDA(cudaEventRecord((*tev)[0], s));
+    }
+    if (p.detect)
+        launch_detect_ploidy_pa(c, d_records, p.pitch, p.n_snp, p.sel.as<uint32_t>(), p.n_sel, s);
+    PaDecodeArgs a;
+    a.records = d_records;
+    a.pitch = p.pitch;
+    a.n_snp = p.n_snp;
+    a.sel = p.sel.as<uint32_t>();
+    a.pop_off = p.pop_off.as<int32_t>();
+    a.P = p.P;
+    a.center_idx = p.center_idx.as<int32_t>();
+    a.n_center = p.n_center;
+    a.snp_col = p.snp_col.as<int32_t>();
+    a.op = p.op;
+    launch_decode_pa(c, a, s);
+    if (tev) STPF2_CUDA(cudaEventRecord((*tev)[1], s));
+    if (p.precision == STP_PREC_FP32_SIMT)
+        launch_f2_simt(c, p.items.as<WorkItem>(), p.n_items, p.blocks.as<BlockInfo>(), p.op, d_f2, d_vpair, s);
+    else
+        launch_f2_umma(c, p.umma, d_f2, d_vpair, s);
+    if (tev) STPF2_CUDA(cudaEventRecord((*tev)[2], s));
+}
+
+void copy_block_sizes(const BlockLayout& L, int32_t* out) {
+    for (int b = 0; b < L.n_block; ++b) out[b] = L.blocks[b].k;
+}
+
+void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
+    need(o.f2 != nullptr || r.n_pop == 0 || r.n_block == 0, "output f2 is NULL");
+    need(o.vpair != nullptr || r.n_pop == 0 || r.n_block == 0, "output vpair is NULL");
+    cudaStream_t s = c.stream;
+    const uint8_t* d_rec = r.geno.records;
+    uint64_t pitch = r.geno.pitch ? r.geno.pitch : r.geno.bytes_per_record;
+    need(pitch >= r.geno.bytes_per_record, "pitch < bytes_per_record");
+    if (!r.geno.on_device && r.geno.n_snp > 0) {
+        need(r.geno.records != nullptr, "records is NULL");
+        const uint64_t dp = (r.geno.bytes_per_record + 15) / 16 * 16;
+        c.ws_records.reserve(static_cast<size_t>(dp) * r.geno.n_snp);
+        STPF2_CUDA(cudaMemcpy2DAsync(c.ws_records.ptr, dp, r.geno.records, pitch, r.geno.bytes_per_record,
+                                     static_cast<size_t>(r.geno.n_snp), cudaMemcpyHostToDevice, s));
+        d_rec = c.ws_records.as<uint8_t>();
+        pitch = dp;
+    }
+    // Operand planes borrow the context's grow-only workspace.
+    {
+        const BlockLayout probe = make_block_layout(r.block_id, r.geno.n_snp, r.n_block);
+        c.ws_misc.reserve(operand_plane_bytes(fmt_of(r.precision), std::max(r.n_pop, 1), probe.ld));
+    }
+    std::unique_ptr<Plan> p = build_plan(c, r, pitch, c.ws_misc.ptr);
+    if (o.block_sizes) copy_block_sizes(p->L, o.block_sizes);
+    const size_t out_elems = static_cast<size_t>(std::max(r.n_pop, 0)) * std::max(r.n_pop, 0) * std::max(r.n_block, 0);
+    double* d_f2 = o.f2;
+    double* d_vp = o.vpair;
+    if (!o.on_device && out_elems) {
+        c.ws_f2.reserve(out_elems * sizeof(double));
+        c.ws_vpair.reserve(out_elems * sizeof(double));
+        d_f2 = c.ws_f2.as<double>();
+        d_vp = c.ws_vpair.as<double>();
+    }
+    run_plan(*p, d_rec, d_f2, d_vp, s);
+    if (!o.on_device && out_elems) {
+        STPF2_CUDA(cudaMemcpyAsync(o.f2, d_f2, out_elems * sizeof(double), cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaMemcpyAsync(o.vpair, d_vp, out_elems * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    if (o.ploidy_out && p->n_sel > 0) {
+        std::vector<uint32_t> sel(static_cast<size_t>(p->n_sel));
+        STPF2_CUDA(cudaMemcpyAsync(sel.data(), p->sel.ptr, sel.size() * 4, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaStreamSynchronize(s));
+        for (size_t g = 0; g < sel.size(); ++g) o.ploidy_out[g] = static_cast<int32_t>(sel[g] & 3u);
+    }
+    STPF2_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+}  // namespace stpf2
+
+struct stp_plan {
+    std::unique_ptr<stpf2::Plan> p;
+};
+
+using namespace stpf2;
+
+extern "C" {
+
+int stp_abi_version(void) { return STPF2_ABI_VERSION; }
+
+const char* stp_last_error(void) { return g_last_error.c_str(); }
+
+stp_ctx* stp_create(int device, stp_status* status) {
+    stp_ctx* out = nullptr;
+    const stp_status st = guarded([&] {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0)
+            fail(STP_NO_DEVICE, "no CUDA device available (a CUDA-capable B200 is required)");
+        need(device >= 0 && device < n, "device ordinal out of range");
+        STPF2_CUDA(cudaSetDevice(device));
+        int major = 0, minor = 0;
+        STPF2_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+        STPF2_CUDA(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device));
+        if (major != 10 || minor != 0)
+            fail(STP_NO_DEVICE, "libstpf2 is built for sm_100a (B200); device has sm_" +
+                                    std::to_string(major) + std::to_string(minor));
+        auto c = std::make_unique<stp_ctx>();
+        c->device = device;
+        STPF2_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+        STPF2_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        out = c.release();
+    });
+    if (status) *status = st;
+    return out;
+}
+
+void stp_destroy(stp_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+}
+
+uint64_t stp_launch_count(const stp_ctx* ctx) { return ctx ? ctx->launches.load() : 0; }
+
+stp_status stp_detect_ploidy(stp_ctx* ctx, const stp_geno_view* geno, const int64_t* sel_rows, int64_t n_sel,
+                             int32_t* ploidy) {
+    return guarded([&] {
+        need(ctx && geno, "null argument");
+        use_device(*ctx);
+        if (n_sel <= 0) return;
+        need(sel_rows && ploidy, "null argument");
+        cudaStream_t s = ctx->stream;
+        std::vector<uint32_t> sel(static_cast<size_t>(n_sel));
+        for (int64_t g = 0; g < n_sel; ++g) {
+            need(sel_rows[g] >= 0 && sel_rows[g] < geno->n_ind, "sel_rows entry outside [0, n_ind)");
+            sel[g] = pack_sel(sel_rows[g], 0);
+        }
+        DevBuf d_sel, d_rec;
+        upload(d_sel, sel, s);
+        const uint8_t* rec = geno->records;
+        uint64_t pitch = geno->pitch ? geno->pitch : geno->bytes_per_record;
+        const int64_t window = std::min<int64_t>(geno->n_snp, 1000);
+        if (!geno->on_device && window > 0) {
+            d_rec.reserve(static_cast<size_t>(pitch) * window);
+            STPF2_CUDA(cudaMemcpyAsync(d_rec.ptr, rec, static_cast<size_t>(pitch) * window, cudaMemcpyHostToDevice, s));
+            rec = d_rec.as<uint8_t>();
+        }
+        launch_detect_ploidy_pa(*ctx, rec, pitch, geno->n_snp, d_sel.as<uint32_t>(), n_sel, s);
+        STPF2_CUDA(cudaMemcpyAsync(sel.data(), d_sel.ptr, sel.size() * 4, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaStreamSynchronize(s));
+        for (int64_t g = 0; g < n_sel; ++g) ploidy[g] = static_cast<int32_t>(sel[g] & 3u);
+    });
+}
+
+stp_status stp_decode_counts(stp_ctx* ctx, const stp_geno_view* geno, const int64_t* sel_rows,
+                             const int64_t* pop_offsets, int32_t n_pop, const int32_t* sample_ploidy,
+                             int32_t ploidy_mode, int32_t* ac2, int32_t* n) {
+    return guarded([&] {
+        need(ctx && geno, "null argument");
+        use_device(*ctx);
+        if (n_pop <= 0 || geno->n_snp <= 0) return;
+        need(ac2 && n, "null output");
+        cudaStream_t s = ctx->stream;
+        // One block spanning all SNPs: the counts do not depend on the block layout.
+        std::vector<int32_t> bid(static_cast<size_t>(geno->n_snp), 0);
+        stp_f2_request r{};
+        r.geno = *geno;
+        r.sel_rows = sel_rows;
+        r.pop_offsets = pop_offsets;
+        r.n_pop = n_pop;
+        r.sample_ploidy = sample_ploidy;
+        r.ploidy_mode = ploidy_mode;
+        r.block_id = bid.data();
+        r.n_block = 1;
+        r.precision = STP_PREC_FP32_SIMT;
+        const uint8_t* d_rec = geno->records;
+        uint64_t pitch = geno->pitch ? geno->pitch : geno->bytes_per_record;
+        DevBuf rec;
+        if (!geno->on_device) {
+            const uint64_t dp = (geno->bytes_per_record + 15) / 16 * 16;
+            rec.reserve(static_cast<size_t>(dp) * geno->n_snp);
+            STPF2_CUDA(cudaMemcpy2DAsync(rec.ptr, dp, geno->records, pitch, geno->bytes_per_record,
+                                         static_cast<size_t>(geno->n_snp), cudaMemcpyHostToDevice, s));
+            d_rec = rec.as<uint8_t>();
+            pitch = dp;
+        }
+        std::unique_ptr<Plan> p = build_plan(*ctx, r, pitch, nullptr);
+        const size_t cnt = static_cast<size_t>(n_pop) * geno->n_snp;
+        DevBuf d_ac2, d_n;
+        d_ac2.reserve(cnt * 4);
+        d_n.reserve(cnt * 4);
+        if (p->detect)
+            launch_detect_ploidy_pa(*ctx, d_rec, pitch, p->n_snp, p->sel.as<uint32_t>(), p->n_sel, s);
+        PaDecodeArgs a;
+        a.records = d_rec;
+        a.pitch = pitch;
+        a.n_snp = geno->n_snp;
+        a.sel = p->sel.as<uint32_t>();
+        a.pop_off = p->pop_off.as<int32_t>();
+        a.P = n_pop;
+        a.center_idx = p->center_idx.as<int32_t>();
+        a.n_center = p->n_center;
+        a.snp_col = p->snp_col.as<int32_t>();
+        a.op = p->op;
+        a.cnt_ac2 = d_ac2.as<int32_t>();
+        a.cnt_n = d_n.as<int32_t>();
+        launch_decode_pa(*ctx, a, s);
+        STPF2_CUDA(cudaMemcpyAsync(ac2, d_ac2.ptr, cnt * 4, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaMemcpyAsync(n, d_n.ptr, cnt * 4, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+stp_status stp_decode_af(stp_ctx* ctx, const uint8_t* packed, uint64_t bpr, int64_t n_snp, int64_t n_ind,
+                         const int64_t* pop_offsets, int32_t n_pop, const int32_t* sample_ploidy, int32_t ploidy,
+                         int32_t detect, int32_t packed_on_device, double* q, double* v, double* n) {
+    return guarded([&] {
+        need(ctx != nullptr, "null context");
+        use_device(*ctx);
+        if (n_pop <= 0 || n_snp <= 0) return;
+        need(q && v && n && pop_offsets, "null argument");
+        need(bpr * 4 >= static_cast<uint64_t>(n_snp), "bytes_per_record too small for n_snp");
+        need(pop_offsets[n_pop] <= n_ind, "pop_offsets exceed n_individuals");
+        cudaStream_t s = ctx->stream;
+        DevBuf d_pk, d_pl, d_po, d_q, d_v, d_n;
+        const uint8_t* pk = packed;
+        if (!packed_on_device) {
+            d_pk.reserve(static_cast<size_t>(bpr) * std::max<int64_t>(n_ind, 1));
+            STPF2_CUDA(cudaMemcpyAsync(d_pk.ptr, packed, static_cast<size_t>(bpr) * n_ind, cudaMemcpyHostToDevice, s));
+            pk = d_pk.as<uint8_t>();
+        }
+        d_pl.reserve(sizeof(int32_t) * std::max<int64_t>(n_ind, 1));
+        if (sample_ploidy) {
+            STPF2_CUDA(cudaMemcpyAsync(d_pl.ptr, sample_ploidy, sizeof(int32_t) * n_ind, cudaMemcpyHostToDevice, s));
+        } else if (detect) {
+            launch_detect_ploidy_canonical(*ctx, pk, bpr, n_snp, n_ind, d_pl.as<int32_t>(), s);
+        } else {
+            std::vector<int32_t> pl(static_cast<size_t>(n_ind), ploidy);
+            upload(d_pl, pl, s);
+        }
+        std::vector<int32_t> po(static_cast<size_t>(n_pop) + 1);
+        for (int i = 0; i <= n_pop; ++i) po[i] = static_cast<int32_t>(pop_offsets[i]);
+        upload(d_po, po, s);
+        const size_t cnt = static_cast<size_t>(n_pop) * n_snp;
+        d_q.reserve(cnt * 8);
+        d_v.reserve(cnt * 8);
+        d_n.reserve(cnt * 8);
+        launch_decode_canonical(*ctx, pk, bpr, n_snp, n_ind, d_po.as<int32_t>(), n_pop, d_pl.as<int32_t>(),
+                                d_q.as<double>(), d_v.as<double>(), d_n.as<double>(), s);
+        STPF2_CUDA(cudaMemcpyAsync(q, d_q.ptr, cnt * 8, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaMemcpyAsync(v, d_v.ptr, cnt * 8, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaMemcpyAsync(n, d_n.ptr, cnt * 8, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+stp_status stp_f2_from_qvn(stp_ctx* ctx, const double* Q, const double* V, const double* N, int32_t P, int64_t M,
+                           const int32_t* block_id, int32_t n_block, int32_t precision, double* f2,
+                           double* vpair, int32_t* block_sizes) {
+    return guarded([&] {
+        need(ctx != nullptr, "null context");
+        use_device(*ctx);
+        need(P >= 0 && M >= 0 && n_block >= 0, "negative extent");
+        const size_t out_elems = static_cast<size_t>(P) * P * n_block;
+        if (n_block > 0 && block_sizes) std::fill(block_sizes, block_sizes + n_block, 0);
+        if (P <= 0 || n_block <= 0) return;
+        need(f2 && vpair, "null output");
+        if (M <= 0) {
+            std::fill(f2, f2 + out_elems, 0.0);
+            std::fill(vpair, vpair + out_elems, 0.0);
+            return;
+        }
+        need(Q && V && N && block_id, "null input");
+        cudaStream_t s = ctx->stream;
+        const BlockLayout L = make_block_layout(block_id, M, n_block);
+        if (block_sizes) copy_block_sizes(L, block_sizes);
+        const OpFmt fmt = fmt_of(precision);
+        DevBuf d_qvn, d_col, d_planes, d_blocks, d_items, d_f2, d_vp;
+        const size_t pm = static_cast<size_t>(P) * M;
+        d_qvn.reserve(3 * pm * 8);
+        double* dq = d_qvn.as<double>();
+        STPF2_CUDA(cudaMemcpyAsync(dq, Q, pm * 8, cudaMemcpyHostToDevice, s));
+        STPF2_CUDA(cudaMemcpyAsync(dq + pm, V, pm * 8, cudaMemcpyHostToDevice, s));
+        STPF2_CUDA(cudaMemcpyAsync(dq + 2 * pm, N, pm * 8, cudaMemcpyHostToDevice, s));
+        upload(d_col, L.snp_col, s);
+        upload(d_blocks, L.blocks, s);
+        const size_t ob = operand_plane_bytes(fmt, P, L.ld);
+        d_planes.reserve(ob);
+        STPF2_CUDA(cudaMemsetAsync(d_planes.ptr, 0, ob, s));
+        OperandPlanes op;
+        bind_operand_planes(op, fmt, P, L.ld, d_planes.ptr);
+        launch_feed_qvn(*ctx, dq, dq + pm, dq + 2 * pm, P, M, d_col.as<int32_t>(), op, s);
+        d_f2.reserve(out_elems * 8);
+        d_vp.reserve(out_elems * 8);
+        if (precision == STP_PREC_FP32_SIMT) {
+            const std::vector<WorkItem> items = make_work_items(L, P, simt_tile());
+            upload(d_items, items, s);
+            launch_f2_simt(*ctx, d_items.as<WorkItem>(), static_cast<int>(items.size()), d_blocks.as<BlockInfo>(), op,
+                           d_f2.as<double>(), d_vp.as<double>(), s);
+        } else {
+            UmmaPlan* up = umma_plan_create(*ctx, op, L);
+            try {
+                launch_f2_umma(*ctx, up, d_f2.as<double>(), d_vp.as<double>(), s);
+            } catch (...) {
+                cudaStreamSynchronize(s);
+                umma_plan_destroy(up);
+                throw;
+            }
+            STPF2_CUDA(cudaStreamSynchronize(s));
+            umma_plan_destroy(up);
+        }
+        STPF2_CUDA(cudaMemcpyAsync(f2, d_f2.ptr, out_elems * 8, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaMemcpyAsync(vpair, d_vp.ptr, out_elems * 8, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+stp_status stp_f2_extract_blocks(stp_ctx* ctx, const stp_f2_request* req, stp_f2_output* out) {
+    return guarded([&] {
+        need(ctx && req && out, "null argument");
+        use_device(*ctx);
+        if (req->n_block > 0 && out->block_sizes) std::fill(out->block_sizes, out->block_sizes + req->n_block, 0);
+        if (req->n_pop <= 0 || req->n_block <= 0) return;
+        extract_one(*ctx, *req, *out);
+    });
+}
+
+stp_status stp_f2_extract_batch(stp_ctx* ctx, const stp_f2_request* reqs, int32_t n_req, stp_f2_output* outs) {
+    return guarded([&] {
+        need(ctx && (reqs || n_req == 0) && (outs || n_req == 0), "null argument");
+        use_device(*ctx);
+        for (int32_t k = 0; k < n_req; ++k) {
+            if (reqs[k].n_block > 0 && outs[k].block_sizes)
+                std::fill(outs[k].block_sizes, outs[k].block_sizes + reqs[k].n_block, 0);
+            if (reqs[k].n_pop <= 0 || reqs[k].n_block <= 0) continue;
+            extract_one(*ctx, reqs[k], outs[k]);
+        }
+    });
+}
+
+stp_status stp_f2_jackknife(stp_ctx* ctx, const double* x, const int32_t* block_sizes, int64_t m, int32_t n_block,
+                            double* est, double* var) {
+    return guarded([&] {
+        need(ctx != nullptr, "null context");
+        use_device(*ctx);
+        if (m <= 0 || n_block <= 0) return;
+        need(x && block_sizes && est && var, "null argument");
+        cudaStream_t s = ctx->stream;
+        DevBuf d_x, d_b, d_e, d_v;
+        const size_t xe = static_cast<size_t>(m) * n_block;
+        d_x.reserve(xe * 8);
+        STPF2_CUDA(cudaMemcpyAsync(d_x.ptr, x, xe * 8, cudaMemcpyHostToDevice, s));
+        std::vector<int32_t> bs(block_sizes, block_sizes + n_block);
+        upload(d_b, bs, s);
+        d_e.reserve(static_cast<size_t>(m) * 8);
+        d_v.reserve(static_cast<size_t>(m) * 8);
+        launch_jackknife(*ctx, d_x.as<double>(), d_b.as<int32_t>(), m, n_block, d_e.as<double>(), d_v.as<double>(), s);
+        STPF2_CUDA(cudaMemcpyAsync(est, d_e.ptr, static_cast<size_t>(m) * 8, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaMemcpyAsync(var, d_v.ptr, static_cast<size_t>(m) * 8, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+stp_plan* stp_plan_create(stp_ctx* ctx, const stp_f2_request* req, stp_status* status) {
+    stp_plan* out = nullptr;
+    const stp_status st = guarded([&] {
+        need(ctx && req, "null argument");
+        use_device(*ctx);
+        need(req->geno.on_device || req->geno.n_snp == 0, "a plan needs device-resident genotype records");
+        const uint64_t pitch = req->geno.pitch ? req->geno.pitch : req->geno.bytes_per_record;
+        std::unique_ptr<Plan> p = build_plan(*ctx, *req, pitch, nullptr);
+        STPF2_CUDA(cudaStreamSynchronize(ctx->stream));
+        auto* sp = new stp_plan();
+        sp->p = std::move(p);
+        out = sp;
+    });
+    if (status) *status = st;
+    return out;
+}
+
+stp_status stp_plan_run(stp_plan* plan, const uint8_t* d_records, double* d_f2, double* d_vpair, void* stream) {
+    return guarded([&] {
+        need(plan != nullptr, "null plan");
+        Plan& p = *plan->p;
+        use_device(*p.ctx);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p.ctx->stream;
+        run_plan(p, d_records, d_f2, d_vpair, s);
+    });
+}
+
+int32_t stp_plan_launches(const stp_plan* plan) { return plan ? plan->p->launches() : 0; }
+
+stp_status stp_plan_set_timing(stp_plan* plan, int32_t enable) {
+    return guarded([&] {
+        need(plan != nullptr, "null plan");
+        plan->p->timing = enable != 0;
+        plan->p->n_timed = 0;
+    });
+}
+
+stp_status stp_plan_last_times(const stp_plan* plan, float* decode_ms, float* contract_ms) {
+    return guarded([&] {
+        need(plan != nullptr, "null plan");
+        const Plan& p = *plan->p;
+        double sa = 0.0, sb = 0.0;
+        for (size_t k = 0; k < p.n_timed; ++k) {
+            STPF2_CUDA(cudaEventSynchronize(p.ev[k][2]));
+            float a = 0.f, b = 0.f;
+            STPF2_CUDA(cudaEventElapsedTime(&a, p.ev[k][0], p.ev[k][1]));
+            STPF2_CUDA(cudaEventElapsedTime(&b, p.ev[k][1], p.ev[k][2]));
+            sa += a;
+            sb += b;
+        }
+        const double n = p.n_timed ? static_cast<double>(p.n_timed) : 1.0;
+        if (decode_ms) *decode_ms = static_cast<float>(sa / n);
+        if (contract_ms) *contract_ms = static_cast<float>(sb / n);
+    });
+}
+
+void stp_plan_destroy(stp_plan* plan) {
+    if (!plan) return;
+    cudaSetDevice(plan->p->ctx->device);
+    cudaStreamSynchronize(plan->p->ctx->stream);
+    delete plan;
+}
+
+}  // extern "C"

@@ -1,0 +1,195 @@
+// steppecu_b200/csrc/stpf2_internal.cuh
+//
+// Shared internals of libstpf2.so: error plumbing, the context, the block layout that
+// maps jackknife blocks onto padded operand columns, and the launch wrappers each .cu
+// file exports to the C-ABI layer (stpf2_abi.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/stpf2.h"
+
+namespace stpf2 {
+
+// ---- errors --------------------------------------------------------------------------
+
+// Carries a status code through C++ code paths; the C-ABI layer turns it into the
+// return value plus the thread's last-error message.
+struct Error : std::runtime_error {
+    stp_status status;
+    Error(stp_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] inline void fail(stp_status s, const std::string& m) { throw Error(s, m); }
+
+inline void cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    const stp_status s = (e == cudaErrorMemoryAllocation) ? STP_DEVICE_OOM : STP_CUDA_ERROR;
+    fail(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define STPF2_CUDA(call) ::stpf2::cuda_check((call), #call)
+
+// ---- device buffers -------------------------------------------------------------------
+
+// Owning device allocation (RAII). Sizes in bytes.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); ptr = o.ptr; bytes = o.bytes; o.ptr = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void release() { if (ptr) cudaFree(ptr); ptr = nullptr; bytes = 0; }
+    // Grows (never shrinks) to at least n bytes; contents are not preserved.
+    void reserve(size_t n) {
+        if (n <= bytes) return;
+        release();
+        if (n == 0) return;
+        STPF2_CUDA(cudaMalloc(&ptr, n));
+        bytes = n;
+    }
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// ---- context --------------------------------------------------------------------------
+
+struct Ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    std::atomic<uint64_t> launches{0};
+    // Grow-only scratch reused across calls of the host-buffer entry points, so repeated
+    // extractions do not pay cudaMalloc each time.
+    DevBuf ws_records, ws_f2, ws_vpair, ws_misc;
+};
+
+// ---- block layout ---------------------------------------------------------------------
+
+// Column padding of every block in the operand planes: a block's first column is a
+// multiple of kColAlign so tensor-core tiles start on aligned addresses, and its tail up
+// to the next multiple stays zero (zero operands contribute nothing to any sum).
+constexpr int kColAlign = 64;
+
+struct BlockInfo {  // device-visible, one per jackknife block
+    int64_t col;    // first padded column
+    int32_t k;      // SNPs in the block
+    int32_t b;      // block id (slab index of the output)
+};
+
+struct BlockLayout {
+    int n_block = 0;
+    int64_t n_snp = 0;
+    int64_t ld = 0;  // padded column count = row pitch of every operand plane
+    std::vector<int64_t> snp_begin;
+    std::vector<BlockInfo> blocks;
+    std::vector<int32_t> snp_col;  // padded column of every SNP
+};
+
+// Validates a contiguous non-decreasing partition (core::block_ranges,
+// src/core/domain/block_partition_rule.hpp:56-96) and builds the padded column map.
+BlockLayout make_block_layout(const int32_t* block_id, int64_t n_snp, int n_block);
+
+// Work item of the contraction: tile pair (ti <= tj) of one block.
+struct WorkItem {
+    int32_t blk;  // index into BlockInfo array
+    int16_t ti, tj;
+};
+
+// Tile pairs of every block, costliest (largest k) first.
+std::vector<WorkItem> make_work_items(const BlockLayout& L, int P, int tile);
+
+// ---- operand planes --------------------------------------------------------------------
+
+// Operand formats the decode/feeder kernels emit, one per contraction arithmetic.
+enum class OpFmt : int { F32 = 0, BF16 = 1, F16 = 2 };
+
+inline OpFmt fmt_of(int precision) {
+    switch (precision) {
+        case STP_PREC_FP32_SIMT: return OpFmt::F32;
+        case STP_PREC_SPLIT_BF16: return OpFmt::BF16;
+        case STP_PREC_SPLIT_F16: return OpFmt::F16;
+    }
+    fail(STP_INVALID_ARGUMENT, "unknown precision mode " + std::to_string(precision));
+}
+
+// Where decode/feeder write. For F32: planes = [Pt f32][Ah f32] (2 planes) + m_u8.
+// For BF16/F16: planes = 16-bit [Pt_hi][Pt_lo][Ah_hi][Ah_lo][M] (5 planes) + m_u8 (int8 M).
+// Plane p, row i, column c at planes + (p * P + i) * ld + c (elements of the plane type).
+// Pt = m*(q - c_s), Ah = m*((q - c_s)^2 - h)/2, h = q(1-q)/max(n-1,1), m = [n > 0];
+// then num(i,j) = 2 * sum_s (Ah_i M_j + M_i Ah_j - Pt_i Pt_j).
+struct OperandPlanes {
+    OpFmt fmt = OpFmt::F32;
+    int P = 0;
+    int64_t ld = 0;
+    void* planes = nullptr;
+    uint8_t* m_u8 = nullptr;
+    double scale_inv = 1.0;  // numerator scale undo (F16 planes are pre-scaled)
+};
+
+constexpr int kF16PtShift = 7;  // F16: Pt scaled by 2^7, Ah by 2^14 (num by 2^14)
+
+size_t operand_plane_bytes(OpFmt f, int P, int64_t ld);
+void bind_operand_planes(OperandPlanes& op, OpFmt f, int P, int64_t ld, void* base);
+
+// ---- launch wrappers (defined in the .cu files) ----------------------------------------
+
+// Selected-sample descriptor for the PA decode: byte offset in the record << 5 |
+// code shift << 2 | ploidy (0 = contributes nothing).
+inline uint32_t pack_sel(int64_t row, int ploidy) {
+    const uint32_t byte = static_cast<uint32_t>(row >> 2);
+    const uint32_t shift = static_cast<uint32_t>(6 - 2 * (row & 3));
+    return (byte << 5) | (shift << 2) | static_cast<uint32_t>(ploidy & 3);
+}
+
+struct PaDecodeArgs {
+    const uint8_t* records = nullptr;
+    uint64_t pitch = 0;
+    int64_t n_snp = 0;
+    const uint32_t* sel = nullptr;      // [n_sel] packed descriptors (ploidy filled in)
+    const int32_t* pop_off = nullptr;   // [P+1]
+    int P = 0;
+    const int32_t* center_idx = nullptr;  // [n_center] indices into sel: the centring subset
+    int n_center = 0;
+    const int32_t* snp_col = nullptr;   // [n_snp]
+    OperandPlanes op;
+    int32_t* cnt_ac2 = nullptr;         // optional [P x n_snp] column-major
+    int32_t* cnt_n = nullptr;
+};
+
+void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_snp,
+                             uint32_t* sel, int64_t n_sel, cudaStream_t s);
+void launch_decode_pa(Ctx& c, const PaDecodeArgs& a, cudaStream_t s);
+void launch_decode_canonical(Ctx& c, const uint8_t* packed, uint64_t bpr, int64_t n_snp,
+                             int64_t n_ind, const int32_t* pop_off, int P, const int32_t* ploidy,
+                             double* q, double* v, double* n, cudaStream_t s);
+void launch_detect_ploidy_canonical(Ctx& c, const uint8_t* packed, uint64_t bpr, int64_t n_snp,
+                                    int64_t n_ind, int32_t* ploidy, cudaStream_t s);
+void launch_feed_qvn(Ctx& c, const double* Q, const double* V, const double* N, int P,
+                     int64_t M, const int32_t* snp_col, const OperandPlanes& op, cudaStream_t s);
+
+void launch_f2_simt(Ctx& c, const WorkItem* items, int n_items, const BlockInfo* blocks,
+                    const OperandPlanes& op, double* f2, double* vpair, cudaStream_t s);
+
+// tcgen05 contraction; returns false if the device cannot run it.
+struct UmmaPlan;
+UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L);
+void umma_plan_destroy(UmmaPlan* p);
+void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s);
+int umma_tile();
+
+void launch_jackknife(Ctx& c, const double* x, const int32_t* block_sizes, int64_t m, int nb,
+                      double* est, double* var, cudaStream_t s);
+
+}  // namespace stpf2

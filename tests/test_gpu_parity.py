@@ -1,0 +1,248 @@
+"""GPU parity through the C ABI against the CPU oracle on identical seeded inputs.
+
+Counts, ploidy, vpair and the canonical decode are compared bit for bit. f2 is compared
+with the tolerance of each contraction arithmetic (see TOL), checked as
+|gpu - oracle| <= atol + rtol * |oracle| element-wise, with the worst errors printed.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from steppecu_b200 import F2Tensor, StpError, extract_f2, read_f2, synth
+from steppecu_b200.synth import write_eigenstrat
+
+pytestmark = pytest.mark.gpu
+
+# Per-arithmetic f2 tolerance: (rtol, atol). The numerator is accumulated over <= 64-SNP
+# chunks in FP32 and summed in FP64; see the precision section of the design notes.
+TOL = {
+    "fp32": (2e-5, 2e-7),
+    "split_bf16": (2e-5, 2e-7),
+    "split_f16": (2e-5, 2e-7),
+}
+MODES = ["fp32"]
+
+
+def oracle_f2(panel, sel, po, ploidy=None, block_id=None, n_block=None):
+    rec = panel.records_numpy()
+    pl = oracle.detect_ploidy_pa(rec, sel) if ploidy is None else ploidy
+    bid = panel.block_id if block_id is None else block_id
+    nb = panel.n_block if n_block is None else n_block
+    f2, vp, bs = oracle.f2_from_panel(rec, sel, po, bid, nb, pl, threads=8)
+    return F2Tensor(f2, vp, bs, len(po) - 1, nb), pl
+
+
+def f2_error(got: np.ndarray, want: np.ndarray) -> dict:
+    d = np.abs(got - want)
+    rel = d / np.maximum(np.abs(want), 1e-300)
+    big = np.abs(want) >= 1e-12
+    return {"max_abs": float(d.max(initial=0)), "max_rel": float(rel[big].max(initial=0)),
+            "max_comb": float((d / (1e-9 + np.abs(want))).max(initial=0))}
+
+
+def assert_f2_close(got: F2Tensor, want: F2Tensor, mode: str):
+    assert got.P == want.P and got.n_block == want.n_block
+    assert np.array_equal(got.block_sizes, want.block_sizes)
+    assert np.array_equal(got.vpair, want.vpair), "vpair must be bit-exact"
+    rtol, atol = TOL[mode]
+    err = f2_error(got.f2, want.f2)
+    print(f"[{mode}] f2 error vs oracle: {err}")
+    bad = np.abs(got.f2 - want.f2) > atol + rtol * np.abs(want.f2)
+    assert not bad.any(), (err, int(bad.sum()))
+    cube = got.cube()
+    assert np.array_equal(cube, cube.transpose(1, 0, 2)), "f2 slabs must be exactly symmetric"
+
+
+@pytest.fixture(scope="module")
+def c1():
+    p = synth.generate("c1", seed=20261203)
+    sel, po = p.selection()
+    want, pl = oracle_f2(p, sel, po)
+    return p, sel, po, want, pl
+
+
+@pytest.fixture(scope="module")
+def uneven():
+    """Uneven population sizes (1..60), half pseudo-haploid, Beta(2,3) missingness,
+    lognormal blocks: the shape of the batched-uneven workload at test size."""
+    p = synth.generate("c4", seed=7, n_snp=40_000, n_pop=37)
+    sel, po = p.selection()
+    want, pl = oracle_f2(p, sel, po)
+    return p, sel, po, want, pl
+
+
+# ---- decode -------------------------------------------------------------------------------
+
+def test_detect_ploidy_bitexact(ctx, uneven):
+    p, sel, po, _, pl = uneven
+    got = ctx.detect_ploidy(p.records_numpy(), p.n_ind, sel)
+    assert np.array_equal(got, pl)
+    # The generator's truth: every diploid with a het in the window is found.
+    assert set(np.unique(got)) <= {1, 2}
+
+
+@pytest.mark.parametrize("ploidy", ["auto", "pseudo", "diploid"])
+def test_decode_counts_bitexact(ctx, uneven, ploidy):
+    p, sel, po, _, pl = uneven
+    rec = p.records_numpy()
+    if ploidy == "auto":
+        opl = pl
+    else:
+        opl = np.full(sel.size, 1 if ploidy == "pseudo" else 2, np.int32)
+    ac2, n = ctx.decode_counts(rec, p.n_ind, sel, po, ploidy=ploidy)
+    wa, wn = oracle.decode_counts_pa(rec, sel, po, opl)
+    P = len(po) - 1
+    assert np.array_equal(ac2, wa.reshape(-1, P).T) and np.array_equal(n, wn.reshape(-1, P).T)
+
+
+def test_decode_counts_device_records(ctx, uneven):
+    import torch
+
+    p, sel, po, _, pl = uneven
+    rec = p.records_numpy()
+    d = torch.as_tensor(rec).cuda()
+    ac2, n = ctx.decode_counts(d, p.n_ind, sel, po, sample_ploidy=pl)
+    wa, wn = oracle.decode_counts_pa(rec, sel, po, pl)
+    P = len(po) - 1
+    assert np.array_equal(ac2, wa.reshape(-1, P).T) and np.array_equal(n, wn.reshape(-1, P).T)
+
+
+@pytest.mark.parametrize("detect", [True, False])
+def test_decode_af_canonical_bitexact(ctx, uneven, detect):
+    p, sel, po, _, _ = uneven
+    canon, obpr = oracle.transpose_pa_to_canonical(p.records_numpy()[:5000], sel)
+    got = ctx.decode_af(canon, obpr, 5000, po, ploidy=2, detect=detect)
+    want = oracle.decode_af_canonical(canon, obpr, 5000, po, ploidy=2, detect=detect)
+    for g, w in zip(got, want):
+        assert np.array_equal(g, w)
+
+
+# ---- f2 ------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("mode", MODES)
+def test_f2_c1_vs_oracle(ctx, c1, mode):
+    p, sel, po, want, pl = c1
+    got = ctx.extract_blocks(p.records_numpy(), p.n_ind, sel, po, p.block_id, p.n_block, precision=mode)
+    assert_f2_close(got, want, mode)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_f2_uneven_vs_oracle(ctx, uneven, mode):
+    p, sel, po, want, pl = uneven
+    got, used = ctx.extract_blocks(p.records_numpy(), p.n_ind, sel, po, p.block_id, p.n_block, precision=mode,
+                                   return_ploidy=True)
+    assert np.array_equal(used, pl)
+    assert_f2_close(got, want, mode)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_f2_from_qvn_vs_oracle(ctx, c1, mode):
+    p, sel, po, want, pl = c1
+    ac2, n = oracle.decode_counts_pa(p.records_numpy(), sel, po, pl)
+    q, v, nd = oracle.counts_to_qvn(ac2, n)
+    got = ctx.f2_from_qvn(q, v, nd, p.n_pop, p.block_id, p.n_block, precision=mode)
+    assert_f2_close(got, want, mode)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("P", [1, 2, 7, 65, 130])
+def test_f2_odd_population_counts(ctx, mode, P):
+    p = synth.generate("c4", seed=100 + P, n_snp=6000, n_pop=P)
+    sel, po = p.selection()
+    want, _ = oracle_f2(p, sel, po)
+    got = ctx.extract_blocks(p.records_numpy(), p.n_ind, sel, po, p.block_id, p.n_block, precision=mode)
+    assert_f2_close(got, want, mode)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_f2_edge_blocks_and_missing(ctx, mode):
+    """Blocks of one SNP, an empty block id, and a population whose samples are all
+    missing in one block (vpair = 0 -> f2 = 0)."""
+    p = synth.generate("c1", seed=9, n_snp=3000, n_pop=5)
+    rec = p.records_numpy().copy()
+    sel, po = p.selection()
+    # population 2 entirely missing in SNPs [100, 400)
+    for g in sel[po[2]:po[3]]:
+        rec[100:400, g // 4] |= np.uint8(3 << (6 - 2 * (g % 4)))
+    bid = np.zeros(3000, np.int32)
+    bid[1:2] = 1            # block 1: one SNP
+    bid[2:100] = 2
+    bid[100:400] = 4        # block 3 left empty
+    bid[400:] = 5
+    nb = 6
+    pl = oracle.detect_ploidy_pa(rec, sel)
+    f2, vp, bs = oracle.f2_from_panel(rec, sel, po, bid, nb, pl)
+    want = F2Tensor(f2, vp, bs, 5, nb)
+    got = ctx.extract_blocks(rec, p.n_ind, sel, po, bid, nb, precision=mode)
+    assert list(got.block_sizes) == [1, 1, 98, 0, 300, 2600]
+    assert not got.f2[25 * 3:25 * 4].any() and not got.vpair[25 * 3:25 * 4].any()
+    assert got.vpair[2 + 5 * 0 + 25 * 4] == 0.0 and got.f2[2 + 5 * 0 + 25 * 4] == 0.0
+    assert_f2_close(got, want, mode)
+
+
+def test_f2_deterministic(ctx, c1):
+    p, sel, po, _, _ = c1
+    a = ctx.extract_blocks(p.records_numpy(), p.n_ind, sel, po, p.block_id, p.n_block, precision=MODES[-1])
+    b = ctx.extract_blocks(p.records_numpy(), p.n_ind, sel, po, p.block_id, p.n_block, precision=MODES[-1])
+    assert np.array_equal(a.f2, b.f2) and np.array_equal(a.vpair, b.vpair)
+
+
+def test_degenerate_requests(ctx):
+    p = synth.generate("c1", seed=1, n_snp=500, n_pop=3)
+    sel, po = p.selection()
+    t = ctx.extract_blocks(p.records_numpy(), p.n_ind, sel, po, p.block_id, 0)
+    assert t.f2.size == 0
+    z = ctx.extract_blocks(p.records_numpy()[:0], p.n_ind, sel, po, np.zeros(0, np.int32), 2)
+    assert z.f2.shape == (18,) and not z.f2.any() and not z.vpair.any() and list(z.block_sizes) == [0, 0]
+
+
+def test_malformed_partition_is_an_error(ctx):
+    p = synth.generate("c1", seed=1, n_snp=500, n_pop=3)
+    sel, po = p.selection()
+    bad = p.block_id.copy()
+    bad[10] = bad[-1] + 5
+    with pytest.raises(StpError, match="runtime_error"):
+        ctx.extract_blocks(p.records_numpy(), p.n_ind, sel, po, bad, p.n_block)
+    with pytest.raises(StpError, match="invalid_argument"):
+        ctx.extract_blocks(p.records_numpy(), p.n_ind, np.array([p.n_ind + 3]), [0, 1], p.block_id, p.n_block)
+
+
+def test_plan_device_resident_matches_one_shot(ctx, c1):
+    import torch
+
+    p, sel, po, want, _ = c1
+    rec = torch.as_tensor(p.records_numpy()).cuda()
+    plan = ctx.plan(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision=MODES[-1])
+    n = p.n_pop ** 2 * p.n_block
+    f2 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    vp = torch.zeros_like(f2)
+    for _ in range(2):
+        plan.run(rec, f2, vp, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    one = ctx.extract_blocks(p.records_numpy(), p.n_ind, sel, po, p.block_id, p.n_block, precision=MODES[-1])
+    assert np.array_equal(f2.cpu().numpy(), one.f2) and np.array_equal(vp.cpu().numpy(), one.vpair)
+    assert plan.launches >= 2
+
+
+def test_jackknife_vs_oracle(ctx, c1):
+    _, _, _, want, _ = c1
+    m = want.P * want.P
+    est, var = ctx.jackknife(want.f2, want.block_sizes, m, want.n_block)
+    e2, v2 = oracle.block_jackknife(want.f2, want.block_sizes, m, want.n_block)
+    np.testing.assert_allclose(est, e2, rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(var, v2, rtol=1e-9, atol=1e-18)
+
+
+def test_extract_f2_files_roundtrip(tmp_path, c1):
+    p, sel, po, want, pl = c1
+    write_eigenstrat(p, tmp_path / "panel")
+    pops = list(reversed(p.pop_labels))  # P axis is sorted by label regardless of the order given
+    out = extract_f2(tmp_path / "panel", pops=pops, out=str(tmp_path / "f2dir"), maxmiss=1.0,
+                     precision=MODES[-1])
+    h = read_f2(out)
+    assert h.pops == sorted(p.pop_labels) and h.P == p.n_pop and h.n_block == p.n_block
+    assert_f2_close(h.tensor, want, MODES[-1])
+    h2 = extract_f2(tmp_path / "panel", pops=pops, maxmiss=1.0, precision=MODES[-1])
+    assert np.array_equal(h2.to_numpy(), h.to_numpy())
