@@ -105,7 +105,7 @@ def make_panel(workload: str, rank: int, device: str, n_snp: int | None = None):
     return synth.generate(workload, seed=20261203 + 1000 * rank, device=device, n_snp=n_snp)
 
 
-def cpu_sample(workload: str, threads: int, seed_rank: int = 0):
+def cpu_sample(workload: str, threads: int, seed_rank: int = 0, gen_device: str = "cpu"):
     """Bounded CPU sample: `threads` blocks of the workload's panel model (one per thread),
     decoded and reduced by the CPU implementation. Returns (units, seconds, kind, desc)."""
     import numpy as np
@@ -116,7 +116,7 @@ def cpu_sample(workload: str, threads: int, seed_rank: int = 0):
     wl = synth.WORKLOADS[workload]
     per_block = max(1, wl.n_snp // 700)
     n_snp = per_block * threads
-    p = synth.generate(workload, seed=20261203 + 17 + seed_rank, device="cpu", n_snp=n_snp)
+    p = synth.generate(workload, seed=20261203 + 17 + seed_rank, device=gen_device, n_snp=n_snp)
     sel, po = p.selection()
     rec = p.records_numpy()
     bid = np.minimum(np.arange(n_snp) // per_block, threads - 1).astype(np.int32)
@@ -164,7 +164,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
-    ap.add_argument("--precision", default="split_bf16")
+    ap.add_argument("--precision", default="split_f16")
+    ap.add_argument("--also", default="split_bf16", help="another tensor-core arithmetic timed beside the headline")
     ap.add_argument("--compare-simt", action="store_true", default=True)
     ap.add_argument("--no-compare-simt", dest="compare_simt", action="store_false")
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -203,11 +204,19 @@ def main():
     sel, po = panel.selection()
     P, M, B = panel.n_pop, panel.n_snp, panel.n_block
     ctx = sb.Context(local)
-    rec = panel.records  # device-resident [M, bpr] uint8
+    # Device-resident records at a 16-byte pitch (128-bit loads); bytes_per_record stays bpr.
+    bpr = panel.bytes_per_record
+    pitch = (bpr + 15) // 16 * 16
+    rec = torch.zeros((M, pitch), dtype=torch.uint8, device=dev)
+    rec[:, :bpr] = panel.records
+    panel.records = None
     n_out = P * P * B
     f2 = torch.empty(n_out, dtype=torch.float64, device=dev)
     vp = torch.empty_like(f2)
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: the library and the CUDA events must see the same stream handle
+    # (torch's legacy default stream has handle 0, which the C ABI reads as "context stream").
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     plan = ctx.plan(rec, panel.n_ind, sel, po, panel.block_id, B, precision=args.precision)
 
     def timed(pl, steps, warm):
@@ -240,19 +249,25 @@ def main():
         ms = float(t.item())
     value = units(P, M) * world / (ms / 1000.0)
 
-    # Plain FP32 SIMT form on the same panel (the comparison arithmetic).
-    simt = None
+    # The other arithmetics on the same panel: the plain FP32 SIMT form (the comparison the
+    # metric names) and the other tensor-core split.
+    others = {}
+    extra = []
     if args.compare_simt and args.precision != "fp32":
-        plan_s = ctx.plan(rec, panel.n_ind, sel, po, panel.block_id, B, precision="fp32")
+        extra.append("fp32")
+    if args.also and args.also != args.precision:
+        extra.append(args.also)
+    for prec in extra:
+        plan_s = ctx.plan(rec, panel.n_ind, sel, po, panel.block_id, B, precision=prec)
         s_steps = max(1, min(args.steps, 3))
         ms_s, dec_s, con_s, _ = timed(plan_s, s_steps, 1)
-        simt = {"value": units(P, M) / (ms_s / 1000.0), "ms_per_step": ms_s, "contract_ms": con_s,
-                "decode_ms": dec_s}
+        others[prec] = {"value": units(P, M) * world / (ms_s / 1000.0), "ms_per_step": ms_s,
+                        "contract_ms": con_s, "decode_ms": dec_s}
         plan_s.close()
 
     # End to end through the C ABI with pinned host buffers.
-    rec_h = torch.empty(rec.shape, dtype=torch.uint8, pin_memory=True)
-    rec_h.copy_(rec)
+    rec_h = torch.empty((M, bpr), dtype=torch.uint8, pin_memory=True)
+    rec_h.copy_(rec[:, :bpr])
     f2_h = torch.empty(n_out, dtype=torch.float64, pin_memory=True)
     vp_h = torch.empty(n_out, dtype=torch.float64, pin_memory=True)
     rec_np, f2_np, vp_np = rec_h.numpy(), f2_h.numpy(), vp_h.numpy()
@@ -269,7 +284,7 @@ def main():
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = {"value": units(P, M) * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(rec.numel()),
+    e2e = {"value": units(P, M) * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(rec_h.numel()),
            "d2h_bytes_per_step": int(2 * n_out * 8), "ms_per_step": 1000.0 * e2e_s, "steps": e2e_steps}
 
     # Roofline of the dominant kernel (the contraction): algorithmic flops per launch =
@@ -281,12 +296,12 @@ def main():
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
                 "kernel_ms": con_ms, "decode_ms": dec_ms,
-                "decode_hbm_gbs": (M * panel.bytes_per_record + 11 * P * M) / (dec_ms / 1000.0) / 1e9}
+                "decode_hbm_gbs": (M * bpr + 11 * P * M) / (dec_ms / 1000.0) / 1e9}
 
     cpu = None
     if rank == 0 and world == 1:
         threads = args.cpu_threads or (os.cpu_count() or 1)
-        u, t, kind, desc = cpu_sample(args.workload, threads)
+        u, t, kind, desc = cpu_sample(args.workload, threads, gen_device=dev)
         cpu = {"value": u / t, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc}
 
     if rank == 0:
@@ -300,7 +315,7 @@ def main():
                        "parallelism": f"block-sharded x{world}" if world > 1 else "1 GPU"},
             "gpu_launches": int(launches), "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
-            "plain_fp32_simt": simt,
+            "other_arithmetics": others,
         }
         print(json.dumps(line), flush=True)
     plan.close()

@@ -25,7 +25,7 @@ PRECISIONS = {
     "f16x3": L.PREC_SPLIT_F16, "split_f16": L.PREC_SPLIT_F16, "fp16": L.PREC_SPLIT_F16,
 }
 PRECISION_TAGS = {L.PREC_FP32_SIMT: "fp32_simt", L.PREC_SPLIT_BF16: "split_bf16", L.PREC_SPLIT_F16: "split_f16"}
-DEFAULT_PRECISION = "split_bf16"
+DEFAULT_PRECISION = "split_f16"
 
 PLOIDY = {"auto": L.PLOIDY_AUTO, "1": L.PLOIDY_PSEUDO, "pseudo": L.PLOIDY_PSEUDO,
           "pseudo_haploid": L.PLOIDY_PSEUDO, "2": L.PLOIDY_DIPLOID, "diploid": L.PLOIDY_DIPLOID}

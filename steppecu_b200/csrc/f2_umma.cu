@@ -1,17 +1,562 @@
-// steppecu_b200/csrc/f2_umma.cu — placeholder until the tcgen05 contraction lands.
+// steppecu_b200/csrc/f2_umma.cu
+//
+// The tensor-core f2 contraction for sm_100a: one persistent, warp-specialised kernel
+// over every (jackknife block, 128x128 population tile pair ti <= tj) work item.
+//
+//   warp 0      TMA producer: per 32-SNP stage, 5 split planes (Pt_hi, Pt_lo, Ah_hi, Ah_lo,
+//               M as 16-bit) + the int8 M plane for the row tile and the column tile
+//               (one side only on diagonal tiles), 64B/32B-swizzled, no multicast.
+//   warp 1      TMEM owner + single-thread tcgen05.mma issuer. Per 16-SNP K step, seven
+//               kind::f16 MMAs accumulate num/2 = sum(Ah_i M_j + M_i Ah_j - Pt_i Pt_j) over
+//               the hi/lo splits (the -Pt Pt products use the descriptor's A-negate bit)
+//               into an FP32 TMEM buffer; one kind::i8 MMA per stage accumulates the exact
+//               both-present count M M^T into an int32 TMEM buffer.
+//   warps 2-9   epilogue: every 32 SNPs, drain the FP32 buffer into FP64 registers
+//               (double-buffered TMEM, so the MMAs run on); at the end of the block, read
+//               vpair, form f2 = num / vpair (0 when vpair = 0, f2_estimator.hpp:42-46) in
+//               FP64 and store (i,j) and (j,i) of the block's slab.
+//
+// TMEM (512 columns): [0,128) and [128,256) FP32 numerator chunks, [256,384) and
+// [384,512) int32 vpair per tile. Every wait is bounded (a few seconds); on expiry the
+// kernel raises an error flag the host turns into STP_DEVICE_TIMEOUT, lets its copies and
+// MMAs finish, frees TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <memory>
+
 #include "stpf2_internal.cuh"
 
 namespace stpf2 {
 
-struct UmmaPlan {};
+namespace {
 
-UmmaPlan* umma_plan_create(Ctx&, const OperandPlanes&, const BlockLayout&) {
-    fail(STP_INVALID_CONFIG, "tcgen05 contraction not built");
+constexpr int kTile = 128;
+constexpr int kStageK = 32;        // SNP columns per pipeline stage
+constexpr int kStages = 2;
+constexpr int kDrainStages = 1;    // FP32 TMEM chunk = 32 SNPs, then FP64
+constexpr int kPlanes = 5;
+constexpr uint32_t kTile16 = kTile * kStageK * 2;                 // 8 KiB
+constexpr uint32_t kTile8 = kTile * kStageK;                      // 4 KiB
+constexpr uint32_t kSideBytes = kPlanes * kTile16 + kTile8;       // 44 KiB
+constexpr uint32_t kStageBytes = 2 * kSideBytes;                  // 88 KiB
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;
+constexpr uint32_t kTmemCols = 512;
+constexpr unsigned long long kTimeoutNs = 4000000000ull;
+
+struct UmmaArgs {
+    const WorkItem* items;
+    int n_items;
+    const BlockInfo* blocks;
+    int P;
+    double* f2;
+    double* vpair;
+    double num_scale;  // 2 * plane scale undo
+    int* err;
+    uint32_t idesc_pp, idesc_am, idesc_i8;
+};
+
+struct SmemCtl {
+    unsigned long long full[kStages], empty[kStages];
+    unsigned long long acc_full[2], acc_empty[2];
+    unsigned long long vp_full[2], vp_empty[2];
+    unsigned long long drain;
+    uint32_t tmem_base;
+    volatile int abort;
+};
+
+// ---- PTX wrappers ---------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(b))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, uint32_t bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
+                     smem_u32(b)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false on timeout (which also raises the CTA's abort flag and the global
+// error flag) or when another role of this CTA has already aborted.
+__device__ __noinline__ bool wait_bounded(unsigned long long* b, uint32_t parity, SmemCtl* ctl, int* err,
+                                          bool honour_abort = true) {
+    if (mbar_try_wait(b, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try_wait(b, parity)) return true;
+        if ((it & 63u) == 0) {
+            if (honour_abort && ctl->abort) return false;
+            if (globaltimer() - t0 > kTimeoutNs) {
+                ctl->abort = 1;
+                atomicExch(err, 1);
+                return false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, int x, int y, int z,
+                                            unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, int x, int y, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_f16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(unsigned long long* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// 32 lanes x 32 consecutive 32-bit TMEM columns -> 32 registers per thread.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// UMMA shared-memory descriptor, K-major, swizzled: start address, LBO (unused for a
+// single swizzle atom along K, encoded 1), SBO = byte distance between 8-row groups,
+// descriptor version 1 (sm_100), layout type (4 = 64B swizzle, 6 = 32B swizzle).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo_bytes, uint64_t layout) {
+    return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (1ull << 16) |
+           (static_cast<uint64_t>(sbo_bytes >> 4) << 32) | (1ull << 46) | (layout << 61);
+}
+
+// ---- roles -------------------------------------------------------------------------------
+
+__device__ __forceinline__ int stages_of(int k) { return (k + kStageK - 1) / kStageK; }
+
+__device__ void producer(const CUtensorMap* tm16, const CUtensorMap* tm8, const UmmaArgs& a, uint8_t* smem,
+                         SmemCtl* ctl) {
+    uint32_t g = 0;
+    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
+        const WorkItem w = a.items[it];
+        const BlockInfo bi = a.blocks[w.blk];
+        const int nst = stages_of(bi.k);
+        const bool diag = w.ti == w.tj;
+        for (int st = 0; st < nst; ++st, ++g) {
+            const int slot = static_cast<int>(g % kStages);
+            const uint32_t ph = (g / kStages) & 1u;
+            if (!wait_bounded(&ctl->empty[slot], ph ^ 1u, ctl, a.err)) goto abort;
+            {
+                uint8_t* sb = smem + slot * kStageBytes;
+                mbar_expect_tx(&ctl->full[slot], diag ? kSideBytes : kStageBytes);
+                const int x = static_cast<int>(bi.col) + st * kStageK;
+                const int ya = w.ti * kTile, yb = w.tj * kTile;
+                for (int p = 0; p < kPlanes; ++p) tma_load_3d(sb + p * kTile16, tm16, x, ya, p, &ctl->full[slot]);
+                tma_load_2d(sb + kPlanes * kTile16, tm8, x, ya, &ctl->full[slot]);
+                if (!diag) {
+                    uint8_t* sbb = sb + kSideBytes;
+                    for (int p = 0; p < kPlanes; ++p) tma_load_3d(sbb + p * kTile16, tm16, x, yb, p, &ctl->full[slot]);
+                    tma_load_2d(sbb + kPlanes * kTile16, tm8, x, yb, &ctl->full[slot]);
+                }
+            }
+        }
+    }
+    return;
+abort:
+    // Let the copies already issued land before the CTA's shared memory goes away.
+    for (uint32_t k = (g >= kStages ? g - kStages : 0); k < g; ++k)
+        wait_bounded(&ctl->full[k % kStages], (k / kStages) & 1u, ctl, a.err, false);
+}
+
+__device__ void mma_issuer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl, uint32_t tmem) {
+    uint32_t g = 0, cs = 0, is = 0;
+    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
+        const WorkItem w = a.items[it];
+        const BlockInfo bi = a.blocks[w.blk];
+        const int nst = stages_of(bi.k);
+        if (nst == 0) continue;
+        const bool diag = w.ti == w.tj;
+        const int vb = static_cast<int>(is & 1u);
+        if (!wait_bounded(&ctl->vp_empty[vb], ((is >> 1) & 1u) ^ 1u, ctl, a.err)) goto done;
+        tc_fence_after();
+        {
+            const uint32_t d_vp = tmem + 256u + static_cast<uint32_t>(vb) * 128u;
+            uint32_t d_num = tmem;
+            int nb = 0;
+            for (int st = 0; st < nst; ++st, ++g) {
+                if (st % kDrainStages == 0) {
+                    nb = static_cast<int>(cs & 1u);
+                    if (!wait_bounded(&ctl->acc_empty[nb], ((cs >> 1) & 1u) ^ 1u, ctl, a.err)) goto done;
+                    tc_fence_after();
+                    d_num = tmem + static_cast<uint32_t>(nb) * 128u;
+                }
+                const int slot = static_cast<int>(g % kStages);
+                if (!wait_bounded(&ctl->full[slot], (g / kStages) & 1u, ctl, a.err)) goto done;
+                tc_fence_after();
+                const uint32_t sa = smem_u32(smem + slot * kStageBytes);
+                const uint32_t sb = diag ? sa : sa + kSideBytes;
+#pragma unroll
+                for (int k = 0; k < kStageK / 16; ++k) {
+                    const uint32_t ko = static_cast<uint32_t>(k) * 32u;  // 16 elements x 2 bytes
+                    const uint64_t aPh = smem_desc(sa + 0 * kTile16 + ko, 512, 4);
+                    const uint64_t aPl = smem_desc(sa + 1 * kTile16 + ko, 512, 4);
+                    const uint64_t aAh = smem_desc(sa + 2 * kTile16 + ko, 512, 4);
+                    const uint64_t aAl = smem_desc(sa + 3 * kTile16 + ko, 512, 4);
+                    const uint64_t aM = smem_desc(sa + 4 * kTile16 + ko, 512, 4);
+                    const uint64_t bPh = smem_desc(sb + 0 * kTile16 + ko, 512, 4);
+                    const uint64_t bPl = smem_desc(sb + 1 * kTile16 + ko, 512, 4);
+                    const uint64_t bAh = smem_desc(sb + 2 * kTile16 + ko, 512, 4);
+                    const uint64_t bAl = smem_desc(sb + 3 * kTile16 + ko, 512, 4);
+                    const uint64_t bM = smem_desc(sb + 4 * kTile16 + ko, 512, 4);
+                    const uint32_t first = (st % kDrainStages == 0 && k == 0) ? 0u : 1u;
+                    // Large terms first and interleaved in sign, the lo corrections last.
+                    mma_f16(d_num, aAh, bM, a.idesc_am, first);
+                    mma_f16(d_num, aPh, bPh, a.idesc_pp, 1u);
+                    mma_f16(d_num, aM, bAh, a.idesc_am, 1u);
+                    mma_f16(d_num, aPh, bPl, a.idesc_pp, 1u);
+                    mma_f16(d_num, aPl, bPh, a.idesc_pp, 1u);
+                    mma_f16(d_num, aAl, bM, a.idesc_am, 1u);
+                    mma_f16(d_num, aM, bAl, a.idesc_am, 1u);
+                }
+                mma_i8(d_vp, smem_desc(sa + kPlanes * kTile16, 256, 6), smem_desc(sb + kPlanes * kTile16, 256, 6),
+                       a.idesc_i8, st > 0 ? 1u : 0u);
+                mma_commit(&ctl->empty[slot]);
+                if (st % kDrainStages == kDrainStages - 1 || st == nst - 1) {
+                    mma_commit(&ctl->acc_full[nb]);
+                    ++cs;
+                }
+            }
+            mma_commit(&ctl->vp_full[vb]);
+            ++is;
+        }
+    }
+done:
+    // Every MMA this thread issued completes before TMEM is released.
+    mma_commit(&ctl->drain);
+    wait_bounded(&ctl->drain, 0u, ctl, a.err, false);
+}
+
+__device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int warp, int lane) {
+    const int e = warp - 2;
+    const int q = warp & 3;                 // TMEM lane quarter this warp may access
+    const int h = e >> 2;                   // column half of the tile
+    const int r = q * 32 + lane;            // tile row (TMEM lane)
+    const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
+    const int P = a.P;
+    uint32_t cs = 0, is = 0;
+    double acc[64];
+    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
+        const WorkItem w = a.items[it];
+        const BlockInfo bi = a.blocks[w.blk];
+        const int nst = stages_of(bi.k);
+        const bool diag = w.ti == w.tj;
+        const int i = w.ti * kTile + r;
+        const int j0 = w.tj * kTile + h * 64;
+        const int64_t slab = static_cast<int64_t>(P) * P * bi.b;
+        if (nst == 0) {  // an empty block id: zeros (cpu_backend.cpp:234)
+            if (i < P)
+                for (int c = 0; c < 64; ++c) {
+                    const int j = j0 + c;
+                    if (j >= P || (diag && j < i)) continue;
+                    a.f2[slab + i + static_cast<int64_t>(P) * j] = 0.0;
+                    a.vpair[slab + i + static_cast<int64_t>(P) * j] = 0.0;
+                    a.f2[slab + j + static_cast<int64_t>(P) * i] = 0.0;
+                    a.vpair[slab + j + static_cast<int64_t>(P) * i] = 0.0;
+                }
+            continue;
+        }
+#pragma unroll
+        for (int c = 0; c < 64; ++c) acc[c] = 0.0;
+        const int nch = (nst + kDrainStages - 1) / kDrainStages;
+        for (int ch = 0; ch < nch; ++ch) {
+            const int nb = static_cast<int>(cs & 1u);
+            bool ok = true;
+            if (lane == 0) ok = wait_bounded(&ctl->acc_full[nb], (cs >> 1) & 1u, ctl, a.err);
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) return;
+            tc_fence_after();
+            uint32_t v[32];
+            const uint32_t base = tmem + lane_addr + static_cast<uint32_t>(nb) * 128u + static_cast<uint32_t>(h) * 64u;
+            tmem_ld32(base, v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 32; ++c) acc[c] += static_cast<double>(__uint_as_float(v[c]));
+            tmem_ld32(base + 32u, v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 32; ++c) acc[32 + c] += static_cast<double>(__uint_as_float(v[c]));
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&ctl->acc_empty[nb]);
+            ++cs;
+        }
+        const int vb = static_cast<int>(is & 1u);
+        {
+            bool ok = true;
+            if (lane == 0) ok = wait_bounded(&ctl->vp_full[vb], (is >> 1) & 1u, ctl, a.err);
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) return;
+        }
+        tc_fence_after();
+        const uint32_t vbase = tmem + lane_addr + 256u + static_cast<uint32_t>(vb) * 128u + static_cast<uint32_t>(h) * 64u;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            uint32_t v[32];
+            tmem_ld32(vbase + static_cast<uint32_t>(half) * 32u, v);
+            tmem_wait_ld();
+            if (half == 1) {
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&ctl->vp_empty[vb]);
+            }
+            if (i < P) {
+                // Fully unrolled so acc[] stays in registers.
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {
+                    const int j = j0 + half * 32 + c;
+                    if (j < P && !(diag && j < i)) {
+                        const double vp = static_cast<double>(static_cast<int32_t>(v[c]));
+                        const double f = (vp > 0.0) ? (acc[half * 32 + c] * a.num_scale) / vp : 0.0;
+                        const int64_t ij = slab + i + static_cast<int64_t>(P) * j;
+                        const int64_t ji = slab + j + static_cast<int64_t>(P) * i;
+                        a.f2[ij] = f;
+                        a.vpair[ij] = vp;
+                        a.f2[ji] = f;
+                        a.vpair[ji] = vp;
+                    }
+                }
+            }
+        }
+        ++is;
+    }
+}
+
+__global__ void __maxnreg__(168)
+f2_umma_kernel(const __grid_constant__ CUtensorMap tm16, const __grid_constant__ CUtensorMap tm8, UmmaArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    SmemCtl* ctl = reinterpret_cast<SmemCtl*>(smem + kStages * kStageBytes);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&ctl->full[s], 1);
+            mbar_init(&ctl->empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&ctl->acc_full[b], 1);
+            mbar_init(&ctl->acc_empty[b], kEpiWarps);
+            mbar_init(&ctl->vp_full[b], 1);
+            mbar_init(&ctl->vp_empty[b], kEpiWarps);
+        }
+        mbar_init(&ctl->drain, 1);
+        ctl->abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&ctl->tmem_base)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = ctl->tmem_base;
+
+    if (warp == 0) {
+        if (lane == 0) producer(&tm16, &tm8, a, smem, ctl);
+    } else if (warp == 1) {
+        if (lane == 0) mma_issuer(a, smem, ctl, tmem);
+    } else {
+        epilogue(a, ctl, tmem, warp, lane);
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+// Instruction descriptors (kind::f16 / kind::i8): D format, A/B formats, A negate,
+// K-major A and B, N >> 3 at bit 17, M >> 4 at bit 24.
+uint32_t idesc_f16(bool bf16, bool negate_a) {
+    const uint32_t fmt = bf16 ? 1u : 0u;
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((negate_a ? 1u : 0u) << 13) | ((kTile >> 3) << 17) |
+           ((kTile >> 4) << 24);
+}
+uint32_t idesc_u8_s32() { return (2u << 4) | (0u << 7) | (0u << 10) | ((kTile >> 3) << 17) | ((kTile >> 4) << 24); }
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q{};
+        void* p = nullptr;
+        STPF2_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) fail(STP_CUDA_ERROR, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+constexpr size_t kSmemBytes = kStages * kStageBytes + sizeof(SmemCtl) + 1024;
+
+}  // namespace
+
+struct UmmaPlan {
+    CUtensorMap tm16{}, tm8{};
+    DevBuf items, blocks, err;
+    int n_items = 0;
+    int P = 0;
+    OpFmt fmt = OpFmt::BF16;
+    double num_scale = 2.0;
+};
+
+int umma_tile() { return kTile; }
+
+UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L) {
+    if (op.fmt == OpFmt::F32) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs split 16-bit planes");
+    auto p = std::make_unique<UmmaPlan>();
+    p->P = op.P;
+    p->fmt = op.fmt;
+    p->num_scale = 2.0 * op.scale_inv;
+    const std::vector<WorkItem> items = make_work_items(L, op.P, kTile);
+    p->n_items = static_cast<int>(items.size());
+    p->items.reserve(std::max<size_t>(items.size() * sizeof(WorkItem), 16));
+    p->blocks.reserve(std::max<size_t>(L.blocks.size() * sizeof(BlockInfo), 16));
+    p->err.reserve(16);
+    STPF2_CUDA(cudaMemcpyAsync(p->items.ptr, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
+                               c.stream));
+    STPF2_CUDA(cudaMemcpyAsync(p->blocks.ptr, L.blocks.data(), L.blocks.size() * sizeof(BlockInfo),
+                               cudaMemcpyHostToDevice, c.stream));
+    STPF2_CUDA(cudaMemsetAsync(p->err.ptr, 0, 16, c.stream));
+
+    auto enc = tensor_map_encoder();
+    const cuuint64_t ld = static_cast<cuuint64_t>(op.ld), P = static_cast<cuuint64_t>(op.P);
+    {
+        const cuuint64_t dims[3] = {ld, P, kPlanes};
+        const cuuint64_t strides[2] = {ld * 2, ld * P * 2};
+        const cuuint32_t box[3] = {kStageK, kTile, 1};
+        const cuuint32_t es[3] = {1, 1, 1};
+        const CUresult r = enc(&p->tm16, op.fmt == OpFmt::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
+                               3, op.planes, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                               CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) fail(STP_CUDA_ERROR, "cuTensorMapEncodeTiled (16-bit planes) failed: " + std::to_string(r));
+    }
+    {
+        const cuuint64_t dims[2] = {ld, P};
+        const cuuint64_t strides[1] = {ld};
+        const cuuint32_t box[2] = {kStageK, kTile};
+        const cuuint32_t es[2] = {1, 1};
+        const CUresult r = enc(&p->tm8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, op.m_u8, dims, strides, box, es,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) fail(STP_CUDA_ERROR, "cuTensorMapEncodeTiled (int8 plane) failed: " + std::to_string(r));
+    }
+    STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(kSmemBytes)));
+    return p.release();
+}
+
 void umma_plan_destroy(UmmaPlan* p) { delete p; }
-void launch_f2_umma(Ctx&, UmmaPlan*, double*, double*, cudaStream_t) {
-    fail(STP_INVALID_CONFIG, "tcgen05 contraction not built");
+
+void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s) {
+    if (!p || p->n_items <= 0) return;
+    UmmaArgs a{};
+    a.items = p->items.as<WorkItem>();
+    a.n_items = p->n_items;
+    a.blocks = p->blocks.as<BlockInfo>();
+    a.P = p->P;
+    a.f2 = f2;
+    a.vpair = vpair;
+    a.num_scale = p->num_scale;
+    a.err = p->err.as<int>();
+    const bool bf16 = p->fmt == OpFmt::BF16;
+    a.idesc_pp = idesc_f16(bf16, true);
+    a.idesc_am = idesc_f16(bf16, false);
+    a.idesc_i8 = idesc_u8_s32();
+    const int grid = std::min(c.sm_count, p->n_items);
+    f2_umma_kernel<<<grid, kThreads, kSmemBytes, s>>>(p->tm16, p->tm8, a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cudaFuncAttributes fa{};
+        cudaFuncGetAttributes(&fa, f2_umma_kernel);
+        fail(STP_CUDA_ERROR, std::string("f2_umma_kernel launch: ") + cudaGetErrorString(e) + " (regs " +
+                                 std::to_string(fa.numRegs) + ", max threads " + std::to_string(fa.maxThreadsPerBlock) +
+                                 ", dyn smem " + std::to_string(kSmemBytes) + ", max dyn smem " +
+                                 std::to_string(fa.maxDynamicSharedSizeBytes) + ", local " +
+                                 std::to_string(fa.localSizeBytes) + ")");
+    }
+    c.launches++;
 }
-int umma_tile() { return 128; }
+
+// Reads (and clears) the kernel's timeout flag; call after the stream has synchronised.
+void umma_check(UmmaPlan* p) {
+    if (!p) return;
+    int e = 0;
+    STPF2_CUDA(cudaMemcpy(&e, p->err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        STPF2_CUDA(cudaMemset(p->err.ptr, 0, sizeof(int)));
+        fail(STP_DEVICE_TIMEOUT, "tensor-core contraction: a bounded device wait expired; results are invalid");
+    }
+}
 
 }  // namespace stpf2

@@ -328,6 +328,7 @@ void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
         for (size_t g = 0; g < sel.size(); ++g) o.ploidy_out[g] = static_cast<int32_t>(sel[g] & 3u);
     }
     STPF2_CUDA(cudaStreamSynchronize(s));
+    umma_check(p->umma);
 }
 
 }  // namespace
@@ -566,6 +567,12 @@ stp_status stp_f2_from_qvn(stp_ctx* ctx, const double* Q, const double* V, const
                 throw;
             }
             STPF2_CUDA(cudaStreamSynchronize(s));
+            try {
+                umma_check(up);
+            } catch (...) {
+                umma_plan_destroy(up);
+                throw;
+            }
             umma_plan_destroy(up);
         }
         STPF2_CUDA(cudaMemcpyAsync(f2, d_f2.ptr, out_elems * 8, cudaMemcpyDeviceToHost, s));
@@ -670,6 +677,8 @@ stp_status stp_plan_last_times(const stp_plan* plan, float* decode_ms, float* co
             sa += a;
             sb += b;
         }
+        STPF2_CUDA(cudaStreamSynchronize(p.ctx->stream));
+        umma_check(p.umma);
         const double n = p.n_timed ? static_cast<double>(p.n_timed) : 1.0;
         if (decode_ms) *decode_ms = static_cast<float>(sa / n);
         if (contract_ms) *contract_ms = static_cast<float>(sb / n);

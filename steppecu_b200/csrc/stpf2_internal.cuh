@@ -187,6 +187,8 @@ struct UmmaPlan;
 UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L);
 void umma_plan_destroy(UmmaPlan* p);
 void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s);
+// After a stream sync: raises STP_DEVICE_TIMEOUT if the kernel's bounded waits expired.
+void umma_check(UmmaPlan* p);
 int umma_tile();
 
 void launch_jackknife(Ctx& c, const double* x, const int32_t* block_sizes, int64_t m, int nb,

@@ -15,14 +15,17 @@ from steppecu_b200.synth import write_eigenstrat
 
 pytestmark = pytest.mark.gpu
 
-# Per-arithmetic f2 tolerance: (rtol, atol). The numerator is accumulated over <= 64-SNP
-# chunks in FP32 and summed in FP64; see the precision section of the design notes.
+# Per-arithmetic f2 tolerance (rtol, atol) against the FP64 oracle. Every form sums the
+# numerator in FP32 over short SNP chunks and combines chunks in FP64. Split-F16 keeps ~22
+# mantissa bits per operand and FP32 SIMT 24; split-BF16 (hi+lo) keeps only ~16, so its
+# per-element error is ~2^-17 and its tolerance is wider.
 TOL = {
-    "fp32": (2e-5, 2e-7),
-    "split_bf16": (2e-5, 2e-7),
-    "split_f16": (2e-5, 2e-7),
+    "fp32": (5e-6, 5e-8),
+    "split_f16": (5e-6, 2e-7),
+    "split_bf16": (3e-4, 3e-6),
 }
-MODES = ["fp32"]
+MODES = ["fp32", "split_bf16", "split_f16"]
+TC_DEFAULT = "split_f16"
 
 
 def oracle_f2(panel, sel, po, ploidy=None, block_id=None, n_block=None):
