@@ -157,6 +157,35 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def run_e2e(args, ctx, rec, panel, sel, po, bpr, n_out, barrier, dist, dev, P, M, B, world):
+    """End to end through the C ABI with pinned host buffers: H2D of the genotypes,
+    extraction, D2H of the FP64 f2 and vpair tensors, every step."""
+    import torch
+
+    rec_h = torch.empty((M, bpr), dtype=torch.uint8, pin_memory=True)
+    rec_h.copy_(rec[:, :bpr])
+    f2_h = torch.empty(n_out, dtype=torch.float64, pin_memory=True)
+    vp_h = torch.empty(n_out, dtype=torch.float64, pin_memory=True)
+    rec_np, f2_np, vp_np = rec_h.numpy(), f2_h.numpy(), vp_h.numpy()
+    e2e_steps = args.e2e_steps or max(1, min(args.steps, 5))
+    ctx.extract_blocks(rec_np, panel.n_ind, sel, po, panel.block_id, B, precision=args.precision,
+                       out=(f2_np, vp_np))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.extract_blocks(rec_np, panel.n_ind, sel, po, panel.block_id, B, precision=args.precision,
+                           out=(f2_np, vp_np))
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": units(P, M) * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(rec_h.numel()),
+           "d2h_bytes_per_step": int(2 * n_out * 8), "ms_per_step": 1000.0 * e2e_s, "steps": e2e_steps}
+
+    return e2e
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -170,6 +199,8 @@ def main():
     ap.add_argument("--no-compare-simt", dest="compare_simt", action="store_false")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-threads", type=int, default=None)
+    ap.add_argument("--snps", type=int, default=None, help="override the workload's SNP count (smaller cases)")
+    ap.add_argument("--quick", action="store_true", help="headline timing only: no other arithmetics, e2e or CPU leg")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -200,7 +231,7 @@ def main():
             dist.barrier()
 
     dev = f"cuda:{local}"
-    panel = make_panel(args.workload, rank, dev)
+    panel = make_panel(args.workload, rank, dev, n_snp=args.snps)
     sel, po = panel.selection()
     P, M, B = panel.n_pop, panel.n_snp, panel.n_block
     ctx = sb.Context(local)
@@ -253,9 +284,9 @@ def main():
     # metric names) and the other tensor-core split.
     others = {}
     extra = []
-    if args.compare_simt and args.precision != "fp32":
+    if args.compare_simt and args.precision != "fp32" and not args.quick:
         extra.append("fp32")
-    if args.also and args.also != args.precision:
+    if args.also and args.also not in (args.precision, "none") and not args.quick:
         extra.append(args.also)
     for prec in extra:
         plan_s = ctx.plan(rec, panel.n_ind, sel, po, panel.block_id, B, precision=prec)
@@ -265,27 +296,9 @@ def main():
                         "contract_ms": con_s, "decode_ms": dec_s}
         plan_s.close()
 
-    # End to end through the C ABI with pinned host buffers.
-    rec_h = torch.empty((M, bpr), dtype=torch.uint8, pin_memory=True)
-    rec_h.copy_(rec[:, :bpr])
-    f2_h = torch.empty(n_out, dtype=torch.float64, pin_memory=True)
-    vp_h = torch.empty(n_out, dtype=torch.float64, pin_memory=True)
-    rec_np, f2_np, vp_np = rec_h.numpy(), f2_h.numpy(), vp_h.numpy()
-    e2e_steps = args.e2e_steps or max(1, min(args.steps, 5))
-    ctx.extract_blocks(rec_np, panel.n_ind, sel, po, panel.block_id, B, precision=args.precision,
-                       out=(f2_np, vp_np))
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        ctx.extract_blocks(rec_np, panel.n_ind, sel, po, panel.block_id, B, precision=args.precision,
-                           out=(f2_np, vp_np))
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": units(P, M) * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(rec_h.numel()),
-           "d2h_bytes_per_step": int(2 * n_out * 8), "ms_per_step": 1000.0 * e2e_s, "steps": e2e_steps}
+    e2e = None
+    if not args.quick:
+        e2e = run_e2e(args, ctx, rec, panel, sel, po, bpr, n_out, barrier, dist, dev, P, M, B, world)
 
     # Roofline of the dominant kernel (the contraction): algorithmic flops per launch =
     # 3 contractions x 2 * P^2 * M (SNP-padded work excluded) over the measured launch time.
@@ -299,7 +312,7 @@ def main():
                 "decode_hbm_gbs": (M * bpr + 11 * P * M) / (dec_ms / 1000.0) / 1e9}
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.quick:
         threads = args.cpu_threads or (os.cpu_count() or 1)
         u, t, kind, desc = cpu_sample(args.workload, threads, gen_device=dev)
         cpu = {"value": u / t, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc}

@@ -12,14 +12,17 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
+
 #include "stpf2_internal.cuh"
 
 namespace stpf2 {
 
 namespace {
 
-constexpr int kDecSnps = 32;       // SNP records per CTA (one per lane)
-constexpr int kDecThreads = 256;   // 8 warps share the CTA's populations
+constexpr int kTileCols = 32;      // columns per canonical tile (8 bytes per sample)
+constexpr int kTransThreads = 320; // transpose: one thread per 16 samples (looping)
+constexpr int kDecThreads2 = 128;  // decode: one thread per (population, tile)
 constexpr int kPloidyWindow = 1000;  // decode_af.hpp:29 (kPloidyDetectSnps)
 
 // Per-element operand terms of one (pop, SNP) from its exact counts. q matches the
@@ -61,12 +64,13 @@ template <> __device__ __forceinline__ double from16<__half>(__half x) {
 // half's normal range (Pt by 2^7, Ah by 2^14, so every product carries 2^14).
 template <OpFmt F>
 __device__ __forceinline__ void emit(const OperandPlanes& op, int i, int64_t col, const Terms& t) {
-    const int64_t row = static_cast<int64_t>(i) * op.ld + col;
-    const int64_t plane = static_cast<int64_t>(op.P) * op.ld;
     if constexpr (F == OpFmt::F32) {
+        const int64_t row = static_cast<int64_t>(i) * op.ld + col;
+        const int64_t plane = static_cast<int64_t>(op.P) * op.ld;
         float* p = static_cast<float*>(op.planes);
         p[row] = static_cast<float>(t.pt);
         p[plane + row] = static_cast<float>(t.ah);
+        op.m_u8[row] = static_cast<uint8_t>(t.m != 0.0);
     } else {
         using T = typename std::conditional<F == OpFmt::BF16, __nv_bfloat16, __half>::type;
         const double sp = (F == OpFmt::F16) ? double(1 << kF16PtShift) : 1.0;
@@ -76,102 +80,315 @@ __device__ __forceinline__ void emit(const OperandPlanes& op, int i, int64_t col
         const T ptl = to16<T>(pt - from16<T>(pth));
         const T ahh = to16<T>(ah);
         const T ahl = to16<T>(ah - from16<T>(ahh));
-        T* p = static_cast<T*>(op.planes);
-        p[row] = pth;
-        p[plane + row] = ptl;
-        p[2 * plane + row] = ahh;
-        p[3 * plane + row] = ahl;
-        p[4 * plane + row] = to16<T>(t.m);
+        const int64_t tile = static_cast<int64_t>(i / kTileRows) * op.n_ck + col / kTileK;
+        const int r = i % kTileRows, k = static_cast<int>(col % kTileK);
+        uint8_t* b = static_cast<uint8_t*>(op.planes) + tile * kTile16Bytes + tile16_offset(r, k);
+        const int64_t ps = static_cast<int64_t>(op.n_rt) * op.n_ck * kTile16Bytes;
+        *reinterpret_cast<T*>(b) = pth;
+        *reinterpret_cast<T*>(b + ps) = ptl;
+        *reinterpret_cast<T*>(b + 2 * ps) = ahh;
+        *reinterpret_cast<T*>(b + 3 * ps) = ahl;
+        *reinterpret_cast<T*>(b + 4 * ps) = to16<T>(t.m);
+        op.m_u8[tile * kTile8Bytes + tile8_offset(r, k)] = static_cast<uint8_t>(t.m != 0.0);
     }
-    op.m_u8[row] = static_cast<uint8_t>(t.m != 0.0);
 }
 
-// Folds one packed sample descriptor (see pack_sel) against a record byte array.
-__device__ __forceinline__ void fold_sel(const uint8_t* rec, uint32_t e, int& a, int& c) {
-    const uint32_t byte = rec[e >> 5];
-    const int code = static_cast<int>((byte >> ((e >> 2) & 7u)) & 3u);
-    const int pl = static_cast<int>(e & 3u);
-    // decode_af.hpp:58-65: a valid code adds code/(3-ploidy) to ac and ploidy to n;
-    // carried doubled: diploid adds 2*code, pseudo-haploid adds code.
-    const bool valid = (code != 3) && (pl == 1 || pl == 2);
-    a += valid ? (code << (pl - 1)) : 0;
-    c += valid ? pl : 0;
+// Operand terms of 8 consecutive columns of one population, rounded to FP32 (enough for
+// the split planes' ~22 significant bits; the splits then run on packed FP32 conversions).
+struct Terms8 {
+    float pt[8], ah[8];
+    uint32_t mbits;  // bit c: column c called
+};
+
+__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 a, __nv_bfloat16 b) {
+    return static_cast<uint32_t>(__bfloat16_as_ushort(a)) | (static_cast<uint32_t>(__bfloat16_as_ushort(b)) << 16);
+}
+__device__ __forceinline__ uint32_t pack2(__half a, __half b) {
+    return static_cast<uint32_t>(__half_as_ushort(a)) | (static_cast<uint32_t>(__half_as_ushort(b)) << 16);
 }
 
+// hi/lo split of two FP32 values into packed 16-bit pairs (round to nearest each).
 template <OpFmt F>
-__global__ void __launch_bounds__(kDecThreads)
-decode_pa_kernel(PaDecodeArgs a, uint32_t stride_words, int vec16) {
-    extern __shared__ __align__(16) uint32_t s_rec[];
-    __shared__ double s_center[kDecSnps];
-
-    const int64_t s0 = static_cast<int64_t>(blockIdx.x) * kDecSnps;
-    const int64_t rem = a.n_snp - s0;
-    const int nrows = rem < kDecSnps ? static_cast<int>(rem) : kDecSnps;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nwarps = kDecThreads / 32;
-
-    // 1. Stage this CTA's records: 128-bit loads, coalesced along each record. The
-    //    shared row stride is an odd number of words so lanes that read the same byte
-    //    column of 32 different records hit 32 different banks.
-    if (vec16) {
-        const uint32_t cpr = static_cast<uint32_t>(a.pitch / 16);
-        const uint32_t total = static_cast<uint32_t>(nrows) * cpr;
-        for (uint32_t c = threadIdx.x; c < total; c += kDecThreads) {
-            const uint32_t r = c / cpr, k = c - r * cpr;
-            const uint4 v = __ldg(reinterpret_cast<const uint4*>(a.records + (s0 + r) * a.pitch) + k);
-            uint32_t* d = s_rec + r * stride_words + k * 4;
-            d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-        }
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+    if constexpr (F == OpFmt::BF16) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+        const float2 hf = __bfloat1622float2(h);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+        hi = pack2(h.x, h.y);
+        lo = pack2(l.x, l.y);
     } else {
-        uint8_t* sb = reinterpret_cast<uint8_t*>(s_rec);
-        const uint32_t bpr = static_cast<uint32_t>(a.pitch);
-        const uint32_t total = static_cast<uint32_t>(nrows) * bpr;
-        for (uint32_t c = threadIdx.x; c < total; c += kDecThreads) {
-            const uint32_t r = c / bpr, k = c - r * bpr;
-            sb[r * stride_words * 4 + k] = a.records[(s0 + r) * a.pitch + k];
+        const __half2 h = __floats2half2_rn(x0, x1);
+        const float2 hf = __half22float2(h);
+        const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+        hi = pack2(h.x, h.y);
+        lo = pack2(l.x, l.y);
+    }
+}
+
+// Writes 8 consecutive columns (starting at a multiple of 8) of every operand plane with
+// 16-byte stores: row-major FP32 planes, or one 16-byte chunk of each tiled 16-bit image
+// (and 8 bytes of the int8 image). Row i, columns col..col+7.
+template <OpFmt F>
+__device__ __forceinline__ void emit8(const OperandPlanes& op, int i, int64_t col, const Terms8& t) {
+    uint2 mv;
+    mv.x = 0;
+    mv.y = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const uint32_t bit = (t.mbits >> c) & 1u;
+        if (c < 4) mv.x |= bit << (8 * c);
+        else mv.y |= bit << (8 * (c - 4));
+    }
+    if constexpr (F == OpFmt::F32) {
+        const int64_t off = static_cast<int64_t>(i) * op.ld + col;
+        const int64_t plane = static_cast<int64_t>(op.P) * op.ld;
+        float* p = static_cast<float*>(op.planes);
+        *reinterpret_cast<float4*>(p + off) = make_float4(t.pt[0], t.pt[1], t.pt[2], t.pt[3]);
+        *reinterpret_cast<float4*>(p + off + 4) = make_float4(t.pt[4], t.pt[5], t.pt[6], t.pt[7]);
+        *reinterpret_cast<float4*>(p + plane + off) = make_float4(t.ah[0], t.ah[1], t.ah[2], t.ah[3]);
+        *reinterpret_cast<float4*>(p + plane + off + 4) = make_float4(t.ah[4], t.ah[5], t.ah[6], t.ah[7]);
+        *reinterpret_cast<uint2*>(op.m_u8 + off) = mv;
+    } else {
+        const float sp = (F == OpFmt::F16) ? float(1 << kF16PtShift) : 1.0f;
+        const float sa = sp * sp;
+        uint4 ph, pl, ahh, ahl, mm;
+        uint32_t* PH = &ph.x;
+        uint32_t* PL = &pl.x;
+        uint32_t* AH = &ahh.x;
+        uint32_t* AL = &ahl.x;
+        uint32_t* MM = &mm.x;
+#pragma unroll
+        for (int c = 0; c < 8; c += 2) {
+            split2<F>(t.pt[c] * sp, t.pt[c + 1] * sp, PH[c / 2], PL[c / 2]);
+            split2<F>(t.ah[c] * sa, t.ah[c + 1] * sa, AH[c / 2], AL[c / 2]);
+            const uint32_t one = (F == OpFmt::BF16) ? 0x3F80u : 0x3C00u;  // 1.0
+            MM[c / 2] = (((t.mbits >> c) & 1u) ? one : 0u) | ((((t.mbits >> (c + 1)) & 1u) ? one : 0u) << 16);
         }
+        const int r = i % kTileRows, k = static_cast<int>(col % kTileK);
+        const int64_t tile = static_cast<int64_t>(i / kTileRows) * op.n_ck + col / kTileK;
+        const int64_t ps = static_cast<int64_t>(op.n_rt) * op.n_ck * kTile16Bytes;
+        uint8_t* b = static_cast<uint8_t*>(op.planes) + tile * kTile16Bytes + tile16_offset(r, k);
+        *reinterpret_cast<uint4*>(b) = ph;
+        *reinterpret_cast<uint4*>(b + ps) = pl;
+        *reinterpret_cast<uint4*>(b + 2 * ps) = ahh;
+        *reinterpret_cast<uint4*>(b + 3 * ps) = ahl;
+        *reinterpret_cast<uint4*>(b + 4 * ps) = mm;
+        *reinterpret_cast<uint2*>(op.m_u8 + tile * kTile8Bytes + tile8_offset(r, k)) = mv;
+    }
+}
+
+// ---- canonical tile-major genotypes ------------------------------------------------------
+//
+// The decode runs in two passes over an intermediate "canonical" copy of the selected
+// samples' genotypes, laid out in the padded column space of the operand planes:
+// tile t = columns [32t, 32t+32); selected sample g owns the 8 bytes canon[t * n_sel + g],
+// column 32t + 4k + j in byte k at bits (7-2j, 6-2j) (MSB-first, as in the .geno records).
+// Padding columns hold code 3 (missing) and therefore decode to zero operands.
+
+// 4x4 transpose of 2-bit elements packed MSB-first in a 32-bit word (row 0 in the top
+// byte): two block-swap steps.
+__device__ __forceinline__ uint32_t transpose4x4_2bit(uint32_t w) {
+    uint32_t t = (w ^ (w >> 12)) & 0x0000F0F0u;
+    w ^= t ^ (t << 12);
+    t = (w ^ (w >> 6)) & 0x00CC00CCu;
+    w ^= t ^ (t << 6);
+    return w;
+}
+
+// Pass 1: SNP-major records -> canonical tiles (gathering the selected samples), plus the
+// per-column centre c_s = pooled frequency of every called genotype in the record, rounded
+// to 1/256. One CTA per 32-column tile: its (<= 32) records are staged in shared memory
+// with 128-bit loads; each thread transposes 16 samples x 32 SNPs with SWAR 4x4 transposes.
+__global__ void __launch_bounds__(kTransThreads)
+transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t n_ind,
+                    const TileInfo* __restrict__ tiles, const int32_t* __restrict__ pos, int64_t n_sel,
+                    uint64_t* __restrict__ canon, float* __restrict__ center, uint32_t words_per_row,
+                    uint32_t stride_words) {
+    extern __shared__ __align__(16) uint32_t srec[];
+    __shared__ int s_sum[kTileCols], s_cnt[kTileCols];
+    const int64_t t = blockIdx.x;
+    const TileInfo ti = tiles[t];
+    const uint32_t vec_per_row = (words_per_row + 3) / 4;
+    for (uint32_t c = threadIdx.x; c < kTileCols * vec_per_row; c += blockDim.x) {
+        const uint32_t r = c / vec_per_row, k = c - r * vec_per_row;
+        uint4 v = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+        if (static_cast<int>(r) < ti.nvalid)
+            v = __ldg(reinterpret_cast<const uint4*>(records + (static_cast<int64_t>(ti.snp0) + r) * pitch) + k);
+        uint32_t* d = srec + r * stride_words + k * 4;
+        d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
     }
     __syncthreads();
 
-    const uint8_t* my_rec = reinterpret_cast<const uint8_t*>(s_rec) + lane * stride_words * 4;
-
-    // 2. Per-SNP centre c_s: pooled frequency of a fixed, evenly spread subset of the
-    //    selected samples, rounded to 1/256 (exact in every operand type). f2 is
-    //    invariant to a per-SNP shift of all frequencies, so c_s only shrinks magnitudes.
-    if (warp == 0) {
-        int ca = 0, cc = 0;
-        if (lane < nrows)
-            for (int g = 0; g < a.n_center; ++g) fold_sel(my_rec, __ldg(a.sel + __ldg(a.center_idx + g)), ca, cc);
-        s_center[lane] = (cc > 0) ? rint((0.5 * ca / cc) * 256.0) / 256.0 : 0.5;
-    }
-    __syncthreads();
-
-    const int64_t s = s0 + lane;
-    const bool live = lane < nrows;
-    const int64_t col = live ? static_cast<int64_t>(__ldg(a.snp_col + s)) : 0;
-    const double center = s_center[lane];
-
-    // 3. Populations round-robin over warps; lane = SNP. Exact integer fold.
-    for (int i = warp; i < a.P; i += nwarps) {
-        const int g0 = __ldg(a.pop_off + i), g1 = __ldg(a.pop_off + i + 1);
-        int ac = 0, cn = 0, ac2 = 0, cn2 = 0;
-        int g = g0;
-        for (; g + 1 < g1; g += 2) {
-            fold_sel(my_rec, __ldg(a.sel + g), ac, cn);
-            fold_sel(my_rec, __ldg(a.sel + g + 1), ac2, cn2);
-        }
-        if (g < g1) fold_sel(my_rec, __ldg(a.sel + g), ac, cn);
-        ac += ac2;
-        cn += cn2;
-        if (live) {
-            const double nd = static_cast<double>(cn);
-            const double q = (cn > 0) ? (static_cast<double>(ac) * 0.5) / nd : 0.0;
-            emit<F>(a.op, i, col, make_terms(q, nd, cn > 0, center));
-            if (a.cnt_ac2) {
-                a.cnt_ac2[static_cast<int64_t>(i) + static_cast<int64_t>(a.P) * s] = ac;
-                a.cnt_n[static_cast<int64_t>(i) + static_cast<int64_t>(a.P) * s] = cn;
+    const int lane = threadIdx.x & 31;
+    // Centre of each column: pooled frequency of the called genotypes among the record's
+    // first 256 samples (warp 0; lane l reads 16 samples). Any per-SNP centre keeps f2
+    // exact; this one only has to be close to the population frequencies.
+    if (threadIdx.x < 32) {
+        const uint32_t w = static_cast<uint32_t>(lane);
+        const int64_t r0 = static_cast<int64_t>(w) * 16;
+        const int64_t rem = n_ind - r0;
+        const int nv = (w < words_per_row && w < 16) ? static_cast<int>(rem < 16 ? rem : 16) : 0;
+        uint32_t vmask = 0;
+        for (int m = 0; m < nv; ++m) vmask |= 3u << (8 * (m >> 2) + 6 - 2 * (m & 3));
+        for (int r = 0; r < kTileCols; ++r) {
+            const uint32_t x = (nv > 0 ? srec[r * stride_words + w] : 0u) & vmask;
+            const uint32_t lo = x & 0x55555555u, hi = (x >> 1) & 0x55555555u;
+            const uint32_t miss = lo & hi;
+            const int cnt = __reduce_add_sync(0xffffffffu, __popc(vmask & 0x55555555u) - __popc(miss));
+            const int sum = __reduce_add_sync(0xffffffffu, __popc(lo & ~miss) + 2 * __popc(hi & ~miss));
+            if (lane == 0) {
+                s_cnt[r] = cnt;
+                s_sum[r] = sum;
             }
         }
+    }
+    for (uint32_t w = threadIdx.x; w < words_per_row; w += blockDim.x) {
+        // Valid samples of this word (the record's last word may be partial).
+        const int64_t r0 = static_cast<int64_t>(w) * 16;
+        const int64_t rem = n_ind - r0;
+        const int nv = static_cast<int>(rem < 16 ? rem : 16);
+        uint64_t out[16];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) out[m] = 0;
+#pragma unroll
+        for (int rg = 0; rg < kTileCols / 4; ++rg) {
+            uint32_t rw[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) rw[r] = srec[(4 * rg + r) * stride_words + w];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t sel = static_cast<uint32_t>(j) | (static_cast<uint32_t>(j + 4) << 4);
+                const uint32_t a = __byte_perm(rw[0], rw[1], sel);
+                const uint32_t b = __byte_perm(rw[2], rw[3], sel);
+                const uint32_t y = transpose4x4_2bit(__byte_perm(a, b, 0x0145));
+#pragma unroll
+                for (int m = 0; m < 4; ++m)
+                    out[4 * j + m] |= static_cast<uint64_t>((y >> (8 * (3 - m))) & 0xFFu) << (8 * rg);
+            }
+        }
+        int32_t g[16];
+        if (nv == 16) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int4 v = __ldg(reinterpret_cast<const int4*>(pos + r0) + q);
+                g[4 * q] = v.x; g[4 * q + 1] = v.y; g[4 * q + 2] = v.z; g[4 * q + 3] = v.w;
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < 16; ++m) g[m] = m < nv ? __ldg(pos + r0 + m) : -1;
+        }
+#pragma unroll
+        for (int m = 0; m < 16; ++m)
+            if (g[m] >= 0) canon[t * n_sel + g[m]] = out[m];
+    }
+    __syncthreads();
+    if (threadIdx.x < kTileCols) {
+        const int c = threadIdx.x;
+        const int cnt = s_cnt[c];
+        center[t * kTileCols + c] =
+            (c < ti.nvalid && cnt > 0) ? static_cast<float>(rint((static_cast<double>(s_sum[c]) / (2.0 * cnt)) * 256.0) / 256.0) : 0.5f;
+    }
+}
+
+// Pass 2: per (population, tile) thread, fold the population's samples into exact integer
+// counts for 32 columns at once (SWAR bytes: PRMT maps four 2-bit codes to four count
+// bytes through the sample's ploidy table), then write the operand planes for the 32
+// columns. Samples are read four at a time (one 32-byte sector of canonical tile t).
+template <OpFmt F>
+__global__ void __launch_bounds__(kDecThreads2)
+decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t n_sel,
+                    const uint32_t* __restrict__ sel, const int32_t* __restrict__ pop_off, int P,
+                    const float* __restrict__ center, const double* __restrict__ rec_n,
+                    const double* __restrict__ rec_nm1, const int32_t* __restrict__ col_snp, OperandPlanes op,
+                    int32_t* __restrict__ cnt_ac2, int32_t* __restrict__ cnt_n) {
+    __shared__ uint16_t s_lut[256];
+    for (int x = threadIdx.x; x < 256; x += blockDim.x) {
+        uint32_t v = 0;
+        for (int k = 0; k < 4; ++k) v |= ((static_cast<uint32_t>(x) >> (6 - 2 * k)) & 3u) << (4 * k);
+        s_lut[x] = static_cast<uint16_t>(v);
+    }
+    __syncthreads();
+    const int i = blockIdx.y;
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n_tiles) return;
+    const int g0 = __ldg(pop_off + i), g1 = __ldg(pop_off + i + 1);
+
+    uint32_t acc[kTileCols];  // ac2 | n << 16 per column
+#pragma unroll
+    for (int c = 0; c < kTileCols; ++c) acc[c] = 0;
+    uint32_t sa[8], sn[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sa[k] = sn[k] = 0;
+    int pending = 0;
+    const uint64_t* row = canon + t * n_sel;
+    for (int gb = g0 & ~3; gb < g1; gb += 4) {
+        const uint4 v0 = __ldg(reinterpret_cast<const uint4*>(row + gb));
+        const uint4 v1 = __ldg(reinterpret_cast<const uint4*>(row + gb) + 1);
+        const uint32_t w[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int g = gb + m;
+            if (g < g0 || g >= g1) continue;
+            const uint32_t pl = __ldg(sel + g) & 3u;
+            const uint32_t la = pl == 2 ? 0x00040200u : (pl == 1 ? 0x00020100u : 0u);
+            const uint32_t ln = pl == 2 ? 0x00020202u : (pl == 1 ? 0x00010101u : 0u);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t byte = (w[2 * m + (k >> 2)] >> (8 * (k & 3))) & 0xFFu;
+                const uint32_t s16 = s_lut[byte];
+                sa[k] += __byte_perm(la, 0, s16);
+                sn[k] += __byte_perm(ln, 0, s16);
+            }
+            if (++pending == 63) {  // byte lanes hold at most 63 samples x 4
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        acc[4 * k + b] += ((sa[k] >> (8 * b)) & 0xFFu) | (((sn[k] >> (8 * b)) & 0xFFu) << 16);
+                    sa[k] = sn[k] = 0;
+                }
+                pending = 0;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            acc[4 * k + b] += ((sa[k] >> (8 * b)) & 0xFFu) | (((sn[k] >> (8 * b)) & 0xFFu) << 16);
+
+    const int64_t col0 = t * kTileCols;
+    if (cnt_ac2) {
+#pragma unroll
+        for (int c = 0; c < kTileCols; ++c) {
+            const int32_t s = __ldg(col_snp + col0 + c);
+            if (s >= 0) {
+                cnt_ac2[static_cast<int64_t>(i) + static_cast<int64_t>(P) * s] = static_cast<int32_t>(acc[c] & 0xFFFFu);
+                cnt_n[static_cast<int64_t>(i) + static_cast<int64_t>(P) * s] = static_cast<int32_t>(acc[c] >> 16);
+            }
+        }
+    }
+    if (!op.planes) return;
+#pragma unroll
+    for (int c8 = 0; c8 < kTileCols; c8 += 8) {
+        Terms8 tm;
+        tm.mbits = 0;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const uint32_t n = acc[c8 + c] >> 16, a2 = acc[c8 + c] & 0xFFFFu;
+            // Terms in FP64 (q from the exact counts), rounded once to FP32 for the planes.
+            double pt = 0.0, ah = 0.0;
+            if (n > 0) {
+                const double q = static_cast<double>(a2) * 0.5 * __ldg(rec_n + n);
+                const double h = q * (1.0 - q) * __ldg(rec_nm1 + n);
+                pt = q - static_cast<double>(__ldg(center + col0 + c8 + c));
+                ah = 0.5 * (pt * pt - h);
+                tm.mbits |= 1u << c;
+            }
+            tm.pt[c] = static_cast<float>(pt);
+            tm.ah[c] = static_cast<float>(ah);
+        }
+        emit8<F>(op, i, col0 + c8, tm);
     }
 }
 
@@ -288,36 +505,39 @@ void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int
     c.launches++;
 }
 
-static int center_count(int64_t n_sel) { return static_cast<int>(n_sel < 256 ? n_sel : 256); }
-
-void launch_decode_pa(Ctx& c, const PaDecodeArgs& a, cudaStream_t s) {
-    if (a.n_snp <= 0 || a.P <= 0) return;
-    // Word stride of one staged record, forced odd (bank-conflict-free column reads).
-    uint32_t words = static_cast<uint32_t>((a.pitch + 3) / 4);
-    if ((words & 1u) == 0) words += 1;
-    const size_t smem = static_cast<size_t>(kDecSnps) * words * 4;
-    if (smem > 200 * 1024)
-        fail(STP_INVALID_ARGUMENT, "decode: genotype record of " + std::to_string(a.pitch) +
+void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_ind, const TileInfo* tiles,
+                         int64_t n_tiles, const int32_t* pos, int64_t n_sel, uint64_t* canon, float* center,
+                         cudaStream_t s) {
+    if (n_tiles <= 0) return;
+    const uint32_t words = static_cast<uint32_t>((n_ind + 15) / 16);
+    const uint32_t vec_per_row = (words + 3) / 4;
+    if (static_cast<uint64_t>(vec_per_row) * 16 > pitch || pitch % 16 != 0 ||
+        reinterpret_cast<uintptr_t>(records) % 16 != 0)
+        fail(STP_INVALID_ARGUMENT, "transpose: genotype records need a 16-byte aligned pitch covering the samples");
+    uint32_t stride = vec_per_row * 4 + 1;  // odd word stride: conflict-free column reads
+    const size_t smem = static_cast<size_t>(kTileCols) * stride * 4;
+    if (smem > 220 * 1024)
+        fail(STP_INVALID_ARGUMENT, "transpose: genotype record of " + std::to_string(pitch) +
                                        " bytes exceeds the 32-record shared-memory tile");
-    const int vec16 = (a.pitch % 16 == 0) && (reinterpret_cast<uintptr_t>(a.records) % 16 == 0);
-    const unsigned grid = static_cast<unsigned>((a.n_snp + kDecSnps - 1) / kDecSnps);
+    STPF2_CUDA(cudaFuncSetAttribute(transpose_pa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int threads = static_cast<int>(std::min<uint32_t>(kTransThreads, (words + 31) / 32 * 32));
+    transpose_pa_kernel<<<static_cast<unsigned>(n_tiles), threads, smem, s>>>(records, pitch, n_ind, tiles, pos, n_sel,
+                                                                             canon, center, words, stride);
+    STPF2_CUDA(cudaGetLastError());
+    c.launches++;
+}
+
+void launch_decode_canon(Ctx& c, const CanonDecodeArgs& a, cudaStream_t s) {
+    if (a.P <= 0 || a.n_tiles <= 0) return;
+    const dim3 grid(static_cast<unsigned>((a.n_tiles + kDecThreads2 - 1) / kDecThreads2), static_cast<unsigned>(a.P));
+    if (a.P > 65535) fail(STP_INVALID_ARGUMENT, "more than 65535 populations");
+#define STPF2_DECODE_ARGS a.canon, a.n_tiles, a.n_sel, a.sel, a.pop_off, a.P, a.center, a.rec_n, a.rec_nm1, a.col_snp, a.op, a.cnt_ac2, a.cnt_n
     switch (a.op.fmt) {
-        case OpFmt::F32:
-            STPF2_CUDA(cudaFuncSetAttribute(decode_pa_kernel<OpFmt::F32>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            decode_pa_kernel<OpFmt::F32><<<grid, kDecThreads, smem, s>>>(a, words, vec16);
-            break;
-        case OpFmt::BF16:
-            STPF2_CUDA(cudaFuncSetAttribute(decode_pa_kernel<OpFmt::BF16>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            decode_pa_kernel<OpFmt::BF16><<<grid, kDecThreads, smem, s>>>(a, words, vec16);
-            break;
-        case OpFmt::F16:
-            STPF2_CUDA(cudaFuncSetAttribute(decode_pa_kernel<OpFmt::F16>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            decode_pa_kernel<OpFmt::F16><<<grid, kDecThreads, smem, s>>>(a, words, vec16);
-            break;
+        case OpFmt::F32: decode_canon_kernel<OpFmt::F32><<<grid, kDecThreads2, 0, s>>>(STPF2_DECODE_ARGS); break;
+        case OpFmt::BF16: decode_canon_kernel<OpFmt::BF16><<<grid, kDecThreads2, 0, s>>>(STPF2_DECODE_ARGS); break;
+        case OpFmt::F16: decode_canon_kernel<OpFmt::F16><<<grid, kDecThreads2, 0, s>>>(STPF2_DECODE_ARGS); break;
     }
+#undef STPF2_DECODE_ARGS
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
 }
@@ -363,6 +583,5 @@ void launch_feed_qvn(Ctx& c, const double* Q, const double* V, const double* N, 
     STPF2_CUDA(cudaFreeAsync(center, s));
 }
 
-int decode_center_count(int64_t n_sel) { return center_count(n_sel); }
 
 }  // namespace stpf2

@@ -3,9 +3,10 @@
 // The tensor-core f2 contraction for sm_100a: one persistent, warp-specialised kernel
 // over every (jackknife block, 128x128 population tile pair ti <= tj) work item.
 //
-//   warp 0      TMA producer: per 32-SNP stage, 5 split planes (Pt_hi, Pt_lo, Ah_hi, Ah_lo,
-//               M as 16-bit) + the int8 M plane for the row tile and the column tile
-//               (one side only on diagonal tiles), 64B/32B-swizzled, no multicast.
+//   warp 0      producer: per 32-SNP stage, bulk-copies the pre-swizzled tile images of the
+//               5 split planes (Pt_hi, Pt_lo, Ah_hi, Ah_lo, M as 16-bit) and of the int8 M
+//               plane for the row tile and the column tile (one side on diagonal tiles);
+//               no tensor maps, no multicast.
 //   warp 1      TMEM owner + single-thread tcgen05.mma issuer. Per 16-SNP K step, seven
 //               kind::f16 MMAs accumulate num/2 = sum(Ah_i M_j + M_i Ah_j - Pt_i Pt_j) over
 //               the hi/lo splits (the -Pt Pt products use the descriptor's A-negate bit)
@@ -20,9 +21,6 @@
 // [384,512) int32 vpair per tile. Every wait is bounded (a few seconds); on expiry the
 // kernel raises an error flag the host turns into STP_DEVICE_TIMEOUT, lets its copies and
 // MMAs finish, frees TMEM and returns.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
 #include <algorithm>
 #include <memory>
 
@@ -42,11 +40,24 @@ constexpr uint32_t kTile8 = kTile * kStageK;                      // 4 KiB
 constexpr uint32_t kSideBytes = kPlanes * kTile16 + kTile8;       // 44 KiB
 constexpr uint32_t kStageBytes = 2 * kSideBytes;                  // 88 KiB
 constexpr int kEpiWarps = 8;
-constexpr int kThreads = 64 + 32 * kEpiWarps;
+constexpr int kEpiWarp0 = 2;                        // epilogue = warps 2..9
+constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);  // 320
+// 10 warps put three warps on some SM sub-partitions, so at most 16384 / (3 * 32) = 170
+// registers per thread; the epilogue's 64 FP64 accumulators fit, the end-of-tile stores spill.
 constexpr uint32_t kTmemCols = 512;
 constexpr unsigned long long kTimeoutNs = 4000000000ull;
+// Per-epilogue-warp staging tile for the transposed stores: f2 and vpair, 32 rows x 8
+// columns each, rows padded to 9 doubles (fewer bank conflicts).
+constexpr int kStagePitch = 9;
+constexpr int kStageHalf = 32 * kStagePitch;
+constexpr int kStageDoubles = 2 * kStageHalf;
+constexpr uint32_t kCtlBytes = 256;
 
 struct UmmaArgs {
+    const uint8_t* planes16;  // tiled 16-bit plane images (5 planes, plane_stride apart)
+    const uint8_t* plane8;    // tiled int8 M images
+    int64_t plane_stride;
+    int64_t n_ck;             // column chunks per row tile
     const WorkItem* items;
     int n_items;
     const BlockInfo* blocks;
@@ -107,7 +118,7 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, uint32_t pa
 
 // Bounded wait: false on timeout (which also raises the CTA's abort flag and the global
 // error flag) or when another role of this CTA has already aborted.
-__device__ __noinline__ bool wait_bounded(unsigned long long* b, uint32_t parity, SmemCtl* ctl, int* err,
+__device__ __forceinline__ bool wait_bounded(unsigned long long* b, uint32_t parity, SmemCtl* ctl, int* err,
                                           bool honour_abort = true) {
     if (mbar_try_wait(b, parity)) return true;
     const unsigned long long t0 = globaltimer();
@@ -124,21 +135,13 @@ __device__ __noinline__ bool wait_bounded(unsigned long long* b, uint32_t parity
     }
 }
 
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, int x, int y, int z,
-                                            unsigned long long* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-        "[%5];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, int x, int y, unsigned long long* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-        "[%4];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
+// Plain bulk copy global -> shared, completing on an mbarrier (no tensor map, no
+// multicast): size and both addresses multiples of 16 bytes.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -175,6 +178,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         : "r"(taddr));
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // UMMA shared-memory descriptor, K-major, swizzled: start address, LBO (unused for a
@@ -189,8 +201,7 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo_bytes,
 
 __device__ __forceinline__ int stages_of(int k) { return (k + kStageK - 1) / kStageK; }
 
-__device__ void producer(const CUtensorMap* tm16, const CUtensorMap* tm8, const UmmaArgs& a, uint8_t* smem,
-                         SmemCtl* ctl) {
+__device__ void producer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl) {
     uint32_t g = 0;
     for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
         const WorkItem w = a.items[it];
@@ -204,14 +215,18 @@ __device__ void producer(const CUtensorMap* tm16, const CUtensorMap* tm8, const 
             {
                 uint8_t* sb = smem + slot * kStageBytes;
                 mbar_expect_tx(&ctl->full[slot], diag ? kSideBytes : kStageBytes);
-                const int x = static_cast<int>(bi.col) + st * kStageK;
-                const int ya = w.ti * kTile, yb = w.tj * kTile;
-                for (int p = 0; p < kPlanes; ++p) tma_load_3d(sb + p * kTile16, tm16, x, ya, p, &ctl->full[slot]);
-                tma_load_2d(sb + kPlanes * kTile16, tm8, x, ya, &ctl->full[slot]);
+                const int64_t chunk = bi.col / kStageK + st;
+                const int64_t ta = static_cast<int64_t>(w.ti) * a.n_ck + chunk;
+                for (int p = 0; p < kPlanes; ++p)
+                    bulk_load(sb + p * kTile16, a.planes16 + p * a.plane_stride + ta * kTile16, kTile16, &ctl->full[slot]);
+                bulk_load(sb + kPlanes * kTile16, a.plane8 + ta * kTile8, kTile8, &ctl->full[slot]);
                 if (!diag) {
                     uint8_t* sbb = sb + kSideBytes;
-                    for (int p = 0; p < kPlanes; ++p) tma_load_3d(sbb + p * kTile16, tm16, x, yb, p, &ctl->full[slot]);
-                    tma_load_2d(sbb + kPlanes * kTile16, tm8, x, yb, &ctl->full[slot]);
+                    const int64_t tb = static_cast<int64_t>(w.tj) * a.n_ck + chunk;
+                    for (int p = 0; p < kPlanes; ++p)
+                        bulk_load(sbb + p * kTile16, a.planes16 + p * a.plane_stride + tb * kTile16, kTile16,
+                                  &ctl->full[slot]);
+                    bulk_load(sbb + kPlanes * kTile16, a.plane8 + tb * kTile8, kTile8, &ctl->full[slot]);
                 }
             }
         }
@@ -291,15 +306,15 @@ done:
     wait_bounded(&ctl->drain, 0u, ctl, a.err, false);
 }
 
-__device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int warp, int lane) {
-    const int e = warp - 2;
+__device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int warp, int lane, double* stage) {
+    const int e = warp - kEpiWarp0;
     const int q = warp & 3;                 // TMEM lane quarter this warp may access
     const int h = e >> 2;                   // column half of the tile
     const int r = q * 32 + lane;            // tile row (TMEM lane)
     const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
     const int P = a.P;
     uint32_t cs = 0, is = 0;
-    double acc[64];
+    double acc[64];  // FP64 running numerator per column
     for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
         const WorkItem w = a.items[it];
         const BlockInfo bi = a.blocks[w.blk];
@@ -330,16 +345,16 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) return;
             tc_fence_after();
-            uint32_t v[32];
             const uint32_t base = tmem + lane_addr + static_cast<uint32_t>(nb) * 128u + static_cast<uint32_t>(h) * 64u;
-            tmem_ld32(base, v);
-            tmem_wait_ld();
 #pragma unroll
-            for (int c = 0; c < 32; ++c) acc[c] += static_cast<double>(__uint_as_float(v[c]));
-            tmem_ld32(base + 32u, v);
-            tmem_wait_ld();
+            for (int q16 = 0; q16 < 4; ++q16) {
+                uint32_t v[16];
+                tmem_ld16(base + static_cast<uint32_t>(q16) * 16u, v);
+                tmem_wait_ld();
 #pragma unroll
-            for (int c = 0; c < 32; ++c) acc[32 + c] += static_cast<double>(__uint_as_float(v[c]));
+                for (int c = 0; c < 16; ++c)
+                    acc[q16 * 16 + c] += static_cast<double>(__uint_as_float(v[c]));
+            }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&ctl->acc_empty[nb]);
@@ -354,32 +369,51 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
         }
         tc_fence_after();
         const uint32_t vbase = tmem + lane_addr + 256u + static_cast<uint32_t>(vb) * 128u + static_cast<uint32_t>(h) * 64u;
+        // Output: (i, j) straight from registers (32 consecutive i per store: full sectors);
+        // (j, i) through this warp's staging tile, so each store covers 4 rows x 8
+        // consecutive j (64-byte segments) instead of 32 scattered 8-byte pieces.
+        const int i0 = w.ti * kTile + q * 32;
+        const int64_t row_i = slab + i;                       // (i, j) at row_i + P*j
+        const int64_t row_j0 = slab + static_cast<int64_t>(P) * i0;  // (j, i0 + rr) at row_j0 + P*rr + j
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            uint32_t v[32];
-            tmem_ld32(vbase + static_cast<uint32_t>(half) * 32u, v);
+        for (int q16 = 0; q16 < 4; ++q16) {
+            uint32_t v[16];
+            tmem_ld16(vbase + static_cast<uint32_t>(q16) * 16u, v);
             tmem_wait_ld();
-            if (half == 1) {
+            if (q16 == 3) {
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&ctl->vp_empty[vb]);
             }
-            if (i < P) {
-                // Fully unrolled so acc[] stays in registers.
 #pragma unroll
-                for (int c = 0; c < 32; ++c) {
-                    const int j = j0 + half * 32 + c;
-                    if (j < P && !(diag && j < i)) {
-                        const double vp = static_cast<double>(static_cast<int32_t>(v[c]));
-                        const double f = (vp > 0.0) ? (acc[half * 32 + c] * a.num_scale) / vp : 0.0;
-                        const int64_t ij = slab + i + static_cast<int64_t>(P) * j;
-                        const int64_t ji = slab + j + static_cast<int64_t>(P) * i;
-                        a.f2[ij] = f;
-                        a.vpair[ij] = vp;
-                        a.f2[ji] = f;
-                        a.vpair[ji] = vp;
+            for (int cg = 0; cg < 16; cg += 8) {
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const int col = q16 * 16 + cg + c;
+                    const int j = j0 + col;
+                    const double vp = static_cast<double>(static_cast<int32_t>(v[cg + c]));
+                    const double num = acc[col];
+                    const double f = (vp > 0.0) ? (num * a.num_scale) / vp : 0.0;
+                    if (i < P && j < P && !(diag && j < i)) {
+                        const int64_t ij = row_i + static_cast<int64_t>(P) * j;
+                        __stcs(a.f2 + ij, f);  // output is never re-read: evict-first
+                        __stcs(a.vpair + ij, vp);
+                    }
+                    stage[lane * kStagePitch + c] = f;
+                    stage[kStageHalf + lane * kStagePitch + c] = vp;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int rr = 4 * k + (lane >> 3), cc = lane & 7;
+                    const int jj = j0 + q16 * 16 + cg + cc;
+                    if (i0 + rr < P && jj < P && !(diag && jj <= i0 + rr)) {
+                        const int64_t ji = row_j0 + static_cast<int64_t>(P) * rr + jj;
+                        __stcs(a.f2 + ji, stage[rr * kStagePitch + cc]);
+                        __stcs(a.vpair + ji, stage[kStageHalf + rr * kStagePitch + cc]);
                     }
                 }
+                __syncwarp();
             }
         }
         ++is;
@@ -387,7 +421,7 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
 }
 
 __global__ void __maxnreg__(168)
-f2_umma_kernel(const __grid_constant__ CUtensorMap tm16, const __grid_constant__ CUtensorMap tm8, UmmaArgs a) {
+f2_umma_kernel(const __grid_constant__ UmmaArgs a) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     SmemCtl* ctl = reinterpret_cast<SmemCtl*>(smem + kStages * kStageBytes);
@@ -420,12 +454,12 @@ f2_umma_kernel(const __grid_constant__ CUtensorMap tm16, const __grid_constant__
     tc_fence_after();
     const uint32_t tmem = ctl->tmem_base;
 
-    if (warp == 0) {
-        if (lane == 0) producer(&tm16, &tm8, a, smem, ctl);
-    } else if (warp == 1) {
-        if (lane == 0) mma_issuer(a, smem, ctl, tmem);
+    if (warp < kEpiWarp0) {
+        if (warp == 0 && lane == 0) producer(a, smem, ctl);
+        if (warp == 1 && lane == 0) mma_issuer(a, smem, ctl, tmem);
     } else {
-        epilogue(a, ctl, tmem, warp, lane);
+        epilogue(a, ctl, tmem, warp, lane,
+                 reinterpret_cast<double*>(smem + kStages * kStageBytes + kCtlBytes) + (warp - kEpiWarp0) * kStageDoubles);
     }
 
     tc_fence_before();
@@ -444,24 +478,14 @@ uint32_t idesc_f16(bool bf16, bool negate_a) {
 }
 uint32_t idesc_u8_s32() { return (2u << 4) | (0u << 7) | (0u << 10) | ((kTile >> 3) << 17) | ((kTile >> 4) << 24); }
 
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        cudaDriverEntryPointQueryResult q{};
-        void* p = nullptr;
-        STPF2_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
-        if (q != cudaDriverEntryPointSuccess || !p) fail(STP_CUDA_ERROR, "cuTensorMapEncodeTiled unavailable");
-        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
-}
-
-constexpr size_t kSmemBytes = kStages * kStageBytes + sizeof(SmemCtl) + 1024;
+constexpr size_t kSmemBytes = kStages * kStageBytes + kCtlBytes + kEpiWarps * kStageDoubles * sizeof(double) + 1024;
 
 }  // namespace
 
 struct UmmaPlan {
-    CUtensorMap tm16{}, tm8{};
+    const uint8_t* planes16 = nullptr;
+    const uint8_t* plane8 = nullptr;
+    int64_t plane_stride = 0, n_ck = 0;
     DevBuf items, blocks, err;
     int n_items = 0;
     int P = 0;
@@ -488,29 +512,11 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
                                cudaMemcpyHostToDevice, c.stream));
     STPF2_CUDA(cudaMemsetAsync(p->err.ptr, 0, 16, c.stream));
 
-    auto enc = tensor_map_encoder();
-    const cuuint64_t ld = static_cast<cuuint64_t>(op.ld), P = static_cast<cuuint64_t>(op.P);
-    {
-        const cuuint64_t dims[3] = {ld, P, kPlanes};
-        const cuuint64_t strides[2] = {ld * 2, ld * P * 2};
-        const cuuint32_t box[3] = {kStageK, kTile, 1};
-        const cuuint32_t es[3] = {1, 1, 1};
-        const CUresult r = enc(&p->tm16, op.fmt == OpFmt::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
-                               3, op.planes, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                               CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) fail(STP_CUDA_ERROR, "cuTensorMapEncodeTiled (16-bit planes) failed: " + std::to_string(r));
-    }
-    {
-        const cuuint64_t dims[2] = {ld, P};
-        const cuuint64_t strides[1] = {ld};
-        const cuuint32_t box[2] = {kStageK, kTile};
-        const cuuint32_t es[2] = {1, 1};
-        const CUresult r = enc(&p->tm8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, op.m_u8, dims, strides, box, es,
-                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
-                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) fail(STP_CUDA_ERROR, "cuTensorMapEncodeTiled (int8 plane) failed: " + std::to_string(r));
-    }
+    if (op.n_rt <= 0 || op.n_ck <= 0) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs tiled planes");
+    p->planes16 = static_cast<const uint8_t*>(op.planes);
+    p->plane8 = op.m_u8;
+    p->n_ck = op.n_ck;
+    p->plane_stride = static_cast<int64_t>(op.n_rt) * op.n_ck * kTile16;
     STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kSmemBytes)));
     return p.release();
@@ -521,6 +527,10 @@ void umma_plan_destroy(UmmaPlan* p) { delete p; }
 void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s) {
     if (!p || p->n_items <= 0) return;
     UmmaArgs a{};
+    a.planes16 = p->planes16;
+    a.plane8 = p->plane8;
+    a.plane_stride = p->plane_stride;
+    a.n_ck = p->n_ck;
     a.items = p->items.as<WorkItem>();
     a.n_items = p->n_items;
     a.blocks = p->blocks.as<BlockInfo>();
@@ -534,7 +544,7 @@ void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t
     a.idesc_am = idesc_f16(bf16, false);
     a.idesc_i8 = idesc_u8_s32();
     const int grid = std::min(c.sm_count, p->n_items);
-    f2_umma_kernel<<<grid, kThreads, kSmemBytes, s>>>(p->tm16, p->tm8, a);
+    f2_umma_kernel<<<grid, kThreads, kSmemBytes, s>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         cudaFuncAttributes fa{};

@@ -21,7 +21,6 @@ struct stp_ctx : stpf2::Ctx {};
 
 namespace stpf2 {
 
-int decode_center_count(int64_t n_sel);
 int simt_tile();
 
 namespace {
@@ -119,20 +118,31 @@ std::vector<WorkItem> make_work_items(const BlockLayout& L, int P, int tile) {
 }
 
 size_t operand_plane_bytes(OpFmt f, int P, int64_t ld) {
-    const size_t pl = static_cast<size_t>(P) * static_cast<size_t>(ld);
-    const size_t main = (f == OpFmt::F32) ? 2 * pl * 4 : 5 * pl * 2;
-    return align256(main) + align256(pl);
+    if (f == OpFmt::F32) {
+        const size_t pl = static_cast<size_t>(P) * static_cast<size_t>(ld);
+        return align256(2 * pl * 4) + align256(pl);
+    }
+    const size_t tiles = static_cast<size_t>((P + kTileRows - 1) / kTileRows) * static_cast<size_t>(ld / kTileK);
+    return align256(5 * tiles * kTile16Bytes) + align256(tiles * kTile8Bytes);
 }
 
 void bind_operand_planes(OperandPlanes& op, OpFmt f, int P, int64_t ld, void* base) {
-    const size_t pl = static_cast<size_t>(P) * static_cast<size_t>(ld);
-    const size_t main = (f == OpFmt::F32) ? 2 * pl * 4 : 5 * pl * 2;
     op.fmt = f;
     op.P = P;
     op.ld = ld;
     op.planes = base;
-    op.m_u8 = static_cast<uint8_t*>(base) + align256(main);
     op.scale_inv = (f == OpFmt::F16) ? 1.0 / double(1 << (2 * kF16PtShift)) : 1.0;
+    if (f == OpFmt::F32) {
+        const size_t pl = static_cast<size_t>(P) * static_cast<size_t>(ld);
+        op.m_u8 = static_cast<uint8_t*>(base) + align256(2 * pl * 4);
+        op.n_rt = 0;
+        op.n_ck = 0;
+    } else {
+        op.n_rt = (P + kTileRows - 1) / kTileRows;
+        op.n_ck = ld / kTileK;
+        const size_t tiles = static_cast<size_t>(op.n_rt) * static_cast<size_t>(op.n_ck);
+        op.m_u8 = static_cast<uint8_t*>(base) + align256(5 * tiles * kTile16Bytes);
+    }
 }
 
 // ---- plan ------------------------------------------------------------------------------
@@ -145,8 +155,11 @@ struct Plan {
     int precision = 0;
     bool detect = false;
     BlockLayout L;
-    DevBuf sel, pop_off, center_idx, snp_col, blocks, items, own_planes;
-    int n_center = 0, n_items = 0;
+    DevBuf sel, pop_off, pos, tiles, col_snp, rec_n, rec_nm1, canon, center, blocks, items, own_planes, repitched;
+    int64_t n_ind = 0, n_tiles = 0, n_sel_pad = 0;
+    int n_items = 0;
+    bool repitch = false;
+    uint64_t src_pitch = 0, bpr = 0;
     OperandPlanes op;
     UmmaPlan* umma = nullptr;
     // Timing: three events per run (start, after decode, after contraction), one set per
@@ -162,7 +175,7 @@ struct Plan {
                 if (e) cudaEventDestroy(e);
     }
 
-    int launches() const { return (detect ? 1 : 0) + 1 + 1; }
+    int launches() const { return (detect ? 1 : 0) + 2 + 1; }
 };
 
 namespace {
@@ -208,16 +221,63 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
     upload(p->sel, sel, s);
 
     std::vector<int32_t> po(static_cast<size_t>(r.n_pop) + 1, 0);
+    int64_t max_pop = 0;
     for (int i = 0; i <= r.n_pop && r.n_pop > 0; ++i) po[i] = static_cast<int32_t>(r.pop_offsets[i]);
+    for (int i = 0; i < r.n_pop; ++i) max_pop = std::max<int64_t>(max_pop, r.pop_offsets[i + 1] - r.pop_offsets[i]);
+    need(max_pop <= 16383, "a population has more than 16383 samples");
     upload(p->pop_off, po, s);
 
-    p->n_center = decode_center_count(n_sel);
-    std::vector<int32_t> ci(static_cast<size_t>(p->n_center));
-    for (int k = 0; k < p->n_center; ++k) ci[k] = static_cast<int32_t>((static_cast<int64_t>(k) * n_sel) / p->n_center);
-    upload(p->center_idx, ci, s);
+    // File row -> selected index (each row may be selected once).
+    p->n_ind = r.geno.n_ind;
+    std::vector<int32_t> pos(static_cast<size_t>(std::max<int64_t>(r.geno.n_ind, 0)), -1);
+    for (int64_t g = 0; g < n_sel; ++g) {
+        int32_t& slot = pos[static_cast<size_t>(r.sel_rows[g])];
+        need(slot < 0, "a sample is selected more than once");
+        slot = static_cast<int32_t>(g);
+    }
+    upload(p->pos, pos, s);
+
+    // 1/n and 1/max(n-1, 1) for every called-allele count a population can reach.
+    const int64_t n_max = 2 * max_pop + 1;
+    std::vector<double> rn(static_cast<size_t>(n_max) + 1, 0.0), rnm1(static_cast<size_t>(n_max) + 1, 1.0);
+    for (int64_t n = 1; n <= n_max; ++n) {
+        rn[n] = 1.0 / static_cast<double>(n);
+        rnm1[n] = 1.0 / std::max(static_cast<double>(n) - 1.0, 1.0);
+    }
+    upload(p->rec_n, rn, s);
+    upload(p->rec_nm1, rnm1, s);
 
     p->L = make_block_layout(r.block_id, r.geno.n_snp, r.n_block);
-    upload(p->snp_col, p->L.snp_col, s);
+    // 32-column tiles of the padded column space (blocks start on 64-column boundaries,
+    // so a tile never spans two blocks).
+    p->n_tiles = p->L.ld / 32;
+    std::vector<TileInfo> tiles(static_cast<size_t>(p->n_tiles), TileInfo{0, 0});
+    std::vector<int32_t> col_snp(static_cast<size_t>(p->L.ld), -1);
+    for (int b = 0; b < p->L.n_block; ++b) {
+        const BlockInfo& bi = p->L.blocks[b];
+        for (int64_t off = 0; off < (bi.k + 31) / 32 * 32; off += 32) {
+            TileInfo& ti = tiles[static_cast<size_t>((bi.col + off) / 32)];
+            ti.snp0 = static_cast<int32_t>(p->L.snp_begin[b] + off);
+            ti.nvalid = static_cast<int32_t>(std::min<int64_t>(32, bi.k - off));
+        }
+        for (int64_t k = 0; k < bi.k; ++k) col_snp[static_cast<size_t>(bi.col + k)] = static_cast<int32_t>(p->L.snp_begin[b] + k);
+    }
+    upload(p->tiles, tiles, s);
+    upload(p->col_snp, col_snp, s);
+    p->n_sel_pad = (n_sel + 3) / 4 * 4;
+    p->canon.reserve(std::max<size_t>(static_cast<size_t>(p->n_tiles) * p->n_sel_pad * 8, 64));
+    p->center.reserve(std::max<size_t>(static_cast<size_t>(p->L.ld) * 4, 64));
+
+    // The transpose reads records with 16-byte loads: records of another pitch are copied
+    // once per run into a 16-byte pitch.
+    p->bpr = r.geno.bytes_per_record;
+    p->src_pitch = pitch;
+    const uint64_t need_bytes = static_cast<uint64_t>((r.geno.n_ind + 63) / 64) * 16;
+    p->repitch = (pitch % 16 != 0) || pitch < need_bytes;
+    if (p->repitch) {
+        p->pitch = (std::max<uint64_t>(r.geno.bytes_per_record, need_bytes) + 15) / 16 * 16;
+        p->repitched.reserve(std::max<size_t>(static_cast<size_t>(p->pitch) * r.geno.n_snp, 64));
+    }
     upload(p->blocks, p->L.blocks, s);
 
     const size_t ob = operand_plane_bytes(fmt, std::max(r.n_pop, 1), p->L.ld);
@@ -239,6 +299,38 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
     return p;
 }
 
+// Ploidy (when detected) -> transpose to canonical tiles -> per-population decode into the
+// operand planes (and, for tests, the integer counts).
+void launch_decode(Plan& p, const uint8_t* d_records, int32_t* cnt_ac2, int32_t* cnt_n, cudaStream_t s) {
+    Ctx& c = *p.ctx;
+    if (p.n_snp <= 0) return;
+    const uint8_t* rec = d_records;
+    if (p.repitch) {
+        STPF2_CUDA(cudaMemcpy2DAsync(p.repitched.ptr, p.pitch, d_records, p.src_pitch, p.bpr,
+                                     static_cast<size_t>(p.n_snp), cudaMemcpyDeviceToDevice, s));
+        rec = p.repitched.as<uint8_t>();
+    }
+    if (p.detect) launch_detect_ploidy_pa(c, rec, p.pitch, p.n_snp, p.sel.as<uint32_t>(), p.n_sel, s);
+    launch_transpose_pa(c, rec, p.pitch, p.n_ind, p.tiles.as<TileInfo>(), p.n_tiles, p.pos.as<int32_t>(), p.n_sel_pad,
+                        p.canon.as<uint64_t>(), p.center.as<float>(), s);
+    CanonDecodeArgs a;
+    a.canon = p.canon.as<uint64_t>();
+    a.n_tiles = p.n_tiles;
+    a.n_sel = p.n_sel_pad;
+    a.sel = p.sel.as<uint32_t>();
+    a.pop_off = p.pop_off.as<int32_t>();
+    a.P = p.P;
+    a.center = p.center.as<float>();
+    a.rec_n = p.rec_n.as<double>();
+    a.rec_nm1 = p.rec_nm1.as<double>();
+    a.col_snp = p.col_snp.as<int32_t>();
+    a.op = p.op;
+    if (cnt_ac2) a.op.planes = nullptr;
+    a.cnt_ac2 = cnt_ac2;
+    a.cnt_n = cnt_n;
+    launch_decode_canon(c, a, s);
+}
+
 void run_plan(Plan& p, const uint8_t* d_records, double* d_f2, double* d_vpair, cudaStream_t s) {
     Ctx& c = *p.ctx;
     const size_t out_elems = static_cast<size_t>(p.P) * p.P * p.L.n_block;
@@ -258,20 +350,7 @@ void run_plan(Plan& p, const uint8_t* d_records, double* d_f2, double* d_vpair, 
         tev = &p.ev[p.n_timed++];
         STPF2_CUDA(cudaEventRecord((*tev)[0], s));
     }
-    if (p.detect)
-        launch_detect_ploidy_pa(c, d_records, p.pitch, p.n_snp, p.sel.as<uint32_t>(), p.n_sel, s);
-    PaDecodeArgs a;
-    a.records = d_records;
-    a.pitch = p.pitch;
-    a.n_snp = p.n_snp;
-    a.sel = p.sel.as<uint32_t>();
-    a.pop_off = p.pop_off.as<int32_t>();
-    a.P = p.P;
-    a.center_idx = p.center_idx.as<int32_t>();
-    a.n_center = p.n_center;
-    a.snp_col = p.snp_col.as<int32_t>();
-    a.op = p.op;
-    launch_decode_pa(c, a, s);
+    launch_decode(p, d_records, nullptr, nullptr, s);
     if (tev) STPF2_CUDA(cudaEventRecord((*tev)[1], s));
     if (p.precision == STP_PREC_FP32_SIMT)
         launch_f2_simt(c, p.items.as<WorkItem>(), p.n_items, p.blocks.as<BlockInfo>(), p.op, d_f2, d_vpair, s);
@@ -449,22 +528,7 @@ stp_status stp_decode_counts(stp_ctx* ctx, const stp_geno_view* geno, const int6
         DevBuf d_ac2, d_n;
         d_ac2.reserve(cnt * 4);
         d_n.reserve(cnt * 4);
-        if (p->detect)
-            launch_detect_ploidy_pa(*ctx, d_rec, pitch, p->n_snp, p->sel.as<uint32_t>(), p->n_sel, s);
-        PaDecodeArgs a;
-        a.records = d_rec;
-        a.pitch = pitch;
-        a.n_snp = geno->n_snp;
-        a.sel = p->sel.as<uint32_t>();
-        a.pop_off = p->pop_off.as<int32_t>();
-        a.P = n_pop;
-        a.center_idx = p->center_idx.as<int32_t>();
-        a.n_center = p->n_center;
-        a.snp_col = p->snp_col.as<int32_t>();
-        a.op = p->op;
-        a.cnt_ac2 = d_ac2.as<int32_t>();
-        a.cnt_n = d_n.as<int32_t>();
-        launch_decode_pa(*ctx, a, s);
+        launch_decode(*p, d_rec, d_ac2.as<int32_t>(), d_n.as<int32_t>(), s);
         STPF2_CUDA(cudaMemcpyAsync(ac2, d_ac2.ptr, cnt * 4, cudaMemcpyDeviceToHost, s));
         STPF2_CUDA(cudaMemcpyAsync(n, d_n.ptr, cnt * 4, cudaMemcpyDeviceToHost, s));
         STPF2_CUDA(cudaStreamSynchronize(s));

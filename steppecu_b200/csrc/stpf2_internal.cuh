@@ -129,6 +129,14 @@ inline OpFmt fmt_of(int precision) {
 // Plane p, row i, column c at planes + (p * P + i) * ld + c (elements of the plane type).
 // Pt = m*(q - c_s), Ah = m*((q - c_s)^2 - h)/2, h = q(1-q)/max(n-1,1), m = [n > 0];
 // then num(i,j) = 2 * sum_s (Ah_i M_j + M_i Ah_j - Pt_i Pt_j).
+//
+// The 16-bit planes (and their int8 M plane) are TILED for the tensor cores: populations
+// in row tiles of 128, columns in chunks of 32, and every (row tile, chunk) stored as one
+// contiguous image of exactly what the MMA reads from shared memory: 128 rows x 64 bytes
+// with the 64-byte swizzle (16-byte chunk index XOR (row / 2) % 4) for 16-bit planes,
+// 128 rows x 32 bytes with the 32-byte swizzle (chunk XOR (row / 4) % 2) for int8. A
+// pipeline stage is then a handful of contiguous 8 KiB / 4 KiB bulk copies. Rows past P
+// stay zero. The FP32 planes of the SIMT contraction stay row-major.
 struct OperandPlanes {
     OpFmt fmt = OpFmt::F32;
     int P = 0;
@@ -136,7 +144,22 @@ struct OperandPlanes {
     void* planes = nullptr;
     uint8_t* m_u8 = nullptr;
     double scale_inv = 1.0;  // numerator scale undo (F16 planes are pre-scaled)
+    int n_rt = 0;            // tiled: row tiles of 128 populations
+    int64_t n_ck = 0;        // tiled: column chunks of 32
 };
+
+constexpr int kTileRows = 128;
+constexpr int kTileK = 32;
+constexpr int64_t kTile16Bytes = kTileRows * kTileK * 2;  // one 16-bit tile image
+constexpr int64_t kTile8Bytes = kTileRows * kTileK;       // one int8 tile image
+
+// Byte offset of element (row r < 128, column k < 32) inside a 16-bit / int8 tile image.
+__host__ __device__ inline uint32_t tile16_offset(int r, int k) {
+    return static_cast<uint32_t>(r * 64 + ((((k >> 3) ^ (r >> 1)) & 3) << 4) + (k & 7) * 2);
+}
+__host__ __device__ inline uint32_t tile8_offset(int r, int k) {
+    return static_cast<uint32_t>(r * 32 + ((((k >> 4) ^ (r >> 2)) & 1) << 4) + (k & 15));
+}
 
 constexpr int kF16PtShift = 7;  // F16: Pt scaled by 2^7, Ah by 2^14 (num by 2^14)
 
@@ -145,32 +168,42 @@ void bind_operand_planes(OperandPlanes& op, OpFmt f, int P, int64_t ld, void* ba
 
 // ---- launch wrappers (defined in the .cu files) ----------------------------------------
 
-// Selected-sample descriptor for the PA decode: byte offset in the record << 5 |
-// code shift << 2 | ploidy (0 = contributes nothing).
+// Selected-sample descriptor: byte offset in the record << 5 | code shift << 2 | ploidy
+// (0 = contributes nothing).
 inline uint32_t pack_sel(int64_t row, int ploidy) {
     const uint32_t byte = static_cast<uint32_t>(row >> 2);
     const uint32_t shift = static_cast<uint32_t>(6 - 2 * (row & 3));
     return (byte << 5) | (shift << 2) | static_cast<uint32_t>(ploidy & 3);
 }
 
-struct PaDecodeArgs {
-    const uint8_t* records = nullptr;
-    uint64_t pitch = 0;
-    int64_t n_snp = 0;
-    const uint32_t* sel = nullptr;      // [n_sel] packed descriptors (ploidy filled in)
-    const int32_t* pop_off = nullptr;   // [P+1]
+// One 32-column tile of the padded column space: the SNP of its first column and how many
+// of its columns hold SNPs (the rest are block padding).
+struct TileInfo {
+    int32_t snp0;
+    int32_t nvalid;
+};
+
+struct CanonDecodeArgs {
+    const uint64_t* canon = nullptr;   // [n_tiles][n_sel] 8-byte canonical tiles
+    int64_t n_tiles = 0, n_sel = 0;
+    const uint32_t* sel = nullptr;     // [n_sel] descriptors (ploidy in the low bits)
+    const int32_t* pop_off = nullptr;  // [P+1]
     int P = 0;
-    const int32_t* center_idx = nullptr;  // [n_center] indices into sel: the centring subset
-    int n_center = 0;
-    const int32_t* snp_col = nullptr;   // [n_snp]
-    OperandPlanes op;
-    int32_t* cnt_ac2 = nullptr;         // optional [P x n_snp] column-major
+    const float* center = nullptr;     // [ld] per-column centre (a multiple of 1/256)
+    const double* rec_n = nullptr;     // [n_max+1] 1/n (0 at n = 0)
+    const double* rec_nm1 = nullptr;   // [n_max+1] 1/max(n-1, 1)
+    const int32_t* col_snp = nullptr;  // [ld] SNP of each column, -1 for padding
+    OperandPlanes op;                  // planes == nullptr: counts only
+    int32_t* cnt_ac2 = nullptr;        // optional [P x n_snp] column-major counts
     int32_t* cnt_n = nullptr;
 };
 
 void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_snp,
                              uint32_t* sel, int64_t n_sel, cudaStream_t s);
-void launch_decode_pa(Ctx& c, const PaDecodeArgs& a, cudaStream_t s);
+void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_ind, const TileInfo* tiles,
+                         int64_t n_tiles, const int32_t* pos, int64_t n_sel, uint64_t* canon, float* center,
+                         cudaStream_t s);
+void launch_decode_canon(Ctx& c, const CanonDecodeArgs& a, cudaStream_t s);
 void launch_decode_canonical(Ctx& c, const uint8_t* packed, uint64_t bpr, int64_t n_snp,
                              int64_t n_ind, const int32_t* pop_off, int P, const int32_t* ploidy,
                              double* q, double* v, double* n, cudaStream_t s);
