@@ -21,8 +21,8 @@ namespace stpf2 {
 namespace {
 
 constexpr int kTileCols = 32;      // columns per canonical tile (8 bytes per sample)
-constexpr int kTransThreads = 320; // transpose: one thread per 16 samples (looping)
-constexpr int kDecThreads2 = 128;  // decode: one thread per (population, tile)
+constexpr int kTransThreads = 256; // transpose: (16 samples, tile) per thread
+constexpr int kDecThreads2 = 512;  // decode: (4 tiles) x (128 populations) per CTA
 constexpr int kPloidyWindow = 1000;  // decode_af.hpp:29 (kPloidyDetectSnps)
 
 // Per-element operand terms of one (pop, SNP) from its exact counts. q matches the
@@ -177,12 +177,13 @@ __device__ __forceinline__ void emit8(const OperandPlanes& op, int i, int64_t co
     }
 }
 
-// ---- canonical tile-major genotypes ------------------------------------------------------
+// ---- canonical genotypes -------------------------------------------------------------------
 //
 // The decode runs in two passes over an intermediate "canonical" copy of the selected
-// samples' genotypes, laid out in the padded column space of the operand planes:
-// tile t = columns [32t, 32t+32); selected sample g owns the 8 bytes canon[t * n_sel + g],
-// column 32t + 4k + j in byte k at bits (7-2j, 6-2j) (MSB-first, as in the .geno records).
+// samples' genotypes, laid out in the padded column space of the operand planes. Columns
+// are grouped in quads of 128 = four 32-column tiles; selected sample g owns one 32-byte
+// sector per quad: canon[((quad * n_sel + g) * 4 + sub] holds tile 4*quad + sub, column
+// 32*tile + 4k + j in byte k at bits (7-2j, 6-2j) (MSB-first, as in the .geno records).
 // Padding columns hold code 3 (missing) and therefore decode to zero operands.
 
 // 4x4 transpose of 2-bit elements packed MSB-first in a 32-bit word (row 0 in the top
@@ -195,66 +196,80 @@ __device__ __forceinline__ uint32_t transpose4x4_2bit(uint32_t w) {
     return w;
 }
 
-// Pass 1: SNP-major records -> canonical tiles (gathering the selected samples), plus the
-// per-column centre c_s = pooled frequency of every called genotype in the record, rounded
-// to 1/256. One CTA per 32-column tile: its (<= 32) records are staged in shared memory
-// with 128-bit loads; each thread transposes 16 samples x 32 SNPs with SWAR 4x4 transposes.
+constexpr int kSliceWords = 64;                      // 1024 samples per transpose CTA
+constexpr int kSliceBytes = kSliceWords * 4;
+constexpr int kRowStride = kSliceWords + 1;          // words per staged record row
+constexpr int kStagedWords = 4 * kTileCols * kRowStride + 32;
+
+// Pass 1: SNP-major records -> canonical quads, gathering the selected samples. One CTA per
+// (quad of 128 columns, slice of 1024 samples): it stages 128 record slices of 256 bytes
+// (coalesced 128-bit loads), then thread (word w, tile sub) transposes 16 samples x 32
+// columns with SWAR 4x4 transposes; the four threads of a sample write its 32-byte sector
+// together. Slice 0 also computes each column's centre c_s: the pooled frequency of the
+// called genotypes among the record's first 256 samples, rounded to 1/256 (f2 is exact for
+// any per-SNP centre; this one only keeps the operand magnitudes small).
 __global__ void __launch_bounds__(kTransThreads)
 transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t n_ind,
-                    const TileInfo* __restrict__ tiles, const int32_t* __restrict__ pos, int64_t n_sel,
-                    uint64_t* __restrict__ canon, float* __restrict__ center, uint32_t words_per_row,
-                    uint32_t stride_words) {
-    extern __shared__ __align__(16) uint32_t srec[];
-    __shared__ int s_sum[kTileCols], s_cnt[kTileCols];
-    const int64_t t = blockIdx.x;
-    const TileInfo ti = tiles[t];
-    const uint32_t vec_per_row = (words_per_row + 3) / 4;
-    for (uint32_t c = threadIdx.x; c < kTileCols * vec_per_row; c += blockDim.x) {
-        const uint32_t r = c / vec_per_row, k = c - r * vec_per_row;
+                    const TileInfo* __restrict__ tiles, int64_t n_tiles, const int32_t* __restrict__ pos,
+                    int64_t n_sel, uint64_t* __restrict__ canon, double* __restrict__ center) {
+    __shared__ uint32_t srec[kStagedWords];
+    const int64_t q = blockIdx.x;
+    const int64_t slice = blockIdx.y;
+    const uint64_t byte0 = static_cast<uint64_t>(slice) * kSliceBytes;
+    // Stage: 4 tiles x 32 rows x 256 bytes; row (sub, r) at word (sub*32 + r)*kRowStride + sub*8
+    // (the sub*8 skew keeps the threads of one warp on distinct banks).
+    for (int c = threadIdx.x; c < 4 * kTileCols * (kSliceBytes / 16); c += blockDim.x) {
+        const int row = c / (kSliceBytes / 16), k = c % (kSliceBytes / 16);
+        const int sub = row / kTileCols, r = row % kTileCols;
+        const int64_t t = 4 * q + sub;
         uint4 v = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
-        if (static_cast<int>(r) < ti.nvalid)
-            v = __ldg(reinterpret_cast<const uint4*>(records + (static_cast<int64_t>(ti.snp0) + r) * pitch) + k);
-        uint32_t* d = srec + r * stride_words + k * 4;
+        if (t < n_tiles) {
+            const TileInfo ti = tiles[t];
+            const uint64_t b = byte0 + static_cast<uint64_t>(k) * 16;
+            if (r < ti.nvalid && b < pitch)
+                v = __ldg(reinterpret_cast<const uint4*>(records + (static_cast<int64_t>(ti.snp0) + r) * pitch + b));
+        }
+        uint32_t* d = srec + (sub * kTileCols + r) * kRowStride + sub * 8 + k * 4;
         d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
     }
     __syncthreads();
 
-    const int lane = threadIdx.x & 31;
-    // Centre of each column: pooled frequency of the called genotypes among the record's
-    // first 256 samples (warp 0; lane l reads 16 samples). Any per-SNP centre keeps f2
-    // exact; this one only has to be close to the population frequencies.
-    if (threadIdx.x < 32) {
-        const uint32_t w = static_cast<uint32_t>(lane);
-        const int64_t r0 = static_cast<int64_t>(w) * 16;
-        const int64_t rem = n_ind - r0;
-        const int nv = (w < words_per_row && w < 16) ? static_cast<int>(rem < 16 ? rem : 16) : 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (slice == 0 && warp < 4) {
+        const int sub = warp;
+        const int64_t t = 4 * q + sub;
+        const int nvalid = t < n_tiles ? tiles[t].nvalid : 0;
+        const int64_t rem = n_ind - static_cast<int64_t>(lane) * 16;
+        const int nv = lane < 16 ? static_cast<int>(rem < 0 ? 0 : (rem < 16 ? rem : 16)) : 0;
         uint32_t vmask = 0;
         for (int m = 0; m < nv; ++m) vmask |= 3u << (8 * (m >> 2) + 6 - 2 * (m & 3));
         for (int r = 0; r < kTileCols; ++r) {
-            const uint32_t x = (nv > 0 ? srec[r * stride_words + w] : 0u) & vmask;
+            const uint32_t x = (nv > 0 ? srec[(sub * kTileCols + r) * kRowStride + sub * 8 + lane] : 0u) & vmask;
             const uint32_t lo = x & 0x55555555u, hi = (x >> 1) & 0x55555555u;
             const uint32_t miss = lo & hi;
             const int cnt = __reduce_add_sync(0xffffffffu, __popc(vmask & 0x55555555u) - __popc(miss));
             const int sum = __reduce_add_sync(0xffffffffu, __popc(lo & ~miss) + 2 * __popc(hi & ~miss));
-            if (lane == 0) {
-                s_cnt[r] = cnt;
-                s_sum[r] = sum;
-            }
+            if (lane == 0 && t < n_tiles)
+                center[t * kTileCols + r] =
+                    (r < nvalid && cnt > 0) ? rint((static_cast<double>(sum) / (2.0 * cnt)) * 256.0) / 256.0 : 0.5;
         }
     }
-    for (uint32_t w = threadIdx.x; w < words_per_row; w += blockDim.x) {
-        // Valid samples of this word (the record's last word may be partial).
-        const int64_t r0 = static_cast<int64_t>(w) * 16;
+
+    const int sub = threadIdx.x & 3;
+    for (int wl = threadIdx.x >> 2; wl < kSliceWords; wl += blockDim.x >> 2) {
+        const int64_t r0 = slice * (kSliceWords * 16) + static_cast<int64_t>(wl) * 16;
         const int64_t rem = n_ind - r0;
+        if (rem <= 0) break;
         const int nv = static_cast<int>(rem < 16 ? rem : 16);
         uint64_t out[16];
 #pragma unroll
         for (int m = 0; m < 16; ++m) out[m] = 0;
+        const uint32_t* base = srec + sub * kTileCols * kRowStride + sub * 8 + wl;
 #pragma unroll
         for (int rg = 0; rg < kTileCols / 4; ++rg) {
             uint32_t rw[4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) rw[r] = srec[(4 * rg + r) * stride_words + w];
+            for (int r = 0; r < 4; ++r) rw[r] = base[(4 * rg + r) * kRowStride];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const uint32_t sel = static_cast<uint32_t>(j) | (static_cast<uint32_t>(j + 4) << 4);
@@ -269,9 +284,9 @@ transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t
         int32_t g[16];
         if (nv == 16) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int4 v = __ldg(reinterpret_cast<const int4*>(pos + r0) + q);
-                g[4 * q] = v.x; g[4 * q + 1] = v.y; g[4 * q + 2] = v.z; g[4 * q + 3] = v.w;
+            for (int k = 0; k < 4; ++k) {
+                const int4 v = __ldg(reinterpret_cast<const int4*>(pos + r0) + k);
+                g[4 * k] = v.x; g[4 * k + 1] = v.y; g[4 * k + 2] = v.z; g[4 * k + 3] = v.w;
             }
         } else {
 #pragma unroll
@@ -279,38 +294,40 @@ transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t
         }
 #pragma unroll
         for (int m = 0; m < 16; ++m)
-            if (g[m] >= 0) canon[t * n_sel + g[m]] = out[m];
-    }
-    __syncthreads();
-    if (threadIdx.x < kTileCols) {
-        const int c = threadIdx.x;
-        const int cnt = s_cnt[c];
-        center[t * kTileCols + c] =
-            (c < ti.nvalid && cnt > 0) ? static_cast<float>(rint((static_cast<double>(s_sum[c]) / (2.0 * cnt)) * 256.0) / 256.0) : 0.5f;
+            if (g[m] >= 0) canon[(q * n_sel + g[m]) * 4 + sub] = out[m];
     }
 }
 
-// Pass 2: per (population, tile) thread, fold the population's samples into exact integer
-// counts for 32 columns at once (SWAR bytes: PRMT maps four 2-bit codes to four count
-// bytes through the sample's ploidy table), then write the operand planes for the 32
-// columns. Samples are read four at a time (one 32-byte sector of canonical tile t).
+// Pass 2: one CTA per (row tile of 128 populations, quad of 4 column tiles), one thread per
+// (tile, population): fold the population's samples into exact integer counts for the
+// tile's 32 columns at once (SWAR bytes: PRMT maps four 2-bit codes to four count bytes
+// through the sample's ploidy table), then write the operand planes of the 32 columns.
+// Lanes of a warp are 32 consecutive populations of one tile, so the stores fill adjacent
+// rows of one tile image; the column centres come from shared memory.
 template <OpFmt F>
 __global__ void __launch_bounds__(kDecThreads2)
 decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t n_sel,
                     const uint32_t* __restrict__ sel, const int32_t* __restrict__ pop_off, int P,
-                    const float* __restrict__ center, const double* __restrict__ rec_n,
+                    const double* __restrict__ center, const double* __restrict__ rec_n,
                     const double* __restrict__ rec_nm1, const int32_t* __restrict__ col_snp, OperandPlanes op,
                     int32_t* __restrict__ cnt_ac2, int32_t* __restrict__ cnt_n) {
     __shared__ uint16_t s_lut[256];
+    __shared__ double s_center[4 * kTileCols];
+    const int64_t q = blockIdx.x;
     for (int x = threadIdx.x; x < 256; x += blockDim.x) {
         uint32_t v = 0;
         for (int k = 0; k < 4; ++k) v |= ((static_cast<uint32_t>(x) >> (6 - 2 * k)) & 3u) << (4 * k);
         s_lut[x] = static_cast<uint16_t>(v);
     }
+    for (int c = threadIdx.x; c < 4 * kTileCols; c += blockDim.x) {
+        const int64_t col = q * 4 * kTileCols + c;
+        s_center[c] = col < n_tiles * kTileCols ? __ldg(center + col) : 0.5;
+    }
     __syncthreads();
-    const int i = blockIdx.y;
-    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= n_tiles) return;
+    const int sub = threadIdx.x >> 7;                       // tile within the quad
+    const int i = blockIdx.y * kTileRows + (threadIdx.x & 127);
+    const int64_t t = 4 * q + sub;
+    if (i >= P || t >= n_tiles) return;
     const int g0 = __ldg(pop_off + i), g1 = __ldg(pop_off + i + 1);
 
     uint32_t acc[kTileCols];  // ac2 | n << 16 per column
@@ -320,21 +337,17 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
 #pragma unroll
     for (int k = 0; k < 8; ++k) sa[k] = sn[k] = 0;
     int pending = 0;
-    const uint64_t* row = canon + t * n_sel;
-    for (int gb = g0 & ~3; gb < g1; gb += 4) {
-        const uint4 v0 = __ldg(reinterpret_cast<const uint4*>(row + gb));
-        const uint4 v1 = __ldg(reinterpret_cast<const uint4*>(row + gb) + 1);
-        const uint32_t w[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const int g = gb + m;
-            if (g < g0 || g >= g1) continue;
+    const uint64_t* col = canon + q * n_sel * 4 + sub;
+    for (int g = g0; g < g1; ++g) {
+        {
+            const uint64_t x = __ldg(col + static_cast<int64_t>(g) * 4);
+            const uint32_t w[2] = {static_cast<uint32_t>(x), static_cast<uint32_t>(x >> 32)};
             const uint32_t pl = __ldg(sel + g) & 3u;
             const uint32_t la = pl == 2 ? 0x00040200u : (pl == 1 ? 0x00020100u : 0u);
             const uint32_t ln = pl == 2 ? 0x00020202u : (pl == 1 ? 0x00010101u : 0u);
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                const uint32_t byte = (w[2 * m + (k >> 2)] >> (8 * (k & 3))) & 0xFFu;
+                const uint32_t byte = (w[k >> 2] >> (8 * (k & 3))) & 0xFFu;
                 const uint32_t s16 = s_lut[byte];
                 sa[k] += __byte_perm(la, 0, s16);
                 sn[k] += __byte_perm(ln, 0, s16);
@@ -369,6 +382,7 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
         }
     }
     if (!op.planes) return;
+    const double* cen = s_center + sub * kTileCols;
 #pragma unroll
     for (int c8 = 0; c8 < kTileCols; c8 += 8) {
         Terms8 tm;
@@ -377,11 +391,13 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
         for (int c = 0; c < 8; ++c) {
             const uint32_t n = acc[c8 + c] >> 16, a2 = acc[c8 + c] & 0xFFFFu;
             // Terms in FP64 (q from the exact counts), rounded once to FP32 for the planes.
+            // a2 -> double through the 2^52 trick (an FP64 add, no conversion unit).
             double pt = 0.0, ah = 0.0;
             if (n > 0) {
-                const double q = static_cast<double>(a2) * 0.5 * __ldg(rec_n + n);
-                const double h = q * (1.0 - q) * __ldg(rec_nm1 + n);
-                pt = q - static_cast<double>(__ldg(center + col0 + c8 + c));
+                const double a2d = __hiloint2double(0x43300000, static_cast<int>(a2)) - 4503599627370496.0;
+                const double qf = a2d * 0.5 * __ldg(rec_n + n);
+                const double h = qf * (1.0 - qf) * __ldg(rec_nm1 + n);
+                pt = qf - cen[c8 + c];
                 ah = 0.5 * (pt * pt - h);
                 tm.mbits |= 1u << c;
             }
@@ -506,31 +522,23 @@ void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int
 }
 
 void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_ind, const TileInfo* tiles,
-                         int64_t n_tiles, const int32_t* pos, int64_t n_sel, uint64_t* canon, float* center,
+                         int64_t n_tiles, const int32_t* pos, int64_t n_sel, uint64_t* canon, double* center,
                          cudaStream_t s) {
     if (n_tiles <= 0) return;
-    const uint32_t words = static_cast<uint32_t>((n_ind + 15) / 16);
-    const uint32_t vec_per_row = (words + 3) / 4;
-    if (static_cast<uint64_t>(vec_per_row) * 16 > pitch || pitch % 16 != 0 ||
-        reinterpret_cast<uintptr_t>(records) % 16 != 0)
-        fail(STP_INVALID_ARGUMENT, "transpose: genotype records need a 16-byte aligned pitch covering the samples");
-    uint32_t stride = vec_per_row * 4 + 1;  // odd word stride: conflict-free column reads
-    const size_t smem = static_cast<size_t>(kTileCols) * stride * 4;
-    if (smem > 220 * 1024)
-        fail(STP_INVALID_ARGUMENT, "transpose: genotype record of " + std::to_string(pitch) +
-                                       " bytes exceeds the 32-record shared-memory tile");
-    STPF2_CUDA(cudaFuncSetAttribute(transpose_pa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int threads = static_cast<int>(std::min<uint32_t>(kTransThreads, (words + 31) / 32 * 32));
-    transpose_pa_kernel<<<static_cast<unsigned>(n_tiles), threads, smem, s>>>(records, pitch, n_ind, tiles, pos, n_sel,
-                                                                             canon, center, words, stride);
+    if (pitch % 16 != 0 || reinterpret_cast<uintptr_t>(records) % 16 != 0)
+        fail(STP_INVALID_ARGUMENT, "transpose: genotype records need a 16-byte aligned pitch");
+    const int64_t n_quads = (n_tiles + 3) / 4;
+    const int64_t n_slices = std::max<int64_t>(1, (n_ind + kSliceWords * 16 - 1) / (kSliceWords * 16));
+    if (n_slices > 65535) fail(STP_INVALID_ARGUMENT, "transpose: too many samples in a record");
+    const dim3 grid(static_cast<unsigned>(n_quads), static_cast<unsigned>(n_slices));
+    transpose_pa_kernel<<<grid, kTransThreads, 0, s>>>(records, pitch, n_ind, tiles, n_tiles, pos, n_sel, canon, center);
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
 }
 
 void launch_decode_canon(Ctx& c, const CanonDecodeArgs& a, cudaStream_t s) {
     if (a.P <= 0 || a.n_tiles <= 0) return;
-    const dim3 grid(static_cast<unsigned>((a.n_tiles + kDecThreads2 - 1) / kDecThreads2), static_cast<unsigned>(a.P));
-    if (a.P > 65535) fail(STP_INVALID_ARGUMENT, "more than 65535 populations");
+    const dim3 grid(static_cast<unsigned>((a.n_tiles + 3) / 4), static_cast<unsigned>((a.P + kTileRows - 1) / kTileRows));
 #define STPF2_DECODE_ARGS a.canon, a.n_tiles, a.n_sel, a.sel, a.pop_off, a.P, a.center, a.rec_n, a.rec_nm1, a.col_snp, a.op, a.cnt_ac2, a.cnt_n
     switch (a.op.fmt) {
         case OpFmt::F32: decode_canon_kernel<OpFmt::F32><<<grid, kDecThreads2, 0, s>>>(STPF2_DECODE_ARGS); break;

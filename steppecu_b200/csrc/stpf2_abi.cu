@@ -265,15 +265,15 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
     upload(p->tiles, tiles, s);
     upload(p->col_snp, col_snp, s);
     p->n_sel_pad = (n_sel + 3) / 4 * 4;
-    p->canon.reserve(std::max<size_t>(static_cast<size_t>(p->n_tiles) * p->n_sel_pad * 8, 64));
-    p->center.reserve(std::max<size_t>(static_cast<size_t>(p->L.ld) * 4, 64));
+    p->canon.reserve(std::max<size_t>(static_cast<size_t>((p->n_tiles + 3) / 4) * p->n_sel_pad * 32, 64));
+    p->center.reserve(std::max<size_t>(static_cast<size_t>(p->L.ld) * 8, 64));
 
     // The transpose reads records with 16-byte loads: records of another pitch are copied
     // once per run into a 16-byte pitch.
     p->bpr = r.geno.bytes_per_record;
     p->src_pitch = pitch;
     const uint64_t need_bytes = static_cast<uint64_t>((r.geno.n_ind + 63) / 64) * 16;
-    p->repitch = (pitch % 16 != 0) || pitch < need_bytes;
+    p->repitch = (pitch % 16 != 0) || pitch < need_bytes || (r.geno.on_device && reinterpret_cast<uintptr_t>(r.geno.records) % 16 != 0);
     if (p->repitch) {
         p->pitch = (std::max<uint64_t>(r.geno.bytes_per_record, need_bytes) + 15) / 16 * 16;
         p->repitched.reserve(std::max<size_t>(static_cast<size_t>(p->pitch) * r.geno.n_snp, 64));
@@ -312,7 +312,7 @@ void launch_decode(Plan& p, const uint8_t* d_records, int32_t* cnt_ac2, int32_t*
     }
     if (p.detect) launch_detect_ploidy_pa(c, rec, p.pitch, p.n_snp, p.sel.as<uint32_t>(), p.n_sel, s);
     launch_transpose_pa(c, rec, p.pitch, p.n_ind, p.tiles.as<TileInfo>(), p.n_tiles, p.pos.as<int32_t>(), p.n_sel_pad,
-                        p.canon.as<uint64_t>(), p.center.as<float>(), s);
+                        p.canon.as<uint64_t>(), p.center.as<double>(), s);
     CanonDecodeArgs a;
     a.canon = p.canon.as<uint64_t>();
     a.n_tiles = p.n_tiles;
@@ -320,7 +320,7 @@ void launch_decode(Plan& p, const uint8_t* d_records, int32_t* cnt_ac2, int32_t*
     a.sel = p.sel.as<uint32_t>();
     a.pop_off = p.pop_off.as<int32_t>();
     a.P = p.P;
-    a.center = p.center.as<float>();
+    a.center = p.center.as<double>();
     a.rec_n = p.rec_n.as<double>();
     a.rec_nm1 = p.rec_nm1.as<double>();
     a.col_snp = p.col_snp.as<int32_t>();

@@ -184,12 +184,12 @@ struct TileInfo {
 };
 
 struct CanonDecodeArgs {
-    const uint64_t* canon = nullptr;   // [n_tiles][n_sel] 8-byte canonical tiles
+    const uint64_t* canon = nullptr;   // [quads][n_sel][4] 8-byte canonical tile words
     int64_t n_tiles = 0, n_sel = 0;
     const uint32_t* sel = nullptr;     // [n_sel] descriptors (ploidy in the low bits)
     const int32_t* pop_off = nullptr;  // [P+1]
     int P = 0;
-    const float* center = nullptr;     // [ld] per-column centre (a multiple of 1/256)
+    const double* center = nullptr;    // [ld] per-column centre (a multiple of 1/256)
     const double* rec_n = nullptr;     // [n_max+1] 1/n (0 at n = 0)
     const double* rec_nm1 = nullptr;   // [n_max+1] 1/max(n-1, 1)
     const int32_t* col_snp = nullptr;  // [ld] SNP of each column, -1 for padding
@@ -201,7 +201,7 @@ struct CanonDecodeArgs {
 void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_snp,
                              uint32_t* sel, int64_t n_sel, cudaStream_t s);
 void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_ind, const TileInfo* tiles,
-                         int64_t n_tiles, const int32_t* pos, int64_t n_sel, uint64_t* canon, float* center,
+                         int64_t n_tiles, const int32_t* pos, int64_t n_sel, uint64_t* canon, double* center,
                          cudaStream_t s);
 void launch_decode_canon(Ctx& c, const CanonDecodeArgs& a, cudaStream_t s);
 void launch_decode_canonical(Ctx& c, const uint8_t* packed, uint64_t bpr, int64_t n_snp,
