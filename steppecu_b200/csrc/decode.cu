@@ -22,7 +22,7 @@ namespace {
 
 constexpr int kTileCols = 32;      // columns per canonical tile (8 bytes per sample)
 constexpr int kTransThreads = 256; // transpose: (16 samples, tile) per thread
-constexpr int kDecThreads2 = 512;  // decode: (4 tiles) x (128 populations) per CTA
+constexpr int kDecThreads2 = 256;  // decode: (64 populations) x (4 tiles) per CTA
 constexpr int kPloidyWindow = 1000;  // decode_af.hpp:29 (kPloidyDetectSnps)
 
 // Per-element operand terms of one (pop, SNP) from its exact counts. q matches the
@@ -298,98 +298,162 @@ transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t
     }
 }
 
-// Pass 2: one CTA per (row tile of 128 populations, quad of 4 column tiles), one thread per
-// (tile, population): fold the population's samples into exact integer counts for the
-// tile's 32 columns at once (SWAR bytes: PRMT maps four 2-bit codes to four count bytes
-// through the sample's ploidy table), then write the operand planes of the 32 columns.
-// Lanes of a warp are 32 consecutive populations of one tile, so the stores fill adjacent
-// rows of one tile image; the column centres come from shared memory.
+// Pass 2: one CTA per (64 populations, quad of 4 column tiles), in two phases.
+//
+// Fold: a warp holds 8 populations x 4 tiles, lane = (population, tile), so the four lanes
+// of a population read one 32-byte sector of the quad per sample. Each thread folds its
+// population's samples into exact integer counts for its tile's 32 columns at once with
+// SWAR bytes: PRMT maps four 2-bit codes, taken as selector nibbles straight from the
+// masked code bits, to four count bytes through the sample's ploidy table (byte b of count
+// word k holds column dec_col(k, b)). Four sample loads stay in flight per thread. Counts
+// go to shared memory (byte lanes spill there every 60 samples).
+//
+// Emit: warp w takes its 8 populations again, now with lane = (population, 8-column chunk),
+// and walks the 4 tiles, so every 16-byte store instruction of a plane fills 8 whole
+// 64-byte rows (512 contiguous bytes) of one tile image.
+constexpr int kDecPops = 64;                        // populations per decode CTA
+constexpr int kDecUnroll = 4;                       // sample loads in flight per thread
+constexpr int kDecFlush = 60 / kDecUnroll;          // iterations between byte-lane spills
+constexpr int kCenterPitch = kTileCols + 1;         // doubles per tile of shared centres
+// Shared counts (ac2 | n << 16) of (tile t, column c, population p) at word
+// t * kCntTile + c * kCntCol + p: fold writes (fixed c; p, t vary) and emit reads (fixed
+// t, c; p and the chunk vary) both touch 32 distinct banks.
+constexpr int kCntCol = kDecPops + 1;
+constexpr int kCntTile = kTileCols * kCntCol + 8;
+constexpr size_t kDecSmemBytes = size_t(4) * kCntTile * 4;
+
+// Column (0..31 within the tile) that byte b of count word k accumulates. Word k = 4h + s
+// comes from half h of the 8 canonical bytes and selector s: s = 0 / 1 take the low 16 bits
+// of lo = w & 0x33333333 / hi = (w >> 2) & 0x33333333, s = 2 / 3 their high 16 bits; byte
+// k' of w holds columns 4k' .. 4k'+3 MSB-first, so lo's nibbles hold columns 4k'+3, 4k'+1
+// and hi's 4k'+2, 4k'.
+__host__ __device__ constexpr int dec_col(int k, int b) {
+    return 16 * (k >> 2) + 8 * ((k >> 1) & 1) + 4 * (b >> 1) + 2 * (1 - (b & 1)) + (1 - (k & 1));
+}
+
+// Adds one sample's codes for 32 columns (x: 8 canonical bytes) to the byte-lane sums.
+// pl is the sample's ploidy (1 pseudo-haploid, 2 diploid, 0 none); the tables map code
+// 0/1/2/3 to ac2 = (0, 1, 2, 0) * pl and n = (1, 1, 1, 0) * pl (decode_af.hpp:58-65).
+__device__ __forceinline__ void fold_sample(uint64_t x, uint32_t pl, uint32_t (&sa)[8], uint32_t (&sn)[8]) {
+    const uint32_t la = 0x00020100u * pl, ln = 0x00010101u * pl;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const uint32_t w = static_cast<uint32_t>(x >> (32 * h));
+        const uint32_t lo = w & 0x33333333u, hi = (w >> 2) & 0x33333333u;
+        const uint32_t sel[4] = {lo, hi, lo >> 16, hi >> 16};
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            sa[4 * h + s] += __byte_perm(la, 0, sel[s]);
+            sn[4 * h + s] += __byte_perm(ln, 0, sel[s]);
+        }
+    }
+}
+
+// Moves the byte-lane sums into the shared counts (adding to what an earlier spill left).
+__device__ __forceinline__ void spill_counts(uint32_t* cnt, bool add, uint32_t (&sa)[8], uint32_t (&sn)[8]) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            // ac2 byte b -> bits 0-7, n byte b -> bits 16-23
+            const uint32_t v = __byte_perm(sa[k], sn[k], b | ((4 + b) << 8)) & 0x00FF00FFu;
+            uint32_t* d = cnt + dec_col(k, b) * kCntCol;
+            *d = (add ? *d : 0u) + v;
+        }
+        sa[k] = sn[k] = 0;
+    }
+}
+
 template <OpFmt F>
-__global__ void __launch_bounds__(kDecThreads2)
+__global__ void __launch_bounds__(kDecThreads2, 4)
 decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t n_sel,
                     const uint32_t* __restrict__ sel, const int32_t* __restrict__ pop_off, int P,
                     const double* __restrict__ center, const double* __restrict__ rec_n,
                     const double* __restrict__ rec_nm1, const int32_t* __restrict__ col_snp, OperandPlanes op,
                     int32_t* __restrict__ cnt_ac2, int32_t* __restrict__ cnt_n) {
-    __shared__ uint16_t s_lut[256];
-    __shared__ double s_center[4 * kTileCols];
+    extern __shared__ uint32_t s_cnt[];
+    __shared__ double s_center[4 * kCenterPitch];
     const int64_t q = blockIdx.x;
-    for (int x = threadIdx.x; x < 256; x += blockDim.x) {
-        uint32_t v = 0;
-        for (int k = 0; k < 4; ++k) v |= ((static_cast<uint32_t>(x) >> (6 - 2 * k)) & 3u) << (4 * k);
-        s_lut[x] = static_cast<uint16_t>(v);
-    }
     for (int c = threadIdx.x; c < 4 * kTileCols; c += blockDim.x) {
         const int64_t col = q * 4 * kTileCols + c;
-        s_center[c] = col < n_tiles * kTileCols ? __ldg(center + col) : 0.5;
+        s_center[(c / kTileCols) * kCenterPitch + c % kTileCols] = col < n_tiles * kTileCols ? __ldg(center + col) : 0.5;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    {
+        const int sub = lane & 3, pl_ = warp * 8 + (lane >> 2);
+        const int i = blockIdx.y * kDecPops + pl_;
+        if (i < P && 4 * q + sub < n_tiles) {
+            const int g0 = __ldg(pop_off + i), g1 = __ldg(pop_off + i + 1);
+            uint32_t* cnt = s_cnt + sub * kCntTile + pl_;
+            uint32_t sa[8], sn[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) sa[k] = sn[k] = 0;
+            bool spilled = false;
+            int it = 0;
+            const uint64_t* col = canon + q * n_sel * 4 + sub;
+            int g = g0;
+            for (; g + kDecUnroll <= g1; g += kDecUnroll) {
+                uint64_t x[kDecUnroll];
+                uint32_t pl[kDecUnroll];
+#pragma unroll
+                for (int u = 0; u < kDecUnroll; ++u) {
+                    x[u] = __ldg(col + static_cast<int64_t>(g + u) * 4);
+                    pl[u] = __ldg(sel + g + u) & 3u;
+                }
+#pragma unroll
+                for (int u = 0; u < kDecUnroll; ++u) fold_sample(x[u], pl[u], sa, sn);
+                if (++it == kDecFlush) {  // byte lanes hold at most 63 samples x 4
+                    spill_counts(cnt, spilled, sa, sn);
+                    spilled = true;
+                    it = 0;
+                }
+            }
+            if (g < g1) {  // fewer than kDecUnroll samples left (at most 59 unspilled in all)
+                uint64_t x[kDecUnroll - 1];
+                uint32_t pl[kDecUnroll - 1];
+#pragma unroll
+                for (int u = 0; u < kDecUnroll - 1; ++u) {
+                    const bool ok = g + u < g1;
+                    x[u] = ok ? __ldg(col + static_cast<int64_t>(g + u) * 4) : ~0ull;
+                    pl[u] = ok ? (__ldg(sel + g + u) & 3u) : 0u;
+                }
+#pragma unroll
+                for (int u = 0; u < kDecUnroll - 1; ++u) fold_sample(x[u], pl[u], sa, sn);
+            }
+            spill_counts(cnt, spilled, sa, sn);
+        }
     }
     __syncthreads();
-    const int sub = threadIdx.x >> 7;                       // tile within the quad
-    const int i = blockIdx.y * kTileRows + (threadIdx.x & 127);
-    const int64_t t = 4 * q + sub;
-    if (i >= P || t >= n_tiles) return;
-    const int g0 = __ldg(pop_off + i), g1 = __ldg(pop_off + i + 1);
 
-    uint32_t acc[kTileCols];  // ac2 | n << 16 per column
+    const int r = lane & 7, chunk = lane >> 3;
+    const int pl_ = warp * 8 + r;
+    const int i = blockIdx.y * kDecPops + pl_;
+    if (i >= P) return;
+#pragma unroll 1
+    for (int sub = 0; sub < 4; ++sub) {
+        const int64_t t = 4 * q + sub;
+        if (t >= n_tiles) break;
+        const int64_t col0 = t * kTileCols + 8 * chunk;
+        const uint32_t* cnt = s_cnt + sub * kCntTile + (8 * chunk) * kCntCol + pl_;
+        const double* cen = s_center + sub * kCenterPitch + 8 * chunk;
+        if (cnt_ac2) {
 #pragma unroll
-    for (int c = 0; c < kTileCols; ++c) acc[c] = 0;
-    uint32_t sa[8], sn[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) sa[k] = sn[k] = 0;
-    int pending = 0;
-    const uint64_t* col = canon + q * n_sel * 4 + sub;
-    for (int g = g0; g < g1; ++g) {
-        {
-            const uint64_t x = __ldg(col + static_cast<int64_t>(g) * 4);
-            const uint32_t w[2] = {static_cast<uint32_t>(x), static_cast<uint32_t>(x >> 32)};
-            const uint32_t pl = __ldg(sel + g) & 3u;
-            const uint32_t la = pl == 2 ? 0x00040200u : (pl == 1 ? 0x00020100u : 0u);
-            const uint32_t ln = pl == 2 ? 0x00020202u : (pl == 1 ? 0x00010101u : 0u);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t byte = (w[k >> 2] >> (8 * (k & 3))) & 0xFFu;
-                const uint32_t s16 = s_lut[byte];
-                sa[k] += __byte_perm(la, 0, s16);
-                sn[k] += __byte_perm(ln, 0, s16);
-            }
-            if (++pending == 63) {  // byte lanes hold at most 63 samples x 4
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-#pragma unroll
-                    for (int b = 0; b < 4; ++b)
-                        acc[4 * k + b] += ((sa[k] >> (8 * b)) & 0xFFu) | (((sn[k] >> (8 * b)) & 0xFFu) << 16);
-                    sa[k] = sn[k] = 0;
+            for (int c = 0; c < 8; ++c) {
+                const int32_t s = __ldg(col_snp + col0 + c);
+                const uint32_t v = cnt[c * kCntCol];
+                if (s >= 0) {
+                    cnt_ac2[static_cast<int64_t>(i) + static_cast<int64_t>(P) * s] = static_cast<int32_t>(v & 0xFFFFu);
+                    cnt_n[static_cast<int64_t>(i) + static_cast<int64_t>(P) * s] = static_cast<int32_t>(v >> 16);
                 }
-                pending = 0;
             }
         }
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-            acc[4 * k + b] += ((sa[k] >> (8 * b)) & 0xFFu) | (((sn[k] >> (8 * b)) & 0xFFu) << 16);
-
-    const int64_t col0 = t * kTileCols;
-    if (cnt_ac2) {
-#pragma unroll
-        for (int c = 0; c < kTileCols; ++c) {
-            const int32_t s = __ldg(col_snp + col0 + c);
-            if (s >= 0) {
-                cnt_ac2[static_cast<int64_t>(i) + static_cast<int64_t>(P) * s] = static_cast<int32_t>(acc[c] & 0xFFFFu);
-                cnt_n[static_cast<int64_t>(i) + static_cast<int64_t>(P) * s] = static_cast<int32_t>(acc[c] >> 16);
-            }
-        }
-    }
-    if (!op.planes) return;
-    const double* cen = s_center + sub * kTileCols;
-#pragma unroll
-    for (int c8 = 0; c8 < kTileCols; c8 += 8) {
+        if (!op.planes) continue;
         Terms8 tm;
         tm.mbits = 0;
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
-            const uint32_t n = acc[c8 + c] >> 16, a2 = acc[c8 + c] & 0xFFFFu;
+            const uint32_t v = cnt[c * kCntCol];
+            const uint32_t n = v >> 16, a2 = v & 0xFFFFu;
             // Terms in FP64 (q from the exact counts), rounded once to FP32 for the planes.
             // a2 -> double through the 2^52 trick (an FP64 add, no conversion unit).
             double pt = 0.0, ah = 0.0;
@@ -397,14 +461,14 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
                 const double a2d = __hiloint2double(0x43300000, static_cast<int>(a2)) - 4503599627370496.0;
                 const double qf = a2d * 0.5 * __ldg(rec_n + n);
                 const double h = qf * (1.0 - qf) * __ldg(rec_nm1 + n);
-                pt = qf - cen[c8 + c];
+                pt = qf - cen[c];
                 ah = 0.5 * (pt * pt - h);
                 tm.mbits |= 1u << c;
             }
             tm.pt[c] = static_cast<float>(pt);
             tm.ah[c] = static_cast<float>(ah);
         }
-        emit8<F>(op, i, col0 + c8, tm);
+        emit8<F>(op, i, col0, tm);
     }
 }
 
@@ -538,12 +602,12 @@ void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t
 
 void launch_decode_canon(Ctx& c, const CanonDecodeArgs& a, cudaStream_t s) {
     if (a.P <= 0 || a.n_tiles <= 0) return;
-    const dim3 grid(static_cast<unsigned>((a.n_tiles + 3) / 4), static_cast<unsigned>((a.P + kTileRows - 1) / kTileRows));
+    const dim3 grid(static_cast<unsigned>((a.n_tiles + 3) / 4), static_cast<unsigned>((a.P + kDecPops - 1) / kDecPops));
 #define STPF2_DECODE_ARGS a.canon, a.n_tiles, a.n_sel, a.sel, a.pop_off, a.P, a.center, a.rec_n, a.rec_nm1, a.col_snp, a.op, a.cnt_ac2, a.cnt_n
     switch (a.op.fmt) {
-        case OpFmt::F32: decode_canon_kernel<OpFmt::F32><<<grid, kDecThreads2, 0, s>>>(STPF2_DECODE_ARGS); break;
-        case OpFmt::BF16: decode_canon_kernel<OpFmt::BF16><<<grid, kDecThreads2, 0, s>>>(STPF2_DECODE_ARGS); break;
-        case OpFmt::F16: decode_canon_kernel<OpFmt::F16><<<grid, kDecThreads2, 0, s>>>(STPF2_DECODE_ARGS); break;
+        case OpFmt::F32: decode_canon_kernel<OpFmt::F32><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS); break;
+        case OpFmt::BF16: decode_canon_kernel<OpFmt::BF16><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS); break;
+        case OpFmt::F16: decode_canon_kernel<OpFmt::F16><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS); break;
     }
 #undef STPF2_DECODE_ARGS
     STPF2_CUDA(cudaGetLastError());

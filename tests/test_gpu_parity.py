@@ -112,6 +112,26 @@ def test_decode_counts_device_records(ctx, uneven):
     assert np.array_equal(ac2, wa.reshape(-1, P).T) and np.array_equal(n, wn.reshape(-1, P).T)
 
 
+@pytest.mark.parametrize("size,n_pop,n_snp", [(250, 5, 3000), (16383, 1, 300)])
+def test_decode_counts_large_populations(ctx, size, n_pop, n_snp):
+    """Populations far above the decode's in-register sample window, up to the largest
+    population the 16-bit count packing admits (ac2 <= 2 * 16383)."""
+    import dataclasses
+
+    wl = dataclasses.replace(synth.WORKLOADS["c2"], name="large", n_pop=n_pop, ind_per_pop=size)
+    p = synth.generate(wl, seed=size, n_snp=n_snp)
+    sel, po = p.selection()
+    rec = p.records_numpy()
+    pl = oracle.detect_ploidy_pa(rec, sel)
+    ac2, n = ctx.decode_counts(rec, p.n_ind, sel, po)
+    wa, wn = oracle.decode_counts_pa(rec, sel, po, pl)
+    assert np.array_equal(ac2, wa.reshape(-1, n_pop).T) and np.array_equal(n, wn.reshape(-1, n_pop).T)
+    if n_pop > 1:
+        want, _ = oracle_f2(p, sel, po)
+        got = ctx.extract_blocks(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision=TC_DEFAULT)
+        assert_f2_close(got, want, TC_DEFAULT)
+
+
 @pytest.mark.parametrize("detect", [True, False])
 def test_decode_af_canonical_bitexact(ctx, uneven, detect):
     p, sel, po, _, _ = uneven
