@@ -82,14 +82,14 @@ __device__ __forceinline__ void emit(const OperandPlanes& op, int i, int64_t col
         const T ahl = to16<T>(ah - from16<T>(ahh));
         const int64_t tile = static_cast<int64_t>(i / kTileRows) * op.n_ck + col / kTileK;
         const int r = i % kTileRows, k = static_cast<int>(col % kTileK);
-        uint8_t* b = static_cast<uint8_t*>(op.planes) + tile * kTile16Bytes + tile16_offset(r, k);
-        const int64_t ps = static_cast<int64_t>(op.n_rt) * op.n_ck * kTile16Bytes;
+        uint8_t* img = static_cast<uint8_t*>(op.planes) + tile * kImageBytes;
+        uint8_t* b = img + tile16_offset(r, k);
         *reinterpret_cast<T*>(b) = pth;
-        *reinterpret_cast<T*>(b + ps) = ptl;
-        *reinterpret_cast<T*>(b + 2 * ps) = ahh;
-        *reinterpret_cast<T*>(b + 3 * ps) = ahl;
-        *reinterpret_cast<T*>(b + 4 * ps) = to16<T>(t.m);
-        op.m_u8[tile * kTile8Bytes + tile8_offset(r, k)] = static_cast<uint8_t>(t.m != 0.0);
+        *reinterpret_cast<T*>(b + kTile16Bytes) = ptl;
+        *reinterpret_cast<T*>(b + 2 * kTile16Bytes) = ahh;
+        *reinterpret_cast<T*>(b + 3 * kTile16Bytes) = ahl;
+        *reinterpret_cast<T*>(b + 4 * kTile16Bytes) = to16<T>(t.m);
+        img[5 * kTile16Bytes + tile8_offset(r, k)] = static_cast<uint8_t>(t.m != 0.0);
     }
 }
 
@@ -166,14 +166,14 @@ __device__ __forceinline__ void emit8(const OperandPlanes& op, int i, int64_t co
         }
         const int r = i % kTileRows, k = static_cast<int>(col % kTileK);
         const int64_t tile = static_cast<int64_t>(i / kTileRows) * op.n_ck + col / kTileK;
-        const int64_t ps = static_cast<int64_t>(op.n_rt) * op.n_ck * kTile16Bytes;
-        uint8_t* b = static_cast<uint8_t*>(op.planes) + tile * kTile16Bytes + tile16_offset(r, k);
+        uint8_t* img = static_cast<uint8_t*>(op.planes) + tile * kImageBytes;
+        uint8_t* b = img + tile16_offset(r, k);
         *reinterpret_cast<uint4*>(b) = ph;
-        *reinterpret_cast<uint4*>(b + ps) = pl;
-        *reinterpret_cast<uint4*>(b + 2 * ps) = ahh;
-        *reinterpret_cast<uint4*>(b + 3 * ps) = ahl;
-        *reinterpret_cast<uint4*>(b + 4 * ps) = mm;
-        *reinterpret_cast<uint2*>(op.m_u8 + tile * kTile8Bytes + tile8_offset(r, k)) = mv;
+        *reinterpret_cast<uint4*>(b + kTile16Bytes) = pl;
+        *reinterpret_cast<uint4*>(b + 2 * kTile16Bytes) = ahh;
+        *reinterpret_cast<uint4*>(b + 3 * kTile16Bytes) = ahl;
+        *reinterpret_cast<uint4*>(b + 4 * kTile16Bytes) = mm;
+        *reinterpret_cast<uint2*>(img + 5 * kTile16Bytes + tile8_offset(r, k)) = mv;
     }
 }
 

@@ -3,22 +3,26 @@
 // The tensor-core f2 contraction for sm_100a: one persistent, warp-specialised kernel
 // over every (jackknife block, 128x128 population tile pair ti <= tj) work item.
 //
-//   warp 0      producer: per 32-SNP stage, bulk-copies the pre-swizzled tile images of the
-//               5 split planes (Pt_hi, Pt_lo, Ah_hi, Ah_lo, M as 16-bit) and of the int8 M
-//               plane for the row tile and the column tile (one side on diagonal tiles);
-//               no tensor maps, no multicast.
+//   warp 0      producer: per 32-SNP stage, bulk-copies the pre-swizzled operand image of
+//               the row tile and of the column tile (one side on diagonal tiles): 44 KiB
+//               each, the 5 split planes (Pt_hi, Pt_lo, Ah_hi, Ah_lo, M as 16-bit) and the
+//               int8 M plane in one contiguous copy; no tensor maps, no multicast.
 //   warp 1      TMEM owner + single-thread tcgen05.mma issuer. Per 16-SNP K step, seven
 //               kind::f16 MMAs accumulate num/2 = sum(Ah_i M_j + M_i Ah_j - Pt_i Pt_j) over
 //               the hi/lo splits (the -Pt Pt products use the descriptor's A-negate bit)
-//               into an FP32 TMEM buffer; one kind::i8 MMA per stage accumulates the exact
-//               both-present count M M^T into an int32 TMEM buffer.
-//   warps 2-9   epilogue: every 32 SNPs, drain the FP32 buffer into FP64 registers
-//               (double-buffered TMEM, so the MMAs run on); at the end of the block, read
-//               vpair, form f2 = num / vpair (0 when vpair = 0, f2_estimator.hpp:42-46) in
-//               FP64 and store (i,j) and (j,i) of the block's slab.
+//               into one FP32 TMEM buffer per 32-SNP chunk; one kind::i8 MMA per stage
+//               accumulates the exact both-present count M M^T into an int32 TMEM buffer.
+//   warps 2-9   epilogue: drains the FP32 chunks two at a time into FP64 registers (one
+//               round-to-nearest FP32 add of the two chunk sums, then one FP32 -> FP64
+//               conversion and FP64 add; the conversions bound this loop, so pairing halves
+//               it); at the end of the block, reads vpair, forms f2 = num / vpair (0 when
+//               vpair = 0, f2_estimator.hpp:42-46) in FP64 and stores (i,j) and (j,i) of the
+//               block's slab.
 //
-// TMEM (512 columns): [0,128) and [128,256) FP32 numerator chunks, [256,384) and
-// [384,512) int32 vpair per tile. Every wait is bounded (a few seconds); on expiry the
+// TMEM (512 columns): a ring of three FP32 numerator chunk buffers at [0,128), [128,256),
+// [256,384) (the MMAs fill the third while a pair drains) and the int32 vpair of the
+// current tile at [384,512) (the issuer waits for the previous tile's vpair to be read
+// before the tile's first i8 MMA). Every wait is bounded (a few seconds); on expiry the
 // kernel raises an error flag the host turns into STP_DEVICE_TIMEOUT, lets its copies and
 // MMAs finish, frees TMEM and returns.
 #include <algorithm>
@@ -33,12 +37,14 @@ namespace {
 constexpr int kTile = 128;
 constexpr int kStageK = 32;        // SNP columns per pipeline stage
 constexpr int kStages = 2;
-constexpr int kDrainStages = 1;    // FP32 TMEM chunk = 32 SNPs, then FP64
+constexpr int kNumBufs = 3;        // FP32 chunk buffers in TMEM (one 32-SNP stage each)
+constexpr uint32_t kVpCol = kNumBufs * 128u;
 constexpr int kPlanes = 5;
 constexpr uint32_t kTile16 = kTile * kStageK * 2;                 // 8 KiB
 constexpr uint32_t kTile8 = kTile * kStageK;                      // 4 KiB
 constexpr uint32_t kSideBytes = kPlanes * kTile16 + kTile8;       // 44 KiB
 constexpr uint32_t kStageBytes = 2 * kSideBytes;                  // 88 KiB
+static_assert(kSideBytes == kImageBytes, "a stage side is one operand image");
 constexpr int kEpiWarps = 8;
 constexpr int kEpiWarp0 = 2;                        // epilogue = warps 2..9
 constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);  // 320
@@ -54,9 +60,7 @@ constexpr int kStageDoubles = 2 * kStageHalf;
 constexpr uint32_t kCtlBytes = 256;
 
 struct UmmaArgs {
-    const uint8_t* planes16;  // tiled 16-bit plane images (5 planes, plane_stride apart)
-    const uint8_t* plane8;    // tiled int8 M images
-    int64_t plane_stride;
+    const uint8_t* images;    // operand images, (row tile, chunk) at (t * n_ck + c) * kSideBytes
     int64_t n_ck;             // column chunks per row tile
     const WorkItem* items;
     int n_items;
@@ -71,8 +75,8 @@ struct UmmaArgs {
 
 struct SmemCtl {
     unsigned long long full[kStages], empty[kStages];
-    unsigned long long acc_full[2], acc_empty[2];
-    unsigned long long vp_full[2], vp_empty[2];
+    unsigned long long acc_full[kNumBufs], acc_empty[kNumBufs];
+    unsigned long long vp_full, vp_empty;
     unsigned long long drain;
     uint32_t tmem_base;
     volatile int abort;
@@ -178,6 +182,12 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         : "r"(taddr));
 }
 
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -217,16 +227,10 @@ __device__ void producer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl) {
                 mbar_expect_tx(&ctl->full[slot], diag ? kSideBytes : kStageBytes);
                 const int64_t chunk = bi.col / kStageK + st;
                 const int64_t ta = static_cast<int64_t>(w.ti) * a.n_ck + chunk;
-                for (int p = 0; p < kPlanes; ++p)
-                    bulk_load(sb + p * kTile16, a.planes16 + p * a.plane_stride + ta * kTile16, kTile16, &ctl->full[slot]);
-                bulk_load(sb + kPlanes * kTile16, a.plane8 + ta * kTile8, kTile8, &ctl->full[slot]);
+                bulk_load(sb, a.images + ta * kSideBytes, kSideBytes, &ctl->full[slot]);
                 if (!diag) {
-                    uint8_t* sbb = sb + kSideBytes;
                     const int64_t tb = static_cast<int64_t>(w.tj) * a.n_ck + chunk;
-                    for (int p = 0; p < kPlanes; ++p)
-                        bulk_load(sbb + p * kTile16, a.planes16 + p * a.plane_stride + tb * kTile16, kTile16,
-                                  &ctl->full[slot]);
-                    bulk_load(sbb + kPlanes * kTile16, a.plane8 + tb * kTile8, kTile8, &ctl->full[slot]);
+                    bulk_load(sb + kSideBytes, a.images + tb * kSideBytes, kSideBytes, &ctl->full[slot]);
                 }
             }
         }
@@ -246,20 +250,13 @@ __device__ void mma_issuer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl, uint3
         const int nst = stages_of(bi.k);
         if (nst == 0) continue;
         const bool diag = w.ti == w.tj;
-        const int vb = static_cast<int>(is & 1u);
-        if (!wait_bounded(&ctl->vp_empty[vb], ((is >> 1) & 1u) ^ 1u, ctl, a.err)) goto done;
-        tc_fence_after();
         {
-            const uint32_t d_vp = tmem + 256u + static_cast<uint32_t>(vb) * 128u;
-            uint32_t d_num = tmem;
-            int nb = 0;
-            for (int st = 0; st < nst; ++st, ++g) {
-                if (st % kDrainStages == 0) {
-                    nb = static_cast<int>(cs & 1u);
-                    if (!wait_bounded(&ctl->acc_empty[nb], ((cs >> 1) & 1u) ^ 1u, ctl, a.err)) goto done;
-                    tc_fence_after();
-                    d_num = tmem + static_cast<uint32_t>(nb) * 128u;
-                }
+            const uint32_t d_vp = tmem + kVpCol;
+            for (int st = 0; st < nst; ++st, ++g, ++cs) {
+                const int nb = static_cast<int>(cs % kNumBufs);
+                if (!wait_bounded(&ctl->acc_empty[nb], ((cs / kNumBufs) & 1u) ^ 1u, ctl, a.err)) goto done;
+                tc_fence_after();
+                const uint32_t d_num = tmem + static_cast<uint32_t>(nb) * 128u;
                 const int slot = static_cast<int>(g % kStages);
                 if (!wait_bounded(&ctl->full[slot], (g / kStages) & 1u, ctl, a.err)) goto done;
                 tc_fence_after();
@@ -278,7 +275,7 @@ __device__ void mma_issuer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl, uint3
                     const uint64_t bAh = smem_desc(sb + 2 * kTile16 + ko, 512, 4);
                     const uint64_t bAl = smem_desc(sb + 3 * kTile16 + ko, 512, 4);
                     const uint64_t bM = smem_desc(sb + 4 * kTile16 + ko, 512, 4);
-                    const uint32_t first = (st % kDrainStages == 0 && k == 0) ? 0u : 1u;
+                    const uint32_t first = k == 0 ? 0u : 1u;
                     // Large terms first and interleaved in sign, the lo corrections last.
                     mma_f16(d_num, aAh, bM, a.idesc_am, first);
                     mma_f16(d_num, aPh, bPh, a.idesc_pp, 1u);
@@ -288,15 +285,16 @@ __device__ void mma_issuer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl, uint3
                     mma_f16(d_num, aAl, bM, a.idesc_am, 1u);
                     mma_f16(d_num, aM, bAl, a.idesc_am, 1u);
                 }
+                if (st == 0) {  // the previous tile's vpair has been read
+                    if (!wait_bounded(&ctl->vp_empty, (is & 1u) ^ 1u, ctl, a.err)) goto done;
+                    tc_fence_after();
+                }
                 mma_i8(d_vp, smem_desc(sa + kPlanes * kTile16, 256, 6), smem_desc(sb + kPlanes * kTile16, 256, 6),
                        a.idesc_i8, st > 0 ? 1u : 0u);
                 mma_commit(&ctl->empty[slot]);
-                if (st % kDrainStages == kDrainStages - 1 || st == nst - 1) {
-                    mma_commit(&ctl->acc_full[nb]);
-                    ++cs;
-                }
+                mma_commit(&ctl->acc_full[nb]);
             }
-            mma_commit(&ctl->vp_full[vb]);
+            mma_commit(&ctl->vp_full);
             ++is;
         }
     }
@@ -337,38 +335,47 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
         }
 #pragma unroll
         for (int c = 0; c < 64; ++c) acc[c] = 0.0;
-        const int nch = (nst + kDrainStages - 1) / kDrainStages;
-        for (int ch = 0; ch < nch; ++ch) {
-            const int nb = static_cast<int>(cs & 1u);
+        for (int ch = 0; ch < nst; ch += 2) {
+            const bool pair = ch + 1 < nst;
+            const int nb0 = static_cast<int>(cs % kNumBufs), nb1 = static_cast<int>((cs + 1) % kNumBufs);
             bool ok = true;
-            if (lane == 0) ok = wait_bounded(&ctl->acc_full[nb], (cs >> 1) & 1u, ctl, a.err);
+            if (lane == 0) {
+                ok = wait_bounded(&ctl->acc_full[nb0], (cs / kNumBufs) & 1u, ctl, a.err);
+                if (ok && pair) ok = wait_bounded(&ctl->acc_full[nb1], ((cs + 1) / kNumBufs) & 1u, ctl, a.err);
+            }
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) return;
             tc_fence_after();
-            const uint32_t base = tmem + lane_addr + static_cast<uint32_t>(nb) * 128u + static_cast<uint32_t>(h) * 64u;
+            const uint32_t b0 = tmem + lane_addr + static_cast<uint32_t>(nb0) * 128u + static_cast<uint32_t>(h) * 64u;
+            // A lone last chunk reads its buffer twice and adds zero (exact).
+            const uint32_t b1 = pair ? tmem + lane_addr + static_cast<uint32_t>(nb1) * 128u + static_cast<uint32_t>(h) * 64u : b0;
+            const float w1 = pair ? 1.0f : 0.0f;
 #pragma unroll
-            for (int q16 = 0; q16 < 4; ++q16) {
-                uint32_t v[16];
-                tmem_ld16(base + static_cast<uint32_t>(q16) * 16u, v);
+            for (int q8 = 0; q8 < 8; ++q8) {
+                uint32_t v0[8], v1[8];
+                tmem_ld8(b0 + static_cast<uint32_t>(q8) * 8u, v0);
+                tmem_ld8(b1 + static_cast<uint32_t>(q8) * 8u, v1);
                 tmem_wait_ld();
 #pragma unroll
-                for (int c = 0; c < 16; ++c)
-                    acc[q16 * 16 + c] += static_cast<double>(__uint_as_float(v[c]));
+                for (int c = 0; c < 8; ++c)
+                    acc[q8 * 8 + c] += static_cast<double>(__fmaf_rn(w1, __uint_as_float(v1[c]), __uint_as_float(v0[c])));
             }
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&ctl->acc_empty[nb]);
-            ++cs;
+            if (lane == 0) {
+                mbar_arrive(&ctl->acc_empty[nb0]);
+                if (pair) mbar_arrive(&ctl->acc_empty[nb1]);
+            }
+            cs += pair ? 2u : 1u;
         }
-        const int vb = static_cast<int>(is & 1u);
         {
             bool ok = true;
-            if (lane == 0) ok = wait_bounded(&ctl->vp_full[vb], (is >> 1) & 1u, ctl, a.err);
+            if (lane == 0) ok = wait_bounded(&ctl->vp_full, is & 1u, ctl, a.err);
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) return;
         }
         tc_fence_after();
-        const uint32_t vbase = tmem + lane_addr + 256u + static_cast<uint32_t>(vb) * 128u + static_cast<uint32_t>(h) * 64u;
+        const uint32_t vbase = tmem + lane_addr + kVpCol + static_cast<uint32_t>(h) * 64u;
         // Output: (i, j) straight from registers (32 consecutive i per store: full sectors);
         // (j, i) through this warp's staging tile, so each store covers 4 rows x 8
         // consecutive j (64-byte segments) instead of 32 scattered 8-byte pieces.
@@ -383,7 +390,7 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
             if (q16 == 3) {
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&ctl->vp_empty[vb]);
+                if (lane == 0) mbar_arrive(&ctl->vp_empty);
             }
 #pragma unroll
             for (int cg = 0; cg < 16; cg += 8) {
@@ -432,12 +439,12 @@ f2_umma_kernel(const __grid_constant__ UmmaArgs a) {
             mbar_init(&ctl->full[s], 1);
             mbar_init(&ctl->empty[s], 1);
         }
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < kNumBufs; ++b) {
             mbar_init(&ctl->acc_full[b], 1);
             mbar_init(&ctl->acc_empty[b], kEpiWarps);
-            mbar_init(&ctl->vp_full[b], 1);
-            mbar_init(&ctl->vp_empty[b], kEpiWarps);
         }
+        mbar_init(&ctl->vp_full, 1);
+        mbar_init(&ctl->vp_empty, kEpiWarps);
         mbar_init(&ctl->drain, 1);
         ctl->abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -483,9 +490,8 @@ constexpr size_t kSmemBytes = kStages * kStageBytes + kCtlBytes + kEpiWarps * kS
 }  // namespace
 
 struct UmmaPlan {
-    const uint8_t* planes16 = nullptr;
-    const uint8_t* plane8 = nullptr;
-    int64_t plane_stride = 0, n_ck = 0;
+    const uint8_t* images = nullptr;
+    int64_t n_ck = 0;
     DevBuf items, blocks, err;
     int n_items = 0;
     int P = 0;
@@ -513,10 +519,8 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
     STPF2_CUDA(cudaMemsetAsync(p->err.ptr, 0, 16, c.stream));
 
     if (op.n_rt <= 0 || op.n_ck <= 0) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs tiled planes");
-    p->planes16 = static_cast<const uint8_t*>(op.planes);
-    p->plane8 = op.m_u8;
+    p->images = static_cast<const uint8_t*>(op.planes);
     p->n_ck = op.n_ck;
-    p->plane_stride = static_cast<int64_t>(op.n_rt) * op.n_ck * kTile16;
     STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kSmemBytes)));
     return p.release();
@@ -527,9 +531,7 @@ void umma_plan_destroy(UmmaPlan* p) { delete p; }
 void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s) {
     if (!p || p->n_items <= 0) return;
     UmmaArgs a{};
-    a.planes16 = p->planes16;
-    a.plane8 = p->plane8;
-    a.plane_stride = p->plane_stride;
+    a.images = p->images;
     a.n_ck = p->n_ck;
     a.items = p->items.as<WorkItem>();
     a.n_items = p->n_items;

@@ -123,7 +123,7 @@ size_t operand_plane_bytes(OpFmt f, int P, int64_t ld) {
         return align256(2 * pl * 4) + align256(pl);
     }
     const size_t tiles = static_cast<size_t>((P + kTileRows - 1) / kTileRows) * static_cast<size_t>(ld / kTileK);
-    return align256(5 * tiles * kTile16Bytes) + align256(tiles * kTile8Bytes);
+    return align256(tiles * kImageBytes);
 }
 
 void bind_operand_planes(OperandPlanes& op, OpFmt f, int P, int64_t ld, void* base) {
@@ -140,8 +140,7 @@ void bind_operand_planes(OperandPlanes& op, OpFmt f, int P, int64_t ld, void* ba
     } else {
         op.n_rt = (P + kTileRows - 1) / kTileRows;
         op.n_ck = ld / kTileK;
-        const size_t tiles = static_cast<size_t>(op.n_rt) * static_cast<size_t>(op.n_ck);
-        op.m_u8 = static_cast<uint8_t*>(base) + align256(5 * tiles * kTile16Bytes);
+        op.m_u8 = nullptr;  // the int8 M tiles live inside the operand images
     }
 }
 

@@ -124,25 +124,26 @@ inline OpFmt fmt_of(int precision) {
     fail(STP_INVALID_ARGUMENT, "unknown precision mode " + std::to_string(precision));
 }
 
-// Where decode/feeder write. For F32: planes = [Pt f32][Ah f32] (2 planes) + m_u8.
-// For BF16/F16: planes = 16-bit [Pt_hi][Pt_lo][Ah_hi][Ah_lo][M] (5 planes) + m_u8 (int8 M).
-// Plane p, row i, column c at planes + (p * P + i) * ld + c (elements of the plane type).
+// Where decode/feeder write. For F32: planes = [Pt f32][Ah f32] (2 planes) + m_u8, plane
+// p, row i, column c at planes + (p * P + i) * ld + c. For BF16/F16: 16-bit [Pt_hi][Pt_lo]
+// [Ah_hi][Ah_lo][M] and int8 M, tiled into operand images (below).
 // Pt = m*(q - c_s), Ah = m*((q - c_s)^2 - h)/2, h = q(1-q)/max(n-1,1), m = [n > 0];
 // then num(i,j) = 2 * sum_s (Ah_i M_j + M_i Ah_j - Pt_i Pt_j).
 //
-// The 16-bit planes (and their int8 M plane) are TILED for the tensor cores: populations
-// in row tiles of 128, columns in chunks of 32, and every (row tile, chunk) stored as one
-// contiguous image of exactly what the MMA reads from shared memory: 128 rows x 64 bytes
-// with the 64-byte swizzle (16-byte chunk index XOR (row / 2) % 4) for 16-bit planes,
-// 128 rows x 32 bytes with the 32-byte swizzle (chunk XOR (row / 4) % 2) for int8. A
-// pipeline stage is then a handful of contiguous 8 KiB / 4 KiB bulk copies. Rows past P
-// stay zero. The FP32 planes of the SIMT contraction stay row-major.
+// The 16-bit planes and the int8 M plane are TILED for the tensor cores: populations in
+// row tiles of 128, columns in chunks of 32, and every (row tile, chunk) stored as ONE
+// contiguous 44 KiB operand image holding exactly what the MMAs read from shared memory:
+// the five 16-bit tiles [Pt_hi][Pt_lo][Ah_hi][Ah_lo][M] (128 rows x 64 bytes each, 64-byte
+// swizzle: 16-byte chunk index XOR (row / 2) % 4), then the int8 M tile (128 rows x 32
+// bytes, 32-byte swizzle: chunk XOR (row / 4) % 2). Image (row tile t, chunk c) sits at
+// planes + (t * n_ck + c) * kImageBytes, so one side of a pipeline stage is a single bulk
+// copy. Rows past P stay zero. The FP32 planes of the SIMT contraction stay row-major.
 struct OperandPlanes {
     OpFmt fmt = OpFmt::F32;
     int P = 0;
     int64_t ld = 0;
     void* planes = nullptr;
-    uint8_t* m_u8 = nullptr;
+    uint8_t* m_u8 = nullptr;  // FP32 form only: row-major int8 M
     double scale_inv = 1.0;  // numerator scale undo (F16 planes are pre-scaled)
     int n_rt = 0;            // tiled: row tiles of 128 populations
     int64_t n_ck = 0;        // tiled: column chunks of 32
@@ -152,6 +153,7 @@ constexpr int kTileRows = 128;
 constexpr int kTileK = 32;
 constexpr int64_t kTile16Bytes = kTileRows * kTileK * 2;  // one 16-bit tile image
 constexpr int64_t kTile8Bytes = kTileRows * kTileK;       // one int8 tile image
+constexpr int64_t kImageBytes = 5 * kTile16Bytes + kTile8Bytes;  // one operand image (44 KiB)
 
 // Byte offset of element (row r < 128, column k < 32) inside a 16-bit / int8 tile image.
 __host__ __device__ inline uint32_t tile16_offset(int r, int k) {
