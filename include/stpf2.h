@@ -108,6 +108,14 @@ uint64_t stp_launch_count(const stp_ctx* ctx);
 stp_status stp_detect_ploidy(stp_ctx* ctx, const stp_geno_view* geno, const int64_t* sel_rows,
                              int64_t n_sel, int32_t* ploidy);
 
+/* ComputeBackend::detect_sample_ploidy_device(DecodeTileView) (src/device/backend.hpp:765)
+ * on the canonical individual-major tile: record r (bytes_per_record >= ceil(n_snp/4))
+ * holds individual r's SNP codes MSB-first; ploidy[r] = 2 if a het occurs within its first
+ * min(1000, n_snp) SNPs, else 1. `packed` is a device pointer when packed_on_device != 0. */
+stp_status stp_detect_ploidy_tile(stp_ctx* ctx, const uint8_t* packed, uint64_t bytes_per_record,
+                                  int64_t n_snp, int64_t n_ind, int32_t packed_on_device,
+                                  int32_t* ploidy);
+
 /* Integer decode (decode_af.hpp:58-65): ac2 = 2*ac and n per (pop, SNP), column-major
  * [P x n_snp] host arrays. The bit-exact form of ComputeBackend::decode_af. */
 stp_status stp_decode_counts(stp_ctx* ctx, const stp_geno_view* geno, const int64_t* sel_rows,

@@ -110,6 +110,15 @@ class Context:
         L.check(L.lib().stp_detect_ploidy(self._h, C.byref(v), L.ptr(sel), sel.size, L.ptr(out)))
         return out
 
+    def detect_ploidy_tile(self, packed, bytes_per_record: int, n_snp: int) -> np.ndarray:
+        """detect_sample_ploidy_device on the canonical individual-major tile: one record of
+        bytes_per_record bytes per individual, SNP codes MSB-first."""
+        pk = np.ascontiguousarray(packed, dtype=np.uint8)
+        n_ind = pk.size // bytes_per_record if bytes_per_record else 0
+        out = np.zeros(n_ind, np.int32)
+        L.check(L.lib().stp_detect_ploidy_tile(self._h, L.ptr(pk), bytes_per_record, n_snp, n_ind, 0, L.ptr(out)))
+        return out
+
     def decode_counts(self, records, n_ind: int, sel_rows, pop_offsets, sample_ploidy=None,
                       ploidy: str | int = "auto") -> tuple[np.ndarray, np.ndarray]:
         """(ac2, n) int32 [P, M] C-order views of the column-major [P x M] counts."""

@@ -577,6 +577,29 @@ stp_status stp_decode_af(stp_ctx* ctx, const uint8_t* packed, uint64_t bpr, int6
     });
 }
 
+stp_status stp_detect_ploidy_tile(stp_ctx* ctx, const uint8_t* packed, uint64_t bpr, int64_t n_snp, int64_t n_ind,
+                                  int32_t packed_on_device, int32_t* ploidy) {
+    return guarded([&] {
+        need(ctx != nullptr, "null context");
+        use_device(*ctx);
+        if (n_ind <= 0) return;
+        need(ploidy != nullptr && packed != nullptr, "null argument");
+        need(n_snp >= 0 && bpr * 4 >= static_cast<uint64_t>(n_snp), "bytes_per_record too small for n_snp");
+        cudaStream_t s = ctx->stream;
+        DevBuf d_pk, d_pl;
+        const uint8_t* pk = packed;
+        if (!packed_on_device) {
+            d_pk.reserve(static_cast<size_t>(bpr) * static_cast<size_t>(n_ind));
+            STPF2_CUDA(cudaMemcpyAsync(d_pk.ptr, packed, static_cast<size_t>(bpr) * n_ind, cudaMemcpyHostToDevice, s));
+            pk = d_pk.as<uint8_t>();
+        }
+        d_pl.reserve(sizeof(int32_t) * static_cast<size_t>(n_ind));
+        launch_detect_ploidy_canonical(*ctx, pk, bpr, n_snp, n_ind, d_pl.as<int32_t>(), s);
+        STPF2_CUDA(cudaMemcpyAsync(ploidy, d_pl.ptr, sizeof(int32_t) * n_ind, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 stp_status stp_f2_from_qvn(stp_ctx* ctx, const double* Q, const double* V, const double* N, int32_t P, int64_t M,
                            const int32_t* block_id, int32_t n_block, int32_t precision, double* f2,
                            double* vpair, int32_t* block_sizes) {

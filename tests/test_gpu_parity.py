@@ -132,6 +132,14 @@ def test_decode_counts_large_populations(ctx, size, n_pop, n_snp):
         assert_f2_close(got, want, TC_DEFAULT)
 
 
+def test_detect_ploidy_tile_bitexact(ctx, uneven):
+    p, sel, _, _, _ = uneven
+    canon, obpr = oracle.transpose_pa_to_canonical(p.records_numpy()[:3000], sel)
+    got = ctx.detect_ploidy_tile(canon, obpr, 3000)
+    want = oracle.detect_ploidy_canonical(canon, obpr, 3000, sel.size)
+    assert np.array_equal(got, want) and set(np.unique(got)) <= {1, 2}
+
+
 @pytest.mark.parametrize("detect", [True, False])
 def test_decode_af_canonical_bitexact(ctx, uneven, detect):
     p, sel, po, _, _ = uneven
