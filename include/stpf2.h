@@ -123,6 +123,28 @@ stp_status stp_decode_counts(stp_ctx* ctx, const stp_geno_view* geno, const int6
                              const int32_t* sample_ploidy, int32_t ploidy_mode,
                              int32_t* ac2, int32_t* n);
 
+/* Allocation-free form of stp_decode_counts. No counterpart in the reference (its backends
+ * allocate per call). For callers that cannot allocate device memory at call time: a
+ * process whose caching allocator or memory pool already owns the device's free memory
+ * (a cudaMalloc there fails or forces the pool to release memory and synchronise), and a
+ * caller on a latency-critical stream (cudaFree synchronises the whole device).
+ *
+ * Records must be on the device (geno->on_device = 1) with a 16-byte aligned base and
+ * pitch; d_ac2 / d_n are caller-owned device buffers of n_pop * n_snp int32, written in
+ * the column-major layout of stp_decode_counts. Every intermediate lives in one static
+ * device array of 32 MiB, whose address the library takes once per device
+ * (cudaGetSymbolAddress) on the first call; make that first call before any stream
+ * capture. A request needing more scratch than that (about n_sel * n_snp / 4 bytes of
+ * canonical genotypes plus 12 bytes per SNP) fails with STP_INVALID_ARGUMENT. The call
+ * sets the scratch that must start at a fixed value (file-row map, error flag) itself.
+ * Calls share the scratch: calls on one device that overlap in time (other threads or
+ * streams) race and must be serialised by the caller. Work runs on `stream` (NULL = the
+ * context stream); the call returns after it has finished. */
+stp_status stp_decode_counts_noalloc(stp_ctx* ctx, const stp_geno_view* geno, const int64_t* sel_rows,
+                                     const int64_t* pop_offsets, int32_t n_pop,
+                                     const int32_t* sample_ploidy, int32_t ploidy_mode,
+                                     int32_t* d_ac2, int32_t* d_n, void* stream);
+
 /* ComputeBackend::decode_af(DecodeTileView) (src/device/backend.hpp:736) on the canonical
  * individual-major tile: record g (bytes_per_record >= ceil(n_snp/4)) holds selected
  * sample g's SNP codes MSB-first; pop_offsets[P+1] index records. sample_ploidy NULL with

@@ -95,6 +95,7 @@ SIGNATURES = {
     "stp_detect_ploidy": (C.c_int, [_P, C.POINTER(GenoView), _P, C.c_int64, _P]),
     "stp_detect_ploidy_tile": (C.c_int, [_P, _P, C.c_uint64, C.c_int64, C.c_int64, C.c_int32, _P]),
     "stp_decode_counts": (C.c_int, [_P, C.POINTER(GenoView), _P, _P, C.c_int32, _P, C.c_int32, _P, _P]),
+    "stp_decode_counts_noalloc": (C.c_int, [_P, C.POINTER(GenoView), _P, _P, C.c_int32, _P, C.c_int32, _P, _P, _P]),
     "stp_decode_af": (C.c_int, [_P, _P, C.c_uint64, C.c_int64, C.c_int64, _P, C.c_int32, _P, C.c_int32,
                                 C.c_int32, C.c_int32, _P, _P, _P]),
     "stp_f2_from_qvn": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int64, _P, C.c_int32, C.c_int32, _P, _P, _P]),

@@ -134,6 +134,22 @@ class Context:
                                           L.ptr(ac2), L.ptr(n)))
         return ac2.reshape(M, P).T, n.reshape(M, P).T
 
+    def decode_counts_noalloc(self, d_records, n_ind: int, sel_rows, pop_offsets, d_ac2, d_n,
+                              sample_ploidy=None, ploidy: str | int = "auto", stream=None) -> None:
+        """stp_decode_counts_noalloc: device records (torch CUDA uint8 [n_snp, pitch], pitch a
+        multiple of 16) -> the caller's device int32 buffers d_ac2 / d_n (n_pop * n_snp each,
+        column-major like decode_counts). Allocates nothing on the device."""
+        if not (_is_torch_cuda(d_records) and _is_torch_cuda(d_ac2) and _is_torch_cuda(d_n)):
+            raise TypeError("decode_counts_noalloc takes torch CUDA tensors")
+        v = self.geno_view(d_records, n_ind)
+        sel, po = _i64(sel_rows), _i64(pop_offsets)
+        sp = None if sample_ploidy is None else _i32(sample_ploidy)
+        mode = PLOIDY[str(ploidy)] if not isinstance(ploidy, int) else ploidy
+        st = None if stream is None else C.c_void_p(stream.cuda_stream)
+        L.check(L.lib().stp_decode_counts_noalloc(self._h, C.byref(v), L.ptr(sel), L.ptr(po), po.size - 1,
+                                                  L.ptr(sp), mode, C.c_void_p(d_ac2.data_ptr()),
+                                                  C.c_void_p(d_n.data_ptr()), st))
+
     def decode_af(self, packed, bytes_per_record: int, n_snp: int, pop_offsets, sample_ploidy=None,
                   ploidy: int = 2, detect: bool = False):
         """ComputeBackend::decode_af on the canonical individual-major tile. Returns flat

@@ -534,6 +534,45 @@ stp_status stp_decode_counts(stp_ctx* ctx, const stp_geno_view* geno, const int6
     });
 }
 
+stp_status stp_decode_counts_noalloc(stp_ctx* ctx, const stp_geno_view* geno, const int64_t* sel_rows,
+                                     const int64_t* pop_offsets, int32_t n_pop, const int32_t* sample_ploidy,
+                                     int32_t ploidy_mode, int32_t* d_ac2, int32_t* d_n, void* stream) {
+    return guarded([&] {
+        need(ctx && geno, "null argument");
+        use_device(*ctx);
+        if (n_pop <= 0 || geno->n_snp <= 0) return;
+        need(geno->on_device != 0, "the no-alloc decode reads device-resident records (geno->on_device = 1)");
+        need(geno->records && pop_offsets && d_ac2 && d_n, "null argument");
+        const uint64_t pitch = geno->pitch ? geno->pitch : geno->bytes_per_record;
+        need(pitch % 16 == 0 && reinterpret_cast<uintptr_t>(geno->records) % 16 == 0,
+             "the no-alloc decode needs 16-byte aligned records and pitch (it cannot repitch without a buffer)");
+        need(pitch >= geno->bytes_per_record, "pitch smaller than bytes_per_record");
+        need(pop_offsets[0] == 0, "pop_offsets[0] must be 0");
+        for (int i = 0; i < n_pop; ++i) {
+            need(pop_offsets[i + 1] >= pop_offsets[i], "pop_offsets must be non-decreasing");
+            need(pop_offsets[i + 1] - pop_offsets[i] <= 16383, "a population has more than 16383 samples");
+        }
+        const int64_t n_sel = pop_offsets[n_pop];
+        need(n_sel == 0 || sel_rows != nullptr, "sel_rows is NULL");
+        need(n_sel < INT_MAX, "too many selected samples");
+        for (int64_t g = 0; g < n_sel; ++g) {
+            need(sel_rows[g] >= 0 && sel_rows[g] < geno->n_ind, "sel_rows entry outside [0, n_ind)");
+            need(static_cast<uint64_t>(sel_rows[g] / 4) < geno->bytes_per_record, "sel_rows entry beyond the record");
+        }
+        int mode_pl = 0;
+        bool detect = false;
+        if (!sample_ploidy) {
+            if (ploidy_mode == STP_PLOIDY_AUTO) detect = true;
+            else if (ploidy_mode == STP_PLOIDY_PSEUDO) mode_pl = 1;
+            else if (ploidy_mode == STP_PLOIDY_DIPLOID) mode_pl = 2;
+            else need(false, "unknown ploidy_mode");
+        }
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+        noalloc_decode_counts(*ctx, geno->records, pitch, geno->n_snp, geno->n_ind, sel_rows, n_sel, pop_offsets,
+                              n_pop, sample_ploidy, mode_pl, detect, d_ac2, d_n, s);
+    });
+}
+
 stp_status stp_decode_af(stp_ctx* ctx, const uint8_t* packed, uint64_t bpr, int64_t n_snp, int64_t n_ind,
                          const int64_t* pop_offsets, int32_t n_pop, const int32_t* sample_ploidy, int32_t ploidy,
                          int32_t detect, int32_t packed_on_device, double* q, double* v, double* n) {

@@ -229,4 +229,13 @@ int umma_tile();
 void launch_jackknife(Ctx& c, const double* x, const int32_t* block_sizes, int64_t m, int nb,
                       double* est, double* var, cudaStream_t s);
 
+// Allocation-free count decode (noalloc.cu): every intermediate lives in one static
+// device array of kNoAllocScratchBytes.
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+size_t noalloc_scratch_bytes(int64_t n_snp, int64_t n_ind, int64_t n_sel, int P, bool copy_ploidy);
+void noalloc_decode_counts(Ctx& c, const uint8_t* d_records, uint64_t pitch, int64_t n_snp, int64_t n_ind,
+                           const int64_t* sel_rows, int64_t n_sel, const int64_t* pop_offsets, int P,
+                           const int32_t* sample_ploidy, int mode_ploidy, bool detect, int32_t* d_ac2,
+                           int32_t* d_n, cudaStream_t s);
+
 }  // namespace stpf2
