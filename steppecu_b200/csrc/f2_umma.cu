@@ -12,12 +12,12 @@
 //               the hi/lo splits (the -Pt Pt products use the descriptor's A-negate bit)
 //               into one FP32 TMEM buffer per 32-SNP chunk; one kind::i8 MMA per stage
 //               accumulates the exact both-present count M M^T into an int32 TMEM buffer.
-//   warps 2-9   epilogue: drains the FP32 chunks two at a time into FP64 registers (one
-//               round-to-nearest FP32 add of the two chunk sums, then one FP32 -> FP64
-//               conversion and FP64 add; the conversions bound this loop, so pairing halves
-//               it); at the end of the block, reads vpair, forms f2 = num / vpair (0 when
-//               vpair = 0, f2_estimator.hpp:42-46) in FP64 and stores (i,j) and (j,i) of the
-//               block's slab.
+//   warps 2-17  epilogue, four warps per TMEM lane quarter, 32 tile columns each: drains
+//               the FP32 chunks two at a time into FP64 registers (one round-to-nearest FP32
+//               add of the two chunk sums, then one FP32 -> FP64 conversion and FP64 add);
+//               at the end of the block, reads vpair, forms f2 = num / vpair in FP64 (0 when
+//               vpair = 0, f2_estimator.hpp:42-46) and stores (i,j) and (j,i) of the block's
+//               slab.
 //
 // TMEM (512 columns): a ring of three FP32 numerator chunk buffers at [0,128), [128,256),
 // [256,384) (the MMAs fill the third while a pair drains) and the int32 vpair of the
@@ -45,18 +45,19 @@ constexpr uint32_t kTile8 = kTile * kStageK;                      // 4 KiB
 constexpr uint32_t kSideBytes = kPlanes * kTile16 + kTile8;       // 44 KiB
 constexpr uint32_t kStageBytes = 2 * kSideBytes;                  // 88 KiB
 static_assert(kSideBytes == kImageBytes, "a stage side is one operand image");
-constexpr int kEpiWarps = 8;
-constexpr int kEpiWarp0 = 2;                        // epilogue = warps 2..9
-constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);  // 320
-// 10 warps put three warps on some SM sub-partitions, so at most 16384 / (3 * 32) = 170
-// registers per thread; the epilogue's 64 FP64 accumulators fit, the end-of-tile stores spill.
+constexpr int kEpiWarps = 16;
+constexpr int kEpiWarp0 = 2;                        // epilogue = warps 2..17
+constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);  // 576
+constexpr int kCols = 4 * kTile / kEpiWarps;        // tile columns per epilogue thread (32)
+// 18 warps put five warps on two SM sub-partitions, so at most 16384 / (5 * 32) = 102
+// registers per thread (96 in allocation steps); 32 FP64 accumulators per thread fit.
+// Four epilogue warps per TMEM lane quarter keep enough tensor-memory loads in flight.
 constexpr uint32_t kTmemCols = 512;
 constexpr unsigned long long kTimeoutNs = 4000000000ull;
-// Per-epilogue-warp staging tile for the transposed stores: f2 and vpair, 32 rows x 8
-// columns each, rows padded to 9 doubles (fewer bank conflicts).
+// Per-epilogue-warp staging tile for the transposed stores (f2, then vpair): 32 rows x 8
+// columns, rows padded to 9 doubles (fewer bank conflicts).
 constexpr int kStagePitch = 9;
-constexpr int kStageHalf = 32 * kStagePitch;
-constexpr int kStageDoubles = 2 * kStageHalf;
+constexpr int kStageDoubles = 32 * kStagePitch;
 constexpr uint32_t kCtlBytes = 256;
 
 struct UmmaArgs {
@@ -69,6 +70,8 @@ struct UmmaArgs {
     double* f2;
     double* vpair;
     double num_scale;  // 2 * plane scale undo
+    const double* rcp; // rcp[k] = 1/k for k = 0..rcp_max (rcp[0] = 0): vpair never exceeds the block size
+    int rcp_max;
     int* err;
     uint32_t idesc_pp, idesc_am, idesc_i8;
 };
@@ -307,23 +310,24 @@ done:
 __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int warp, int lane, double* stage) {
     const int e = warp - kEpiWarp0;
     const int q = warp & 3;                 // TMEM lane quarter this warp may access
-    const int h = e >> 2;                   // column half of the tile
+    const int h = e >> 2;                   // column part of the tile (kCols columns)
     const int r = q * 32 + lane;            // tile row (TMEM lane)
     const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
+    const uint32_t col_addr = static_cast<uint32_t>(h * kCols);
     const int P = a.P;
     uint32_t cs = 0, is = 0;
-    double acc[64];  // FP64 running numerator per column
+    double acc[kCols];  // FP64 running numerator per column
     for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
         const WorkItem w = a.items[it];
         const BlockInfo bi = a.blocks[w.blk];
         const int nst = stages_of(bi.k);
         const bool diag = w.ti == w.tj;
         const int i = w.ti * kTile + r;
-        const int j0 = w.tj * kTile + h * 64;
+        const int j0 = w.tj * kTile + h * kCols;
         const int64_t slab = static_cast<int64_t>(P) * P * bi.b;
         if (nst == 0) {  // an empty block id: zeros (cpu_backend.cpp:234)
             if (i < P)
-                for (int c = 0; c < 64; ++c) {
+                for (int c = 0; c < kCols; ++c) {
                     const int j = j0 + c;
                     if (j >= P || (diag && j < i)) continue;
                     a.f2[slab + i + static_cast<int64_t>(P) * j] = 0.0;
@@ -334,7 +338,7 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
             continue;
         }
 #pragma unroll
-        for (int c = 0; c < 64; ++c) acc[c] = 0.0;
+        for (int c = 0; c < kCols; ++c) acc[c] = 0.0;
         for (int ch = 0; ch < nst; ch += 2) {
             const bool pair = ch + 1 < nst;
             const int nb0 = static_cast<int>(cs % kNumBufs), nb1 = static_cast<int>((cs + 1) % kNumBufs);
@@ -346,12 +350,12 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) return;
             tc_fence_after();
-            const uint32_t b0 = tmem + lane_addr + static_cast<uint32_t>(nb0) * 128u + static_cast<uint32_t>(h) * 64u;
+            const uint32_t b0 = tmem + lane_addr + static_cast<uint32_t>(nb0) * 128u + col_addr;
             // A lone last chunk reads its buffer twice and adds zero (exact).
-            const uint32_t b1 = pair ? tmem + lane_addr + static_cast<uint32_t>(nb1) * 128u + static_cast<uint32_t>(h) * 64u : b0;
+            const uint32_t b1 = pair ? tmem + lane_addr + static_cast<uint32_t>(nb1) * 128u + col_addr : b0;
             const float w1 = pair ? 1.0f : 0.0f;
 #pragma unroll
-            for (int q8 = 0; q8 < 8; ++q8) {
+            for (int q8 = 0; q8 < kCols / 8; ++q8) {
                 uint32_t v0[8], v1[8];
                 tmem_ld8(b0 + static_cast<uint32_t>(q8) * 8u, v0);
                 tmem_ld8(b1 + static_cast<uint32_t>(q8) * 8u, v1);
@@ -375,50 +379,52 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
             if (!ok) return;
         }
         tc_fence_after();
-        const uint32_t vbase = tmem + lane_addr + kVpCol + static_cast<uint32_t>(h) * 64u;
+        const uint32_t vbase = tmem + lane_addr + kVpCol + col_addr;
         // Output: (i, j) straight from registers (32 consecutive i per store: full sectors);
         // (j, i) through this warp's staging tile, so each store covers 4 rows x 8
         // consecutive j (64-byte segments) instead of 32 scattered 8-byte pieces.
         const int i0 = w.ti * kTile + q * 32;
-        const int64_t row_i = slab + i;                       // (i, j) at row_i + P*j
+        const int64_t row_i = slab + i;                              // (i, j) at row_i + P*j
         const int64_t row_j0 = slab + static_cast<int64_t>(P) * i0;  // (j, i0 + rr) at row_j0 + P*rr + j
 #pragma unroll
-        for (int q16 = 0; q16 < 4; ++q16) {
-            uint32_t v[16];
-            tmem_ld16(vbase + static_cast<uint32_t>(q16) * 16u, v);
+        for (int q8 = 0; q8 < kCols / 8; ++q8) {
+            uint32_t v[8];
+            tmem_ld8(vbase + static_cast<uint32_t>(q8) * 8u, v);
             tmem_wait_ld();
-            if (q16 == 3) {
+            if (q8 == kCols / 8 - 1) {
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&ctl->vp_empty);
             }
+            double fv[8], vv[8];
 #pragma unroll
-            for (int cg = 0; cg < 16; cg += 8) {
-#pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    const int col = q16 * 16 + cg + c;
-                    const int j = j0 + col;
-                    const double vp = static_cast<double>(static_cast<int32_t>(v[cg + c]));
-                    const double num = acc[col];
-                    const double f = (vp > 0.0) ? (num * a.num_scale) / vp : 0.0;
-                    if (i < P && j < P && !(diag && j < i)) {
-                        const int64_t ij = row_i + static_cast<int64_t>(P) * j;
-                        __stcs(a.f2 + ij, f);  // output is never re-read: evict-first
-                        __stcs(a.vpair + ij, vp);
-                    }
-                    stage[lane * kStagePitch + c] = f;
-                    stage[kStageHalf + lane * kStagePitch + c] = vp;
+            for (int c = 0; c < 8; ++c) {
+                const int col = q8 * 8 + c;
+                const int j = j0 + col;
+                // vpair is an exact count <= the block size: convert it with the 2^52 trick
+                // (an FP64 add) and divide through the 1/k table (within 2 ulp of num / vp).
+                const int32_t vpi = static_cast<int32_t>(v[c]);
+                const int32_t vk = vpi < a.rcp_max ? vpi : a.rcp_max;
+                vv[c] = __hiloint2double(0x43300000, vpi) - 4503599627370496.0;
+                fv[c] = vk > 0 ? acc[col] * a.num_scale * __ldg(a.rcp + vk) : 0.0;
+                if (i < P && j < P && !(diag && j < i)) {
+                    const int64_t ij = row_i + static_cast<int64_t>(P) * j;
+                    __stcs(a.f2 + ij, fv[c]);  // output is never re-read: evict-first
+                    __stcs(a.vpair + ij, vv[c]);
                 }
+            }
+            const int jj = j0 + q8 * 8 + (lane & 7);
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+                double* out = part == 0 ? a.f2 : a.vpair;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) stage[lane * kStagePitch + c] = part == 0 ? fv[c] : vv[c];
                 __syncwarp();
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
-                    const int rr = 4 * k + (lane >> 3), cc = lane & 7;
-                    const int jj = j0 + q16 * 16 + cg + cc;
-                    if (i0 + rr < P && jj < P && !(diag && jj <= i0 + rr)) {
-                        const int64_t ji = row_j0 + static_cast<int64_t>(P) * rr + jj;
-                        __stcs(a.f2 + ji, stage[rr * kStagePitch + cc]);
-                        __stcs(a.vpair + ji, stage[kStageHalf + rr * kStagePitch + cc]);
-                    }
+                    const int rr = 4 * k + (lane >> 3);
+                    if (i0 + rr < P && jj < P && !(diag && jj <= i0 + rr))
+                        __stcs(out + row_j0 + static_cast<int64_t>(P) * rr + jj, stage[rr * kStagePitch + (lane & 7)]);
                 }
                 __syncwarp();
             }
@@ -427,7 +433,7 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
     }
 }
 
-__global__ void __maxnreg__(168)
+__global__ void __maxnreg__(96)
 f2_umma_kernel(const __grid_constant__ UmmaArgs a) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -492,8 +498,9 @@ constexpr size_t kSmemBytes = kStages * kStageBytes + kCtlBytes + kEpiWarps * kS
 struct UmmaPlan {
     const uint8_t* images = nullptr;
     int64_t n_ck = 0;
-    DevBuf items, blocks, err;
+    DevBuf items, blocks, err, rcp;
     int n_items = 0;
+    int rcp_max = 0;
     int P = 0;
     OpFmt fmt = OpFmt::BF16;
     double num_scale = 2.0;
@@ -517,6 +524,14 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
     STPF2_CUDA(cudaMemcpyAsync(p->blocks.ptr, L.blocks.data(), L.blocks.size() * sizeof(BlockInfo),
                                cudaMemcpyHostToDevice, c.stream));
     STPF2_CUDA(cudaMemsetAsync(p->err.ptr, 0, 16, c.stream));
+    int max_k = 0;
+    for (const BlockInfo& b : L.blocks) max_k = std::max(max_k, b.k);
+    std::vector<double> rcp(static_cast<size_t>(max_k) + 1, 0.0);
+    for (int k = 1; k <= max_k; ++k) rcp[k] = 1.0 / static_cast<double>(k);
+    p->rcp_max = max_k;
+    p->rcp.reserve(rcp.size() * sizeof(double));
+    STPF2_CUDA(cudaMemcpyAsync(p->rcp.ptr, rcp.data(), rcp.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    STPF2_CUDA(cudaStreamSynchronize(c.stream));  // the host tables above go out of scope
 
     if (op.n_rt <= 0 || op.n_ck <= 0) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs tiled planes");
     p->images = static_cast<const uint8_t*>(op.planes);
@@ -540,6 +555,8 @@ void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t
     a.f2 = f2;
     a.vpair = vpair;
     a.num_scale = p->num_scale;
+    a.rcp = p->rcp.as<double>();
+    a.rcp_max = p->rcp_max;
     a.err = p->err.as<int>();
     const bool bf16 = p->fmt == OpFmt::BF16;
     a.idesc_pp = idesc_f16(bf16, true);
