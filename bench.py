@@ -3,8 +3,8 @@
 Metric: f2 SNP-pop-pairs/s = M * P*(P-1)/2 per extraction pass, per second. A step is one
 pass of the hot path (ploidy -> decode -> per-block contraction -> FP64 f2/vpair) over
 one synthetic panel already resident in HBM. Workload (default): 1,000 populations x 10
-samples (10,000 total), 1,150,000 SNPs on 22 chromosomes, 5 cM blocks (~700), split-BF16
-tensor-core contraction. The panel (2.9 GB of genotypes, ~12 GB of operands) is far larger
+samples (10,000 total), 1,150,000 SNPs on 22 chromosomes, 5 cM blocks (~700), split-F16
+tensor-core contraction (split-BF16 and the plain FP32 SIMT form are timed beside it). The panel (2.9 GB of genotypes, ~12 GB of operands) is far larger
 than L2, so no flush is needed between steps.
 
 `e2e` times the same extraction through the C ABI with host buffers: pinned genotypes in,
@@ -12,7 +12,9 @@ H2D copy, extraction, D2H of the FP64 f2 and vpair tensors, every step.
 
 `--impl reference` times the reference's own CpuBackend (oracle/_ref, built from the
 reference sources; the C restatement when that is absent) on the host cores, one
-jackknife block per thread, on a bounded sample of the same workload.
+jackknife block per thread, on a bounded sample of the same workload. The same sample is
+extracted on the GPU in every arithmetic and compared with it: `precision` reports the
+max abs / rel f2 error against the reference at the workload's full population count.
 
 Multi-GPU (torchrun): blocks are independent, so every rank extracts its own panel (a
 different genome segment of the same shape): weak scaling, no data-path collective.
@@ -105,9 +107,10 @@ def make_panel(workload: str, rank: int, device: str, n_snp: int | None = None):
     return synth.generate(workload, seed=20261203 + 1000 * rank, device=device, n_snp=n_snp)
 
 
-def cpu_sample(workload: str, threads: int, seed_rank: int = 0, gen_device: str = "cpu"):
+def cpu_sample(workload: str, threads: int, seed_rank: int = 0, gen_device: str = "cpu", keep: bool = False):
     """Bounded CPU sample: `threads` blocks of the workload's panel model (one per thread),
-    decoded and reduced by the CPU implementation. Returns (units, seconds, kind, desc)."""
+    decoded and reduced by the CPU implementation. Returns (units, seconds, kind, desc) and,
+    with keep=True, also (panel, block ids, f2, vpair) for the precision check."""
     import numpy as np
 
     import oracle
@@ -126,11 +129,35 @@ def cpu_sample(workload: str, threads: int, seed_rank: int = 0, gen_device: str 
     pl = oracle.detect_ploidy_pa(rec, sel)
     ac2, n = oracle.decode_counts_pa(rec, sel, po, pl)
     q, v, nd = oracle.counts_to_qvn(ac2, n)
-    oracle.compute_f2_blocks_sharded(q, v, nd, p.n_pop, bid, threads, threads=threads, lib=lib)
+    f2, vp, _ = oracle.compute_f2_blocks_sharded(q, v, nd, p.n_pop, bid, threads, threads=threads, lib=lib)
     dt = time.perf_counter() - t0
     desc = (f"{threads} blocks x {per_block} SNPs of the {workload} panel model (P={p.n_pop}, "
             f"N={p.n_ind}), decode + f2 on {threads} threads, one block per thread")
+    if keep:
+        return units(p.n_pop, n_snp), dt, kind, desc, (p, bid, threads, f2, vp)
     return units(p.n_pop, n_snp), dt, kind, desc
+
+
+def precision_report(ctx, sample, modes) -> dict:
+    """GPU extraction of the CPU sample in each arithmetic against the CPU result."""
+    import numpy as np
+
+    p, bid, nb, f2_ref, vp_ref = sample
+    sel, po = p.selection()
+    rec = p.records_numpy()
+    a = np.abs(f2_ref)
+    big, sig = a >= 1e-12, a >= 1e-2
+    out = {}
+    for mode in modes:
+        t = ctx.extract_blocks(rec, p.n_ind, sel, po, bid, nb, precision=mode)
+        d = np.abs(t.f2 - f2_ref)
+        # Relative error is unbounded where a block's f2 estimate crosses zero, in every
+        # arithmetic; max_rel_f2_ge_0.01 is the relative error over non-degenerate values.
+        out[mode] = {"max_abs": float(d.max()), "max_rel": float((d[big] / a[big]).max()),
+                     "max_rel_f2_ge_0.01": float((d[sig] / a[sig]).max()),
+                     "frac_f2_ge_0.01": float(sig.mean()),
+                     "vpair_bit_exact": bool(np.array_equal(t.vpair, vp_ref))}
+    return out
 
 
 def run_reference(args, rank: int, world: int):
@@ -271,8 +298,28 @@ def main():
         barrier()
         return ms, dec, con, launches
 
+    def timed_graph(pl, steps, warm):
+        # The pass replayed from one CUDA graph (ploidy, transpose, decode, contraction).
+        for _ in range(warm):
+            pl.run_graph(rec, f2, vp, stream.cuda_stream)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        l0 = ctx.launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            pl.run_graph(rec, f2, vp, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = ctx.launches - l0
+        barrier()
+        return e0.elapsed_time(e1) / steps, launches
+
     with Clocks(local) as clk:
-        ms, dec_ms, con_ms, launches = timed(plan, args.steps, args.warmup)
+        ms, launches = timed_graph(plan, args.steps, args.warmup)
+        # Per-kernel split (decode vs contraction) from event-bracketed plain runs.
+        _, dec_ms, con_ms, _ = timed(plan, args.steps, args.warmup)
     clocks = clk.summary()
     if dist is not None:
         t = torch.tensor([ms], device=dev)
@@ -312,10 +359,13 @@ def main():
                 "decode_hbm_gbs": (M * bpr + 11 * P * M) / (dec_ms / 1000.0) / 1e9}
 
     cpu = None
+    precision = None
     if rank == 0 and world == 1 and not args.quick:
         threads = args.cpu_threads or (os.cpu_count() or 1)
-        u, t, kind, desc = cpu_sample(args.workload, threads, gen_device=dev)
+        u, t, kind, desc, sample = cpu_sample(args.workload, threads, gen_device=dev, keep=True)
         cpu = {"value": u / t, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc}
+        modes = [args.precision] + [m for m in ("split_bf16", "fp32") if m != args.precision]
+        precision = {"against": f"{kind} CPU f2 on the cpu_baseline sample", **precision_report(ctx, sample, modes)}
 
     if rank == 0:
         line = {
@@ -325,8 +375,10 @@ def main():
             "data": "synthetic",
             "config": {"workload": args.workload, "populations": P, "samples": panel.n_ind, "snps": M,
                        "blocks": B, "precision": args.precision, "l2": "inputs larger than L2 (no flush)",
+                       "cuda_graph": True,
                        "parallelism": f"block-sharded x{world}" if world > 1 else "1 GPU"},
             "gpu_launches": int(launches), "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "precision": precision,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "other_arithmetics": others,
         }

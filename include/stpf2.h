@@ -187,6 +187,12 @@ stp_plan* stp_plan_create(stp_ctx* ctx, const stp_f2_request* req, stp_status* s
  * d_f2/d_vpair are device buffers of P*P*n_block doubles. Asynchronous. */
 stp_status stp_plan_run(stp_plan* plan, const uint8_t* d_records, double* d_f2, double* d_vpair,
                         void* stream);
+/* The same pass as stp_plan_run, replayed from one CUDA graph: the first call for a given
+ * (d_records, d_f2, d_vpair) captures the pass's kernels (ploidy, transpose, decode,
+ * contraction) into a graph and instantiates it; later calls only launch it on `stream`.
+ * Plan timing must be off. Asynchronous. */
+stp_status stp_plan_run_graph(stp_plan* plan, const uint8_t* d_records, double* d_f2, double* d_vpair,
+                              void* stream);
 /* Kernel launches one stp_plan_run issues. */
 int32_t stp_plan_launches(const stp_plan* plan);
 /* Timing: with timing enabled, every stp_plan_run records CUDA events on its stream around

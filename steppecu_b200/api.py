@@ -241,6 +241,12 @@ class Plan:
         L.check(L.lib().stp_plan_run(self._h, _data_ptr(records), _data_ptr(f2), _data_ptr(vpair),
                                      stream or None))
 
+    def run_graph(self, records, f2, vpair, stream: int = 0) -> None:
+        """The same pass replayed from a CUDA graph (captured on the first call for these
+        buffers)."""
+        L.check(L.lib().stp_plan_run_graph(self._h, _data_ptr(records), _data_ptr(f2), _data_ptr(vpair),
+                                           stream or None))
+
     @property
     def launches(self) -> int:
         return int(L.lib().stp_plan_launches(self._h))

@@ -166,8 +166,12 @@ struct Plan {
     bool timing = false;
     std::vector<std::array<cudaEvent_t, 3>> ev;
     size_t n_timed = 0;
+    // One executable graph of the whole pass, instantiated for one (records, f2, vpair).
+    cudaGraphExec_t graph = nullptr;
+    const void* graph_key[3] = {nullptr, nullptr, nullptr};
 
     ~Plan() {
+        if (graph) cudaGraphExecDestroy(graph);
         if (umma) umma_plan_destroy(umma);
         for (auto& t : ev)
             for (auto e : t)
@@ -776,6 +780,43 @@ stp_status stp_plan_run(stp_plan* plan, const uint8_t* d_records, double* d_f2, 
         use_device(*p.ctx);
         cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p.ctx->stream;
         run_plan(p, d_records, d_f2, d_vpair, s);
+    });
+}
+
+stp_status stp_plan_run_graph(stp_plan* plan, const uint8_t* d_records, double* d_f2, double* d_vpair,
+                              void* stream) {
+    return guarded([&] {
+        need(plan != nullptr, "null plan");
+        Plan& p = *plan->p;
+        use_device(*p.ctx);
+        need(!p.timing, "disable plan timing before replaying the plan as a graph");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p.ctx->stream;
+        const void* key[3] = {d_records, d_f2, d_vpair};
+        if (!p.graph || !std::equal(key, key + 3, p.graph_key)) {
+            if (p.graph) {
+                STPF2_CUDA(cudaGraphExecDestroy(p.graph));
+                p.graph = nullptr;
+            }
+            const uint64_t before = p.ctx->launches.load();
+            cudaGraph_t g = nullptr;
+            STPF2_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try {
+                run_plan(p, d_records, d_f2, d_vpair, s);
+            } catch (...) {
+                cudaStreamEndCapture(s, &g);
+                if (g) cudaGraphDestroy(g);
+                p.ctx->launches = before;
+                throw;
+            }
+            STPF2_CUDA(cudaStreamEndCapture(s, &g));
+            const cudaError_t e = cudaGraphInstantiate(&p.graph, g, 0);
+            cudaGraphDestroy(g);
+            p.ctx->launches = before;  // capturing launched nothing
+            STPF2_CUDA(e);
+            std::copy(key, key + 3, p.graph_key);
+        }
+        STPF2_CUDA(cudaGraphLaunch(p.graph, s));
+        p.ctx->launches += static_cast<uint64_t>(p.launches());
     });
 }
 

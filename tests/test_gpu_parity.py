@@ -257,6 +257,28 @@ def test_plan_device_resident_matches_one_shot(ctx, c1):
     assert plan.launches >= 2
 
 
+def test_plan_graph_replay_equals_plan_run(ctx, c1):
+    import torch
+
+    p, sel, po, _, _ = c1
+    rec = torch.as_tensor(p.records_numpy()).cuda()
+    plan = ctx.plan(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision=TC_DEFAULT)
+    n = p.n_pop * p.n_pop * p.n_block
+    f_a, v_a = torch.zeros(n, dtype=torch.float64, device="cuda"), torch.zeros(n, dtype=torch.float64, device="cuda")
+    plan.run(rec, f_a, v_a)
+    torch.cuda.synchronize()
+    f_b, v_b = torch.full_like(f_a, 7.0), torch.full_like(v_a, 7.0)
+    before = ctx.launches
+    for _ in range(3):  # the first call captures, the others replay
+        f_b.fill_(7.0)
+        v_b.fill_(7.0)
+        plan.run_graph(rec, f_b, v_b)
+    torch.cuda.synchronize()
+    assert ctx.launches - before == 3 * plan.launches
+    assert torch.equal(f_a, f_b) and torch.equal(v_a, v_b)
+    plan.close()
+
+
 def test_jackknife_vs_oracle(ctx, c1):
     _, _, _, want, _ = c1
     m = want.P * want.P
