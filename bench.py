@@ -38,6 +38,8 @@ sys.path.insert(0, str(ROOT / "oracle"))
 METRIC = "f2 SNP·pop-pairs/s: split-BF16 TC vs plain FP32 on 1 B200, rel err ≤1e-6 vs FP64"
 UNIT = "SNP·pop-pairs/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# dram__bytes_read.sum + dram__bytes_write.sum of one f2_umma_kernel launch (ncu, one pass).
+CONTRACTION_TRAFFIC = {("c3", "split_f16"): 25.82e9 + 12.41e9}
 
 
 def load_peaks():
@@ -343,6 +345,15 @@ def main():
                         "contract_ms": con_s, "decode_ms": dec_s}
         plan_s.close()
 
+    # The grouped schedule against one contraction launch per jackknife block.
+    per_block = None
+    if args.precision != "fp32" and not args.quick:
+        plan.set_per_block_launch(True)
+        ms_b, dec_b, con_b, l_b = timed(plan, max(1, min(args.steps, 3)), 1)
+        plan.set_per_block_launch(False)
+        per_block = {"ms_per_step": ms_b, "contract_ms": con_b, "launches_per_step": l_b / max(1, min(args.steps, 3)),
+                     "value": units(P, M) * world / (ms_b / 1000.0)}
+
     e2e = None
     if not args.quick:
         e2e = run_e2e(args, ctx, rec, panel, sel, po, bpr, n_out, barrier, dist, dev, P, M, B, world)
@@ -353,8 +364,11 @@ def main():
     flops = 6.0 * P * P * M
     achieved = flops / (con_ms / 1000.0) / 1e12
     peak = float(peaks.get("bf16_tflops", PEAKS_FALLBACK["bf16_tflops"]))
+    # DRAM bytes (read + write) of one contraction launch on this workload, from the ncu
+    # capture summarised in profiles/traffic_full_workload_1000pops_1.15M_snps.md.
+    traffic = CONTRACTION_TRAFFIC.get((args.workload, args.precision)) if args.snps is None else None
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                 "kernel_ms": con_ms, "decode_ms": dec_ms,
                 "decode_hbm_gbs": (M * bpr + 11 * P * M) / (dec_ms / 1000.0) / 1e9}
 
@@ -381,6 +395,7 @@ def main():
             "precision": precision,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "other_arithmetics": others,
+            "per_block_launches": per_block,
         }
         print(json.dumps(line), flush=True)
     plan.close()

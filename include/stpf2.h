@@ -193,6 +193,9 @@ stp_status stp_plan_run(stp_plan* plan, const uint8_t* d_records, double* d_f2, 
  * Plan timing must be off. Asynchronous. */
 stp_status stp_plan_run_graph(stp_plan* plan, const uint8_t* d_records, double* d_f2, double* d_vpair,
                               void* stream);
+/* Comparison form of the contraction (tensor-core plans): one launch per jackknife block
+ * instead of one persistent launch over every block's tile pairs. Same results. */
+stp_status stp_plan_set_per_block_launch(stp_plan* plan, int32_t enable);
 /* Kernel launches one stp_plan_run issues. */
 int32_t stp_plan_launches(const stp_plan* plan);
 /* Timing: with timing enabled, every stp_plan_run records CUDA events on its stream around

@@ -105,6 +105,7 @@ SIGNATURES = {
     "stp_plan_create": (_P, [_P, C.POINTER(F2Request), C.POINTER(C.c_int)]),
     "stp_plan_run": (C.c_int, [_P, _P, _P, _P, _P]),
     "stp_plan_run_graph": (C.c_int, [_P, _P, _P, _P, _P]),
+    "stp_plan_set_per_block_launch": (C.c_int, [_P, C.c_int32]),
     "stp_plan_launches": (C.c_int32, [_P]),
     "stp_plan_set_timing": (C.c_int, [_P, C.c_int32]),
     "stp_plan_last_times": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),

@@ -251,6 +251,10 @@ class Plan:
     def launches(self) -> int:
         return int(L.lib().stp_plan_launches(self._h))
 
+    def set_per_block_launch(self, on: bool = True) -> None:
+        """Comparison form: one contraction launch per jackknife block."""
+        L.check(L.lib().stp_plan_set_per_block_launch(self._h, 1 if on else 0))
+
     def set_timing(self, on: bool = True) -> None:
         L.check(L.lib().stp_plan_set_timing(self._h, 1 if on else 0))
 

@@ -498,7 +498,8 @@ constexpr size_t kSmemBytes = kStages * kStageBytes + kCtlBytes + kEpiWarps * kS
 struct UmmaPlan {
     const uint8_t* images = nullptr;
     int64_t n_ck = 0;
-    DevBuf items, blocks, err, rcp;
+    DevBuf items, blocks, err, rcp, block_items;
+    std::vector<int> block_item_off;  // per block: its tile pairs in block_items
     int n_items = 0;
     int rcp_max = 0;
     int P = 0;
@@ -516,6 +517,15 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
     p->num_scale = 2.0 * op.scale_inv;
     const std::vector<WorkItem> items = make_work_items(L, op.P, kTile);
     p->n_items = static_cast<int>(items.size());
+    // The same items grouped by block, for the one-launch-per-block comparison form.
+    std::vector<WorkItem> by_block(items);
+    std::stable_sort(by_block.begin(), by_block.end(), [](const WorkItem& x, const WorkItem& y) { return x.blk < y.blk; });
+    p->block_item_off.assign(L.blocks.size() + 1, 0);
+    for (const WorkItem& w : by_block) p->block_item_off[static_cast<size_t>(w.blk) + 1]++;
+    for (size_t b = 0; b < L.blocks.size(); ++b) p->block_item_off[b + 1] += p->block_item_off[b];
+    p->block_items.reserve(std::max<size_t>(by_block.size() * sizeof(WorkItem), 16));
+    STPF2_CUDA(cudaMemcpyAsync(p->block_items.ptr, by_block.data(), by_block.size() * sizeof(WorkItem),
+                               cudaMemcpyHostToDevice, c.stream));
     p->items.reserve(std::max<size_t>(items.size() * sizeof(WorkItem), 16));
     p->blocks.reserve(std::max<size_t>(L.blocks.size() * sizeof(BlockInfo), 16));
     p->err.reserve(16);
@@ -543,13 +553,28 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
 
 void umma_plan_destroy(UmmaPlan* p) { delete p; }
 
-void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s) {
+void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, double* f2, double* vpair,
+                       cudaStream_t s);
+
+void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s, bool per_block) {
     if (!p || p->n_items <= 0) return;
+    if (per_block) {  // comparison form: one launch per jackknife block
+        for (size_t b = 0; b + 1 < p->block_item_off.size(); ++b) {
+            const int n = p->block_item_off[b + 1] - p->block_item_off[b];
+            if (n > 0) launch_umma_items(c, p, p->block_items.as<WorkItem>() + p->block_item_off[b], n, f2, vpair, s);
+        }
+        return;
+    }
+    launch_umma_items(c, p, p->items.as<WorkItem>(), p->n_items, f2, vpair, s);
+}
+
+void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, double* f2, double* vpair,
+                       cudaStream_t s) {
     UmmaArgs a{};
     a.images = p->images;
     a.n_ck = p->n_ck;
-    a.items = p->items.as<WorkItem>();
-    a.n_items = p->n_items;
+    a.items = items;
+    a.n_items = n_items;
     a.blocks = p->blocks.as<BlockInfo>();
     a.P = p->P;
     a.f2 = f2;
@@ -562,7 +587,7 @@ void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t
     a.idesc_pp = idesc_f16(bf16, true);
     a.idesc_am = idesc_f16(bf16, false);
     a.idesc_i8 = idesc_u8_s32();
-    const int grid = std::min(c.sm_count, p->n_items);
+    const int grid = std::min(c.sm_count, n_items);
     f2_umma_kernel<<<grid, kThreads, kSmemBytes, s>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

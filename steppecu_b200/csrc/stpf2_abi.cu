@@ -169,6 +169,7 @@ struct Plan {
     // One executable graph of the whole pass, instantiated for one (records, f2, vpair).
     cudaGraphExec_t graph = nullptr;
     const void* graph_key[3] = {nullptr, nullptr, nullptr};
+    bool per_block = false;  // comparison form: one contraction launch per block
 
     ~Plan() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -178,7 +179,10 @@ struct Plan {
                 if (e) cudaEventDestroy(e);
     }
 
-    int launches() const { return (detect ? 1 : 0) + 2 + 1; }
+    int launches() const {
+        const int contract = (per_block && umma) ? static_cast<int>(L.blocks.size()) : 1;
+        return (detect ? 1 : 0) + 2 + contract;
+    }
 };
 
 namespace {
@@ -358,7 +362,7 @@ void run_plan(Plan& p, const uint8_t* d_records, double* d_f2, double* d_vpair, 
     if (p.precision == STP_PREC_FP32_SIMT)
         launch_f2_simt(c, p.items.as<WorkItem>(), p.n_items, p.blocks.as<BlockInfo>(), p.op, d_f2, d_vpair, s);
     else
-        launch_f2_umma(c, p.umma, d_f2, d_vpair, s);
+        launch_f2_umma(c, p.umma, d_f2, d_vpair, s, p.per_block);
     if (tev) STPF2_CUDA(cudaEventRecord((*tev)[2], s));
 }
 
@@ -821,6 +825,17 @@ stp_status stp_plan_run_graph(stp_plan* plan, const uint8_t* d_records, double* 
 }
 
 int32_t stp_plan_launches(const stp_plan* plan) { return plan ? plan->p->launches() : 0; }
+
+stp_status stp_plan_set_per_block_launch(stp_plan* plan, int32_t enable) {
+    return guarded([&] {
+        need(plan != nullptr, "null plan");
+        plan->p->per_block = enable != 0;
+        if (plan->p->graph) {  // the captured graph holds the other launch form
+            STPF2_CUDA(cudaGraphExecDestroy(plan->p->graph));
+            plan->p->graph = nullptr;
+        }
+    });
+}
 
 stp_status stp_plan_set_timing(stp_plan* plan, int32_t enable) {
     return guarded([&] {

@@ -221,7 +221,9 @@ void launch_f2_simt(Ctx& c, const WorkItem* items, int n_items, const BlockInfo*
 struct UmmaPlan;
 UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L);
 void umma_plan_destroy(UmmaPlan* p);
-void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s);
+// per_block: one launch per jackknife block instead of one persistent launch over all
+// blocks (the comparison form of the grouped schedule).
+void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s, bool per_block = false);
 // After a stream sync: raises STP_DEVICE_TIMEOUT if the kernel's bounded waits expired.
 void umma_check(UmmaPlan* p);
 int umma_tile();

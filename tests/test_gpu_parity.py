@@ -279,6 +279,24 @@ def test_plan_graph_replay_equals_plan_run(ctx, c1):
     plan.close()
 
 
+def test_per_block_launches_equal_persistent_launch(ctx, uneven):
+    import torch
+
+    p, sel, po, _, _ = uneven
+    rec = torch.as_tensor(p.records_numpy()).cuda()
+    plan = ctx.plan(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision=TC_DEFAULT)
+    n = p.n_pop * p.n_pop * p.n_block
+    out = [torch.full((n,), 3.0, dtype=torch.float64, device="cuda") for _ in range(4)]
+    plan.run(rec, out[0], out[1])
+    plan.set_per_block_launch(True)
+    before = ctx.launches
+    plan.run(rec, out[2], out[3])
+    torch.cuda.synchronize()
+    assert ctx.launches - before == plan.launches == 3 + p.n_block
+    assert torch.equal(out[0], out[2]) and torch.equal(out[1], out[3])
+    plan.close()
+
+
 def test_jackknife_vs_oracle(ctx, c1):
     _, _, _, want, _ = c1
     m = want.P * want.P
