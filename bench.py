@@ -39,7 +39,7 @@ METRIC = "f2 SNPÂ·pop-pairs/s: split-BF16 TC vs plain FP32 on 1 B200, rel err â‰
 UNIT = "SNPÂ·pop-pairs/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # dram__bytes_read.sum + dram__bytes_write.sum of one f2_umma_kernel launch (ncu, one pass).
-CONTRACTION_TRAFFIC = {("c3", "split_f16"): 25.82e9 + 12.41e9}
+CONTRACTION_TRAFFIC = {("c3", "split_f16"): 13.58e9 + 12.24e9}
 
 
 def load_peaks():

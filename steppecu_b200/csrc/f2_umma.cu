@@ -73,10 +73,15 @@ struct UmmaArgs {
     const double* rcp; // rcp[k] = 1/k for k = 0..rcp_max (rcp[0] = 0): vpair never exceeds the block size
     int rcp_max;
     int* err;
+    int* next_item;    // work-item counter, zero at launch
     uint32_t idesc_pp, idesc_am, idesc_i8;
 };
 
+constexpr int kItemRing = 4;  // work items handed from the producer to the other roles
+
 struct SmemCtl {
+    unsigned long long item_full[kItemRing], item_empty[kItemRing];
+    int item_idx[kItemRing];
     unsigned long long full[kStages], empty[kStages];
     unsigned long long acc_full[kNumBufs], acc_empty[kNumBufs];
     unsigned long long vp_full, vp_empty;
@@ -214,9 +219,38 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo_bytes,
 
 __device__ __forceinline__ int stages_of(int k) { return (k + kStageK - 1) / kStageK; }
 
+// Work items are handed out dynamically, in list order (costliest block first, a block's
+// tile pairs together): the producer takes the next item from a global counter and
+// publishes its index to the issuer and the epilogue warps through a small ring, so the
+// CTAs stay within a window of consecutive items and a block's operand images are reused
+// from L2 by all of its tile pairs. Index -1 ends the work.
+__device__ __forceinline__ int take_item(const UmmaArgs& a, SmemCtl* ctl, uint32_t gi, bool& ok) {
+    const int slot = static_cast<int>(gi % kItemRing);
+    ok = wait_bounded(&ctl->item_empty[slot], ((gi / kItemRing) & 1u) ^ 1u, ctl, a.err);
+    if (!ok) return -1;
+    int it = atomicAdd(a.next_item, 1);
+    if (it >= a.n_items) it = -1;
+    *reinterpret_cast<volatile int*>(&ctl->item_idx[slot]) = it;
+    mbar_arrive(&ctl->item_full[slot]);
+    return it;
+}
+
+// Consumer side (one thread): the gi-th item index, or -1 when the work ends or on abort.
+__device__ __forceinline__ int read_item(const UmmaArgs& a, SmemCtl* ctl, uint32_t gi) {
+    const int slot = static_cast<int>(gi % kItemRing);
+    if (!wait_bounded(&ctl->item_full[slot], (gi / kItemRing) & 1u, ctl, a.err)) return -2;
+    const int it = *reinterpret_cast<volatile int*>(&ctl->item_idx[slot]);
+    mbar_arrive(&ctl->item_empty[slot]);
+    return it;
+}
+
 __device__ void producer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl) {
     uint32_t g = 0;
-    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
+    for (uint32_t gi = 0;; ++gi) {
+        bool ok = true;
+        const int it = take_item(a, ctl, gi, ok);
+        if (!ok) goto abort;
+        if (it < 0) break;
         const WorkItem w = a.items[it];
         const BlockInfo bi = a.blocks[w.blk];
         const int nst = stages_of(bi.k);
@@ -247,7 +281,9 @@ abort:
 
 __device__ void mma_issuer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl, uint32_t tmem) {
     uint32_t g = 0, cs = 0, is = 0;
-    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
+    for (uint32_t gi = 0;; ++gi) {
+        const int it = read_item(a, ctl, gi);
+        if (it < 0) break;
         const WorkItem w = a.items[it];
         const BlockInfo bi = a.blocks[w.blk];
         const int nst = stages_of(bi.k);
@@ -317,7 +353,11 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
     const int P = a.P;
     uint32_t cs = 0, is = 0;
     double acc[kCols];  // FP64 running numerator per column
-    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
+    for (uint32_t gi = 0;; ++gi) {
+        int it = 0;
+        if (lane == 0) it = read_item(a, ctl, gi);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it < 0) return;
         const WorkItem w = a.items[it];
         const BlockInfo bi = a.blocks[w.blk];
         const int nst = stages_of(bi.k);
@@ -441,6 +481,10 @@ f2_umma_kernel(const __grid_constant__ UmmaArgs a) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
+        for (int s = 0; s < kItemRing; ++s) {
+            mbar_init(&ctl->item_full[s], 1);
+            mbar_init(&ctl->item_empty[s], 1 + kEpiWarps);  // the issuer and every epilogue warp
+        }
         for (int s = 0; s < kStages; ++s) {
             mbar_init(&ctl->full[s], 1);
             mbar_init(&ctl->empty[s], 1);
@@ -492,13 +536,14 @@ uint32_t idesc_f16(bool bf16, bool negate_a) {
 uint32_t idesc_u8_s32() { return (2u << 4) | (0u << 7) | (0u << 10) | ((kTile >> 3) << 17) | ((kTile >> 4) << 24); }
 
 constexpr size_t kSmemBytes = kStages * kStageBytes + kCtlBytes + kEpiWarps * kStageDoubles * sizeof(double) + 1024;
+static_assert(sizeof(SmemCtl) <= kCtlBytes, "barrier block overflows its slot");
 
 }  // namespace
 
 struct UmmaPlan {
     const uint8_t* images = nullptr;
     int64_t n_ck = 0;
-    DevBuf items, blocks, err, rcp, block_items;
+    DevBuf items, blocks, err, rcp, block_items, counter;
     std::vector<int> block_item_off;  // per block: its tile pairs in block_items
     int n_items = 0;
     int rcp_max = 0;
@@ -529,6 +574,7 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
     p->items.reserve(std::max<size_t>(items.size() * sizeof(WorkItem), 16));
     p->blocks.reserve(std::max<size_t>(L.blocks.size() * sizeof(BlockInfo), 16));
     p->err.reserve(16);
+    p->counter.reserve(16);
     STPF2_CUDA(cudaMemcpyAsync(p->items.ptr, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
                                c.stream));
     STPF2_CUDA(cudaMemcpyAsync(p->blocks.ptr, L.blocks.data(), L.blocks.size() * sizeof(BlockInfo),
@@ -575,6 +621,8 @@ void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, 
     a.n_ck = p->n_ck;
     a.items = items;
     a.n_items = n_items;
+    a.next_item = p->counter.as<int>();
+    STPF2_CUDA(cudaMemsetAsync(a.next_item, 0, sizeof(int), s));
     a.blocks = p->blocks.as<BlockInfo>();
     a.P = p->P;
     a.f2 = f2;
