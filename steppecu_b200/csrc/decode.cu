@@ -196,105 +196,132 @@ __device__ __forceinline__ uint32_t transpose4x4_2bit(uint32_t w) {
     return w;
 }
 
-constexpr int kSliceWords = 64;                      // 1024 samples per transpose CTA
+constexpr int kSliceWords = 64;                      // 1024 samples per staged slice
 constexpr int kSliceBytes = kSliceWords * 4;
-constexpr int kRowStride = kSliceWords + 1;          // words per staged record row
+constexpr int kRowStride = kSliceWords + 4;          // words per staged record row (16-byte rows)
 constexpr int kStagedWords = 4 * kTileCols * kRowStride + 32;
+constexpr size_t kTransSmemBytes = 2 * kStagedWords * sizeof(uint32_t);
 
-// Pass 1: SNP-major records -> canonical quads, gathering the selected samples. One CTA per
-// (quad of 128 columns, slice of 1024 samples): it stages 128 record slices of 256 bytes
-// (coalesced 128-bit loads), then thread (word w, tile sub) transposes 16 samples x 32
-// columns with SWAR 4x4 transposes; the four threads of a sample write its 32-byte sector
-// together. Slice 0 also computes each column's centre c_s: the pooled frequency of the
-// called genotypes among the record's first 256 samples, rounded to 1/256 (f2 is exact for
-// any per-SNP centre; this one only keeps the operand magnitudes small).
-__global__ void __launch_bounds__(kTransThreads)
-transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t n_ind,
-                    const TileInfo* __restrict__ tiles, int64_t n_tiles, const int32_t* __restrict__ pos,
-                    int64_t n_sel, uint64_t* __restrict__ canon, double* __restrict__ center) {
-    __shared__ uint32_t srec[kStagedWords];
-    const int64_t q = blockIdx.x;
-    const int64_t slice = blockIdx.y;
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+
+// Stages slice `slice` of the quad's 128 records into buf: row (sub, r) at word
+// (sub*32 + r)*kRowStride + sub*8 (the sub*8 skew keeps the threads of one warp on
+// distinct banks when they read it back); bytes past the record, rows past the tile's
+// SNPs and tiles past the last hold code 3 (missing).
+__device__ __forceinline__ void stage_slice(uint32_t* buf, const uint8_t* __restrict__ records, uint64_t pitch,
+                                            const TileInfo* __restrict__ tiles, int64_t n_tiles, int64_t q,
+                                            int64_t slice) {
     const uint64_t byte0 = static_cast<uint64_t>(slice) * kSliceBytes;
-    // Stage: 4 tiles x 32 rows x 256 bytes; row (sub, r) at word (sub*32 + r)*kRowStride + sub*8
-    // (the sub*8 skew keeps the threads of one warp on distinct banks).
     for (int c = threadIdx.x; c < 4 * kTileCols * (kSliceBytes / 16); c += blockDim.x) {
         const int row = c / (kSliceBytes / 16), k = c % (kSliceBytes / 16);
         const int sub = row / kTileCols, r = row % kTileCols;
         const int64_t t = 4 * q + sub;
-        uint4 v = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+        uint32_t* d = buf + (sub * kTileCols + r) * kRowStride + sub * 8 + k * 4;
+        bool loaded = false;
         if (t < n_tiles) {
             const TileInfo ti = tiles[t];
             const uint64_t b = byte0 + static_cast<uint64_t>(k) * 16;
-            if (r < ti.nvalid && b < pitch)
-                v = __ldg(reinterpret_cast<const uint4*>(records + (static_cast<int64_t>(ti.snp0) + r) * pitch + b));
+            if (r < ti.nvalid && b < pitch) {
+                cp_async16(d, records + (static_cast<int64_t>(ti.snp0) + r) * pitch + b);
+                loaded = true;
+            }
         }
-        uint32_t* d = srec + (sub * kTileCols + r) * kRowStride + sub * 8 + k * 4;
-        d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+        if (!loaded) *reinterpret_cast<uint4*>(d) = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
     }
-    __syncthreads();
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
 
+// Pass 1: SNP-major records -> canonical quads, gathering the selected samples. One CTA per
+// quad of 128 columns walks the record slices of 1024 samples, staging slice s+1 with
+// cp.async while it transposes slice s: thread (word w, tile sub) transposes 16 samples x
+// 32 columns with SWAR 4x4 transposes, and the four threads of a sample write its 32-byte
+// sector together. The first slice also yields each column's centre c_s: the pooled
+// frequency of the called genotypes among the record's first 256 samples, rounded to 1/256
+// (f2 is exact for any per-SNP centre; this one only keeps the operand magnitudes small).
+__global__ void __launch_bounds__(kTransThreads)
+transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t n_ind,
+                    const TileInfo* __restrict__ tiles, int64_t n_tiles, const int32_t* __restrict__ pos,
+                    int64_t n_sel, int64_t n_slices, uint64_t* __restrict__ canon, double* __restrict__ center) {
+    extern __shared__ __align__(16) uint32_t srec_all[];
+    const int64_t q = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (slice == 0 && warp < 4) {
-        const int sub = warp;
-        const int64_t t = 4 * q + sub;
-        const int nvalid = t < n_tiles ? tiles[t].nvalid : 0;
-        const int64_t rem = n_ind - static_cast<int64_t>(lane) * 16;
-        const int nv = lane < 16 ? static_cast<int>(rem < 0 ? 0 : (rem < 16 ? rem : 16)) : 0;
-        uint32_t vmask = 0;
-        for (int m = 0; m < nv; ++m) vmask |= 3u << (8 * (m >> 2) + 6 - 2 * (m & 3));
-        for (int r = 0; r < kTileCols; ++r) {
-            const uint32_t x = (nv > 0 ? srec[(sub * kTileCols + r) * kRowStride + sub * 8 + lane] : 0u) & vmask;
-            const uint32_t lo = x & 0x55555555u, hi = (x >> 1) & 0x55555555u;
-            const uint32_t miss = lo & hi;
-            const int cnt = __reduce_add_sync(0xffffffffu, __popc(vmask & 0x55555555u) - __popc(miss));
-            const int sum = __reduce_add_sync(0xffffffffu, __popc(lo & ~miss) + 2 * __popc(hi & ~miss));
-            if (lane == 0 && t < n_tiles)
-                center[t * kTileCols + r] =
-                    (r < nvalid && cnt > 0) ? rint((static_cast<double>(sum) / (2.0 * cnt)) * 256.0) / 256.0 : 0.5;
-        }
-    }
-
-    const int sub = threadIdx.x & 3;
-    for (int wl = threadIdx.x >> 2; wl < kSliceWords; wl += blockDim.x >> 2) {
-        const int64_t r0 = slice * (kSliceWords * 16) + static_cast<int64_t>(wl) * 16;
-        const int64_t rem = n_ind - r0;
-        if (rem <= 0) break;
-        const int nv = static_cast<int>(rem < 16 ? rem : 16);
-        uint64_t out[16];
-#pragma unroll
-        for (int m = 0; m < 16; ++m) out[m] = 0;
-        const uint32_t* base = srec + sub * kTileCols * kRowStride + sub * 8 + wl;
-#pragma unroll
-        for (int rg = 0; rg < kTileCols / 4; ++rg) {
-            uint32_t rw[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) rw[r] = base[(4 * rg + r) * kRowStride];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const uint32_t sel = static_cast<uint32_t>(j) | (static_cast<uint32_t>(j + 4) << 4);
-                const uint32_t a = __byte_perm(rw[0], rw[1], sel);
-                const uint32_t b = __byte_perm(rw[2], rw[3], sel);
-                const uint32_t y = transpose4x4_2bit(__byte_perm(a, b, 0x0145));
-#pragma unroll
-                for (int m = 0; m < 4; ++m)
-                    out[4 * j + m] |= static_cast<uint64_t>((y >> (8 * (3 - m))) & 0xFFu) << (8 * rg);
-            }
-        }
-        int32_t g[16];
-        if (nv == 16) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int4 v = __ldg(reinterpret_cast<const int4*>(pos + r0) + k);
-                g[4 * k] = v.x; g[4 * k + 1] = v.y; g[4 * k + 2] = v.z; g[4 * k + 3] = v.w;
-            }
+    stage_slice(srec_all, records, pitch, tiles, n_tiles, q, 0);
+    for (int64_t slice = 0; slice < n_slices; ++slice) {
+        uint32_t* srec = srec_all + (slice & 1) * kStagedWords;
+        if (slice + 1 < n_slices) {
+            stage_slice(srec_all + ((slice + 1) & 1) * kStagedWords, records, pitch, tiles, n_tiles, q, slice + 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
         } else {
-#pragma unroll
-            for (int m = 0; m < 16; ++m) g[m] = m < nv ? __ldg(pos + r0 + m) : -1;
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
+        __syncthreads();
+
+        if (slice == 0 && warp < 4) {
+            const int sub = warp;
+            const int64_t t = 4 * q + sub;
+            const int nvalid = t < n_tiles ? tiles[t].nvalid : 0;
+            const int64_t rem = n_ind - static_cast<int64_t>(lane) * 16;
+            const int nv = lane < 16 ? static_cast<int>(rem < 0 ? 0 : (rem < 16 ? rem : 16)) : 0;
+            uint32_t vmask = 0;
+            for (int m = 0; m < nv; ++m) vmask |= 3u << (8 * (m >> 2) + 6 - 2 * (m & 3));
+            for (int r = 0; r < kTileCols; ++r) {
+                const uint32_t x = (nv > 0 ? srec[(sub * kTileCols + r) * kRowStride + sub * 8 + lane] : 0u) & vmask;
+                const uint32_t lo = x & 0x55555555u, hi = (x >> 1) & 0x55555555u;
+                const uint32_t miss = lo & hi;
+                const int cnt = __reduce_add_sync(0xffffffffu, __popc(vmask & 0x55555555u) - __popc(miss));
+                const int sum = __reduce_add_sync(0xffffffffu, __popc(lo & ~miss) + 2 * __popc(hi & ~miss));
+                if (lane == 0 && t < n_tiles)
+                    center[t * kTileCols + r] =
+                        (r < nvalid && cnt > 0) ? rint((static_cast<double>(sum) / (2.0 * cnt)) * 256.0) / 256.0 : 0.5;
+            }
+        }
+
+        const int sub = threadIdx.x & 3;
+        for (int wl = threadIdx.x >> 2; wl < kSliceWords; wl += blockDim.x >> 2) {
+            const int64_t r0 = slice * (kSliceWords * 16) + static_cast<int64_t>(wl) * 16;
+            const int64_t rem = n_ind - r0;
+            if (rem <= 0) break;
+            const int nv = static_cast<int>(rem < 16 ? rem : 16);
+            uint64_t out[16];
 #pragma unroll
-        for (int m = 0; m < 16; ++m)
-            if (g[m] >= 0) canon[(q * n_sel + g[m]) * 4 + sub] = out[m];
+            for (int m = 0; m < 16; ++m) out[m] = 0;
+            const uint32_t* base = srec + sub * kTileCols * kRowStride + sub * 8 + wl;
+#pragma unroll
+            for (int rg = 0; rg < kTileCols / 4; ++rg) {
+                uint32_t rw[4];
+#pragma unroll
+                for (int r = 0; r < 4; ++r) rw[r] = base[(4 * rg + r) * kRowStride];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const uint32_t sel = static_cast<uint32_t>(j) | (static_cast<uint32_t>(j + 4) << 4);
+                    const uint32_t a = __byte_perm(rw[0], rw[1], sel);
+                    const uint32_t b = __byte_perm(rw[2], rw[3], sel);
+                    const uint32_t y = transpose4x4_2bit(__byte_perm(a, b, 0x0145));
+#pragma unroll
+                    for (int m = 0; m < 4; ++m)
+                        out[4 * j + m] |= static_cast<uint64_t>((y >> (8 * (3 - m))) & 0xFFu) << (8 * rg);
+                }
+            }
+            int32_t g[16];
+            if (nv == 16) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int4 v = __ldg(reinterpret_cast<const int4*>(pos + r0) + k);
+                    g[4 * k] = v.x; g[4 * k + 1] = v.y; g[4 * k + 2] = v.z; g[4 * k + 3] = v.w;
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < 16; ++m) g[m] = m < nv ? __ldg(pos + r0 + m) : -1;
+            }
+#pragma unroll
+            for (int m = 0; m < 16; ++m)
+                if (g[m] >= 0) canon[(q * n_sel + g[m]) * 4 + sub] = out[m];
+        }
+        __syncthreads();  // this buffer is restaged two slices later
     }
 }
 
@@ -593,9 +620,14 @@ void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t
         fail(STP_INVALID_ARGUMENT, "transpose: genotype records need a 16-byte aligned pitch");
     const int64_t n_quads = (n_tiles + 3) / 4;
     const int64_t n_slices = std::max<int64_t>(1, (n_ind + kSliceWords * 16 - 1) / (kSliceWords * 16));
-    if (n_slices > 65535) fail(STP_INVALID_ARGUMENT, "transpose: too many samples in a record");
-    const dim3 grid(static_cast<unsigned>(n_quads), static_cast<unsigned>(n_slices));
-    transpose_pa_kernel<<<grid, kTransThreads, 0, s>>>(records, pitch, n_ind, tiles, n_tiles, pos, n_sel, canon, center);
+    static bool attr_set[64] = {};  // per device ordinal
+    if (c.device < 0 || c.device >= 64 || !attr_set[c.device]) {
+        STPF2_CUDA(cudaFuncSetAttribute(transpose_pa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(kTransSmemBytes)));
+        if (c.device >= 0 && c.device < 64) attr_set[c.device] = true;
+    }
+    transpose_pa_kernel<<<static_cast<unsigned>(n_quads), kTransThreads, kTransSmemBytes, s>>>(
+        records, pitch, n_ind, tiles, n_tiles, pos, n_sel, n_slices, canon, center);
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
 }
