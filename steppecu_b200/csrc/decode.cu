@@ -208,10 +208,19 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
                  : "memory");
 }
 
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+
 // Stages slice `slice` of the quad's 128 records into buf: row (sub, r) at word
 // (sub*32 + r)*kRowStride + sub*8 (the sub*8 skew keeps the threads of one warp on
 // distinct banks when they read it back); bytes past the record, rows past the tile's
-// SNPs and tiles past the last hold code 3 (missing).
+// SNPs and tiles past the last hold code 3 (missing). kVec16: records and pitch are
+// 16-byte aligned (16-byte copies); otherwise 4-byte aligned (4-byte copies, so a host
+// panel keeps its own pitch on the device).
+template <bool kVec16>
 __device__ __forceinline__ void stage_slice(uint32_t* buf, const uint8_t* __restrict__ records, uint64_t pitch,
                                             const TileInfo* __restrict__ tiles, int64_t n_tiles, int64_t q,
                                             int64_t slice) {
@@ -221,16 +230,22 @@ __device__ __forceinline__ void stage_slice(uint32_t* buf, const uint8_t* __rest
         const int sub = row / kTileCols, r = row % kTileCols;
         const int64_t t = 4 * q + sub;
         uint32_t* d = buf + (sub * kTileCols + r) * kRowStride + sub * 8 + k * 4;
-        bool loaded = false;
+        const uint64_t b = byte0 + static_cast<uint64_t>(k) * 16;
+        const uint8_t* src = nullptr;
         if (t < n_tiles) {
             const TileInfo ti = tiles[t];
-            const uint64_t b = byte0 + static_cast<uint64_t>(k) * 16;
-            if (r < ti.nvalid && b < pitch) {
-                cp_async16(d, records + (static_cast<int64_t>(ti.snp0) + r) * pitch + b);
-                loaded = true;
+            if (r < ti.nvalid) src = records + (static_cast<int64_t>(ti.snp0) + r) * pitch;
+        }
+        if constexpr (kVec16) {
+            if (src && b < pitch) cp_async16(d, src + b);
+            else *reinterpret_cast<uint4*>(d) = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+        } else {
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                if (src && b + 4 * w < pitch) cp_async4(d + w, src + b + 4 * w);
+                else d[w] = 0xFFFFFFFFu;
             }
         }
-        if (!loaded) *reinterpret_cast<uint4*>(d) = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
@@ -242,6 +257,7 @@ __device__ __forceinline__ void stage_slice(uint32_t* buf, const uint8_t* __rest
 // sector together. The first slice also yields each column's centre c_s: the pooled
 // frequency of the called genotypes among the record's first 256 samples, rounded to 1/256
 // (f2 is exact for any per-SNP centre; this one only keeps the operand magnitudes small).
+template <bool kVec16>
 __global__ void __launch_bounds__(kTransThreads)
 transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t n_ind,
                     const TileInfo* __restrict__ tiles, int64_t n_tiles, const int32_t* __restrict__ pos,
@@ -249,11 +265,11 @@ transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t
     extern __shared__ __align__(16) uint32_t srec_all[];
     const int64_t q = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    stage_slice(srec_all, records, pitch, tiles, n_tiles, q, 0);
+    stage_slice<kVec16>(srec_all, records, pitch, tiles, n_tiles, q, 0);
     for (int64_t slice = 0; slice < n_slices; ++slice) {
         uint32_t* srec = srec_all + (slice & 1) * kStagedWords;
         if (slice + 1 < n_slices) {
-            stage_slice(srec_all + ((slice + 1) & 1) * kStagedWords, records, pitch, tiles, n_tiles, q, slice + 1);
+            stage_slice<kVec16>(srec_all + ((slice + 1) & 1) * kStagedWords, records, pitch, tiles, n_tiles, q, slice + 1);
             asm volatile("cp.async.wait_group 1;" ::: "memory");
         } else {
             asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -396,8 +412,8 @@ __global__ void __launch_bounds__(kDecThreads2, 4)
 decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t n_sel,
                     const uint32_t* __restrict__ sel, const int32_t* __restrict__ pop_off, int P,
                     const double* __restrict__ center, const double* __restrict__ rec_n,
-                    const double* __restrict__ rec_nm1, const int32_t* __restrict__ col_snp, OperandPlanes op,
-                    int32_t* __restrict__ cnt_ac2, int32_t* __restrict__ cnt_n) {
+                    const double* __restrict__ rec_nm1, const int32_t* __restrict__ col_snp, int64_t col_base,
+                    OperandPlanes op, int32_t* __restrict__ cnt_ac2, int32_t* __restrict__ cnt_n) {
     extern __shared__ uint32_t s_cnt[];
     __shared__ double s_center[4 * kCenterPitch];
     const int64_t q = blockIdx.x;
@@ -495,7 +511,7 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
             tm.pt[c] = static_cast<float>(pt);
             tm.ah[c] = static_cast<float>(ah);
         }
-        emit8<F>(op, i, col0, tm);
+        emit8<F>(op, i, col_base + col0, tm);
     }
 }
 
@@ -616,18 +632,23 @@ void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t
                          int64_t n_tiles, const int32_t* pos, int64_t n_sel, uint64_t* canon, double* center,
                          cudaStream_t s) {
     if (n_tiles <= 0) return;
-    if (pitch % 16 != 0 || reinterpret_cast<uintptr_t>(records) % 16 != 0)
-        fail(STP_INVALID_ARGUMENT, "transpose: genotype records need a 16-byte aligned pitch");
+    const uint64_t align = pitch | static_cast<uint64_t>(reinterpret_cast<uintptr_t>(records));
+    if (align % 4 != 0) fail(STP_INVALID_ARGUMENT, "transpose: genotype records need a 4-byte aligned pitch");
+    const bool vec16 = align % 16 == 0;
     const int64_t n_quads = (n_tiles + 3) / 4;
     const int64_t n_slices = std::max<int64_t>(1, (n_ind + kSliceWords * 16 - 1) / (kSliceWords * 16));
-    static bool attr_set[64] = {};  // per device ordinal
-    if (c.device < 0 || c.device >= 64 || !attr_set[c.device]) {
-        STPF2_CUDA(cudaFuncSetAttribute(transpose_pa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(kTransSmemBytes)));
-        if (c.device >= 0 && c.device < 64) attr_set[c.device] = true;
+    static bool attr_set[2][64] = {};  // per form and device ordinal
+    if (c.device < 0 || c.device >= 64 || !attr_set[vec16][c.device]) {
+        STPF2_CUDA(cudaFuncSetAttribute(vec16 ? transpose_pa_kernel<true> : transpose_pa_kernel<false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kTransSmemBytes)));
+        if (c.device >= 0 && c.device < 64) attr_set[vec16][c.device] = true;
     }
-    transpose_pa_kernel<<<static_cast<unsigned>(n_quads), kTransThreads, kTransSmemBytes, s>>>(
-        records, pitch, n_ind, tiles, n_tiles, pos, n_sel, n_slices, canon, center);
+    if (vec16)
+        transpose_pa_kernel<true><<<static_cast<unsigned>(n_quads), kTransThreads, kTransSmemBytes, s>>>(
+            records, pitch, n_ind, tiles, n_tiles, pos, n_sel, n_slices, canon, center);
+    else
+        transpose_pa_kernel<false><<<static_cast<unsigned>(n_quads), kTransThreads, kTransSmemBytes, s>>>(
+            records, pitch, n_ind, tiles, n_tiles, pos, n_sel, n_slices, canon, center);
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
 }
@@ -635,7 +656,7 @@ void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t
 void launch_decode_canon(Ctx& c, const CanonDecodeArgs& a, cudaStream_t s) {
     if (a.P <= 0 || a.n_tiles <= 0) return;
     const dim3 grid(static_cast<unsigned>((a.n_tiles + 3) / 4), static_cast<unsigned>((a.P + kDecPops - 1) / kDecPops));
-#define STPF2_DECODE_ARGS a.canon, a.n_tiles, a.n_sel, a.sel, a.pop_off, a.P, a.center, a.rec_n, a.rec_nm1, a.col_snp, a.op, a.cnt_ac2, a.cnt_n
+#define STPF2_DECODE_ARGS a.canon, a.n_tiles, a.n_sel, a.sel, a.pop_off, a.P, a.center, a.rec_n, a.rec_nm1, a.col_snp, a.col_base, a.op, a.cnt_ac2, a.cnt_n
     switch (a.op.fmt) {
         case OpFmt::F32: decode_canon_kernel<OpFmt::F32><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS); break;
         case OpFmt::BF16: decode_canon_kernel<OpFmt::BF16><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS); break;

@@ -614,6 +614,13 @@ void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t
     launch_umma_items(c, p, p->items.as<WorkItem>(), p->n_items, f2, vpair, s);
 }
 
+void launch_f2_umma_blocks(Ctx& c, UmmaPlan* p, int b0, int b1, double* f2, double* vpair, cudaStream_t s) {
+    if (!p || b1 <= b0) return;
+    const int n = p->block_item_off[static_cast<size_t>(b1)] - p->block_item_off[static_cast<size_t>(b0)];
+    if (n > 0)
+        launch_umma_items(c, p, p->block_items.as<WorkItem>() + p->block_item_off[static_cast<size_t>(b0)], n, f2, vpair, s);
+}
+
 void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, double* f2, double* vpair,
                        cudaStream_t s) {
     UmmaArgs a{};

@@ -275,12 +275,13 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
     p->canon.reserve(std::max<size_t>(static_cast<size_t>((p->n_tiles + 3) / 4) * p->n_sel_pad * 32, 64));
     p->center.reserve(std::max<size_t>(static_cast<size_t>(p->L.ld) * 8, 64));
 
-    // The transpose reads records with 16-byte loads: records of another pitch are copied
-    // once per run into a 16-byte pitch.
+    // The transpose reads records with 4-byte (16-byte when aligned so) copies: records of
+    // a pitch that is not a multiple of 4 are copied once per run into a 16-byte pitch.
     p->bpr = r.geno.bytes_per_record;
     p->src_pitch = pitch;
     const uint64_t need_bytes = static_cast<uint64_t>((r.geno.n_ind + 63) / 64) * 16;
-    p->repitch = (pitch % 16 != 0) || pitch < need_bytes || (r.geno.on_device && reinterpret_cast<uintptr_t>(r.geno.records) % 16 != 0);
+    p->repitch = (pitch % 4 != 0) || pitch < static_cast<uint64_t>((r.geno.n_ind + 3) / 4) ||
+                 (r.geno.on_device && reinterpret_cast<uintptr_t>(r.geno.records) % 4 != 0);
     if (p->repitch) {
         p->pitch = (std::max<uint64_t>(r.geno.bytes_per_record, need_bytes) + 15) / 16 * 16;
         p->repitched.reserve(std::max<size_t>(static_cast<size_t>(p->pitch) * r.geno.n_snp, 64));
@@ -308,29 +309,36 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
 
 // Ploidy (when detected) -> transpose to canonical tiles -> per-population decode into the
 // operand planes (and, for tests, the integer counts).
-void launch_decode(Plan& p, const uint8_t* d_records, int32_t* cnt_ac2, int32_t* cnt_n, cudaStream_t s) {
+// Tiles [t0, t1) only (t1 < 0: to the end): a tile range whose canonical quads and
+// centres are indexed from t0, for the pipelined host-buffer path; detect runs the ploidy
+// pass first (it reads the first min(1000, M) SNPs).
+void launch_decode(Plan& p, const uint8_t* d_records, int32_t* cnt_ac2, int32_t* cnt_n, cudaStream_t s,
+                   int64_t t0 = 0, int64_t t1 = -1, bool detect = true) {
     Ctx& c = *p.ctx;
     if (p.n_snp <= 0) return;
+    if (t1 < 0) t1 = p.n_tiles;
     const uint8_t* rec = d_records;
     if (p.repitch) {
         STPF2_CUDA(cudaMemcpy2DAsync(p.repitched.ptr, p.pitch, d_records, p.src_pitch, p.bpr,
                                      static_cast<size_t>(p.n_snp), cudaMemcpyDeviceToDevice, s));
         rec = p.repitched.as<uint8_t>();
     }
-    if (p.detect) launch_detect_ploidy_pa(c, rec, p.pitch, p.n_snp, p.sel.as<uint32_t>(), p.n_sel, s);
-    launch_transpose_pa(c, rec, p.pitch, p.n_ind, p.tiles.as<TileInfo>(), p.n_tiles, p.pos.as<int32_t>(), p.n_sel_pad,
-                        p.canon.as<uint64_t>(), p.center.as<double>(), s);
+    if (p.detect && detect) launch_detect_ploidy_pa(c, rec, p.pitch, p.n_snp, p.sel.as<uint32_t>(), p.n_sel, s);
+    if (t1 <= t0) return;
+    launch_transpose_pa(c, rec, p.pitch, p.n_ind, p.tiles.as<TileInfo>() + t0, t1 - t0, p.pos.as<int32_t>(),
+                        p.n_sel_pad, p.canon.as<uint64_t>(), p.center.as<double>() + t0 * kTileK, s);
     CanonDecodeArgs a;
     a.canon = p.canon.as<uint64_t>();
-    a.n_tiles = p.n_tiles;
+    a.n_tiles = t1 - t0;
     a.n_sel = p.n_sel_pad;
     a.sel = p.sel.as<uint32_t>();
     a.pop_off = p.pop_off.as<int32_t>();
     a.P = p.P;
-    a.center = p.center.as<double>();
+    a.center = p.center.as<double>() + t0 * kTileK;
     a.rec_n = p.rec_n.as<double>();
     a.rec_nm1 = p.rec_nm1.as<double>();
-    a.col_snp = p.col_snp.as<int32_t>();
+    a.col_snp = p.col_snp.as<int32_t>() + t0 * kTileK;
+    a.col_base = t0 * kTileK;
     a.op = p.op;
     if (cnt_ac2) a.op.planes = nullptr;
     a.cnt_ac2 = cnt_ac2;
@@ -370,6 +378,86 @@ void copy_block_sizes(const BlockLayout& L, int32_t* out) {
     for (int b = 0; b < L.n_block; ++b) out[b] = L.blocks[b].k;
 }
 
+// Device pitch for host records: their own pitch when the transpose can read it (a
+// multiple of 4 bytes), so the upload is one contiguous copy; else rounded up to 16.
+uint64_t device_pitch(const stp_geno_view& g) {
+    const uint64_t hp = g.pitch ? g.pitch : g.bytes_per_record;
+    return hp % 4 == 0 ? hp : (g.bytes_per_record + 15) / 16 * 16;
+}
+
+// Copies record rows [s0, s0 + n) from the host into d (pitch dp) on stream st: one
+// contiguous copy when the pitches agree (the last row only up to bytes_per_record, which
+// is all a host buffer is sure to hold), else a pitched copy.
+void upload_rows(const stp_geno_view& g, uint8_t* d, uint64_t dp, int64_t s0, int64_t n, cudaStream_t st) {
+    if (n <= 0) return;
+    const uint64_t hp = g.pitch ? g.pitch : g.bytes_per_record;
+    if (hp == dp) {
+        const size_t bytes = static_cast<size_t>(n - 1) * hp + g.bytes_per_record;
+        STPF2_CUDA(cudaMemcpyAsync(d + s0 * static_cast<int64_t>(dp), g.records + s0 * static_cast<int64_t>(hp), bytes,
+                                   cudaMemcpyHostToDevice, st));
+    } else {
+        STPF2_CUDA(cudaMemcpy2DAsync(d + s0 * static_cast<int64_t>(dp), dp, g.records + s0 * static_cast<int64_t>(hp), hp,
+                                     g.bytes_per_record, static_cast<size_t>(n), cudaMemcpyHostToDevice, st));
+    }
+}
+
+// Host buffers in and out, tensor-core arithmetic: the pass runs in segments of whole
+// blocks (about a twelfth of the SNPs each, the first covering the ploidy window) so the
+// upload of segment k+1, the decode and contraction of segment k and the download of
+// segment k-1's f2 / vpair slabs overlap on three streams. A segment's records are a
+// contiguous run of SNP rows, its operand columns a tile range, its output a contiguous
+// run of block slabs.
+void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, uint8_t* d_rec, uint64_t dp,
+                   double* d_f2, double* d_vp) {
+    const BlockLayout& L = p.L;
+    const int B = L.n_block;
+    const int64_t M = L.n_snp;
+    const size_t slab = static_cast<size_t>(p.P) * static_cast<size_t>(p.P);
+    const int64_t window = std::min<int64_t>(M, 1000);
+    const int64_t target = std::max<int64_t>((M + 11) / 12, window);
+    std::vector<int> bounds{0};
+    int64_t acc = 0;
+    for (int b = 0; b < B; ++b) {
+        acc += L.blocks[b].k;
+        if (acc >= target && b + 1 < B) {
+            bounds.push_back(b + 1);
+            acc = 0;
+        }
+    }
+    bounds.push_back(B);
+    const size_t nseg = bounds.size() - 1;
+    std::vector<cudaEvent_t> ev(2 * nseg, nullptr);
+    struct Free {
+        std::vector<cudaEvent_t>& ev;
+        ~Free() {
+            for (auto e : ev)
+                if (e) cudaEventDestroy(e);
+        }
+    } free_events{ev};
+    for (auto& e : ev) STPF2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    int64_t snp0 = 0;
+    for (size_t k = 0; k < nseg; ++k) {
+        const int b0 = bounds[k], b1 = bounds[k + 1];
+        int64_t nsnp = 0;
+        for (int b = b0; b < b1; ++b) nsnp += L.blocks[b].k;
+        const int64_t t0 = L.blocks[b0].col / kTileK;
+        const int64_t t1 = (b1 < B ? L.blocks[b1].col : L.ld) / kTileK;
+        upload_rows(r.geno, d_rec, dp, snp0, nsnp, c.h2d);
+        STPF2_CUDA(cudaEventRecord(ev[2 * k], c.h2d));
+        STPF2_CUDA(cudaStreamWaitEvent(c.stream, ev[2 * k], 0));
+        launch_decode(p, d_rec, nullptr, nullptr, c.stream, t0, t1, k == 0);
+        launch_f2_umma_blocks(c, p.umma, b0, b1, d_f2, d_vp, c.stream);
+        STPF2_CUDA(cudaEventRecord(ev[2 * k + 1], c.stream));
+        STPF2_CUDA(cudaStreamWaitEvent(c.d2h, ev[2 * k + 1], 0));
+        const size_t bytes = slab * static_cast<size_t>(b1 - b0) * sizeof(double);
+        STPF2_CUDA(cudaMemcpyAsync(o.f2 + slab * b0, d_f2 + slab * b0, bytes, cudaMemcpyDeviceToHost, c.d2h));
+        STPF2_CUDA(cudaMemcpyAsync(o.vpair + slab * b0, d_vp + slab * b0, bytes, cudaMemcpyDeviceToHost, c.d2h));
+        snp0 += nsnp;
+    }
+    STPF2_CUDA(cudaStreamSynchronize(c.d2h));
+    STPF2_CUDA(cudaStreamSynchronize(c.stream));
+}
+
 void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
     need(o.f2 != nullptr || r.n_pop == 0 || r.n_block == 0, "output f2 is NULL");
     need(o.vpair != nullptr || r.n_pop == 0 || r.n_block == 0, "output vpair is NULL");
@@ -377,12 +465,15 @@ void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
     const uint8_t* d_rec = r.geno.records;
     uint64_t pitch = r.geno.pitch ? r.geno.pitch : r.geno.bytes_per_record;
     need(pitch >= r.geno.bytes_per_record, "pitch < bytes_per_record");
-    if (!r.geno.on_device && r.geno.n_snp > 0) {
+    const bool host_in = !r.geno.on_device && r.geno.n_snp > 0;
+    const bool pipelined = host_in && !o.on_device && r.precision != STP_PREC_FP32_SIMT && r.n_pop > 0 &&
+                           r.n_block >= 2;
+    uint64_t dp = 0;
+    if (host_in) {
         need(r.geno.records != nullptr, "records is NULL");
-        const uint64_t dp = (r.geno.bytes_per_record + 15) / 16 * 16;
+        dp = device_pitch(r.geno);
         c.ws_records.reserve(static_cast<size_t>(dp) * r.geno.n_snp);
-        STPF2_CUDA(cudaMemcpy2DAsync(c.ws_records.ptr, dp, r.geno.records, pitch, r.geno.bytes_per_record,
-                                     static_cast<size_t>(r.geno.n_snp), cudaMemcpyHostToDevice, s));
+        if (!pipelined) upload_rows(r.geno, c.ws_records.as<uint8_t>(), dp, 0, r.geno.n_snp, s);
         d_rec = c.ws_records.as<uint8_t>();
         pitch = dp;
     }
@@ -402,10 +493,16 @@ void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
         d_f2 = c.ws_f2.as<double>();
         d_vp = c.ws_vpair.as<double>();
     }
-    run_plan(*p, d_rec, d_f2, d_vp, s);
-    if (!o.on_device && out_elems) {
-        STPF2_CUDA(cudaMemcpyAsync(o.f2, d_f2, out_elems * sizeof(double), cudaMemcpyDeviceToHost, s));
-        STPF2_CUDA(cudaMemcpyAsync(o.vpair, d_vp, out_elems * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (pipelined && p->umma && !p->repitch && out_elems) {
+        STPF2_CUDA(cudaStreamSynchronize(s));  // the plan's tables are uploaded on s
+        run_pipelined(c, r, o, *p, c.ws_records.as<uint8_t>(), dp, d_f2, d_vp);
+    } else {
+        if (pipelined) upload_rows(r.geno, c.ws_records.as<uint8_t>(), dp, 0, r.geno.n_snp, s);
+        run_plan(*p, d_rec, d_f2, d_vp, s);
+        if (!o.on_device && out_elems) {
+            STPF2_CUDA(cudaMemcpyAsync(o.f2, d_f2, out_elems * sizeof(double), cudaMemcpyDeviceToHost, s));
+            STPF2_CUDA(cudaMemcpyAsync(o.vpair, d_vp, out_elems * sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
     }
     if (o.ploidy_out && p->n_sel > 0) {
         std::vector<uint32_t> sel(static_cast<size_t>(p->n_sel));
@@ -450,6 +547,8 @@ stp_ctx* stp_create(int device, stp_status* status) {
         c->device = device;
         STPF2_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
         STPF2_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        STPF2_CUDA(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+        STPF2_CUDA(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
         out = c.release();
     });
     if (status) *status = st;
@@ -459,9 +558,11 @@ stp_ctx* stp_create(int device, stp_status* status) {
 void stp_destroy(stp_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    if (ctx->stream) {
-        cudaStreamSynchronize(ctx->stream);
-        cudaStreamDestroy(ctx->stream);
+    for (cudaStream_t s : {ctx->stream, ctx->h2d, ctx->d2h}) {
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
     }
     delete ctx;
 }
@@ -523,10 +624,9 @@ stp_status stp_decode_counts(stp_ctx* ctx, const stp_geno_view* geno, const int6
         uint64_t pitch = geno->pitch ? geno->pitch : geno->bytes_per_record;
         DevBuf rec;
         if (!geno->on_device) {
-            const uint64_t dp = (geno->bytes_per_record + 15) / 16 * 16;
+            const uint64_t dp = device_pitch(*geno);
             rec.reserve(static_cast<size_t>(dp) * geno->n_snp);
-            STPF2_CUDA(cudaMemcpy2DAsync(rec.ptr, dp, geno->records, pitch, geno->bytes_per_record,
-                                         static_cast<size_t>(geno->n_snp), cudaMemcpyHostToDevice, s));
+            upload_rows(*geno, rec.as<uint8_t>(), dp, 0, geno->n_snp, s);
             d_rec = rec.as<uint8_t>();
             pitch = dp;
         }

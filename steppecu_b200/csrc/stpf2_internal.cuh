@@ -70,6 +70,7 @@ struct Ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     std::atomic<uint64_t> launches{0};
+    cudaStream_t h2d = nullptr, d2h = nullptr;  // copy streams of the pipelined host-buffer path
     // Grow-only scratch reused across calls of the host-buffer entry points, so repeated
     // extractions do not pay cudaMalloc each time.
     DevBuf ws_records, ws_f2, ws_vpair, ws_misc;
@@ -195,6 +196,7 @@ struct CanonDecodeArgs {
     const double* rec_n = nullptr;     // [n_max+1] 1/n (0 at n = 0)
     const double* rec_nm1 = nullptr;   // [n_max+1] 1/max(n-1, 1)
     const int32_t* col_snp = nullptr;  // [ld] SNP of each column, -1 for padding
+    int64_t col_base = 0;              // padded column of tile 0 (a range of the column space)
     OperandPlanes op;                  // planes == nullptr: counts only
     int32_t* cnt_ac2 = nullptr;        // optional [P x n_snp] column-major counts
     int32_t* cnt_n = nullptr;
@@ -224,6 +226,8 @@ void umma_plan_destroy(UmmaPlan* p);
 // per_block: one launch per jackknife block instead of one persistent launch over all
 // blocks (the comparison form of the grouped schedule).
 void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s, bool per_block = false);
+// The tile pairs of blocks [b0, b1) only, in one launch.
+void launch_f2_umma_blocks(Ctx& c, UmmaPlan* p, int b0, int b1, double* f2, double* vpair, cudaStream_t s);
 // After a stream sync: raises STP_DEVICE_TIMEOUT if the kernel's bounded waits expired.
 void umma_check(UmmaPlan* p);
 int umma_tile();
