@@ -132,7 +132,8 @@ stp_status stp_decode_counts(stp_ctx* ctx, const stp_geno_view* geno, const int6
  * Records must be on the device (geno->on_device = 1) with a 16-byte aligned base and
  * pitch; d_ac2 / d_n are caller-owned device buffers of n_pop * n_snp int32, written in
  * the column-major layout of stp_decode_counts. Every intermediate lives in one static
- * device array of 32 MiB, whose address the library takes once per device
+ * device array of 32 MiB (every GPU that loads the library holds it until the process
+ * exits), whose address the library takes once per device
  * (cudaGetSymbolAddress) on the first call; make that first call before any stream
  * capture. A request needing more scratch than that (about n_sel * n_snp / 4 bytes of
  * canonical genotypes plus 12 bytes per SNP) fails with STP_INVALID_ARGUMENT. The call
