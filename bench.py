@@ -223,7 +223,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--precision", default="split_f16")
-    ap.add_argument("--also", default="split_bf16", help="another tensor-core arithmetic timed beside the headline")
+    ap.add_argument("--also", default="split_bf16,split_f16_fine",
+                    help="other tensor-core arithmetics timed beside the headline (comma-separated, or none)")
     ap.add_argument("--compare-simt", action="store_true", default=True)
     ap.add_argument("--no-compare-simt", dest="compare_simt", action="store_false")
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -335,8 +336,8 @@ def main():
     extra = []
     if args.compare_simt and args.precision != "fp32" and not args.quick:
         extra.append("fp32")
-    if args.also and args.also not in (args.precision, "none") and not args.quick:
-        extra.append(args.also)
+    if args.also and not args.quick:
+        extra += [m for m in args.also.split(",") if m and m not in (args.precision, "none")]
     for prec in extra:
         plan_s = ctx.plan(rec, panel.n_ind, sel, po, panel.block_id, B, precision=prec)
         s_steps = max(1, min(args.steps, 3))
@@ -378,14 +379,14 @@ def main():
         threads = args.cpu_threads or (os.cpu_count() or 1)
         u, t, kind, desc, sample = cpu_sample(args.workload, threads, gen_device=dev, keep=True)
         cpu = {"value": u / t, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc}
-        modes = [args.precision] + [m for m in ("split_bf16", "fp32") if m != args.precision]
+        modes = [args.precision] + [m for m in ("split_f16_fine", "split_bf16", "fp32") if m != args.precision]
         precision = {"against": f"{kind} CPU f2 on the cpu_baseline sample", **precision_report(ctx, sample, modes)}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": {"split_bf16": "bf16x3", "split_f16": "f16x3"}.get(args.precision, "f32"),
+            "vs_baseline": None, "dtype": {"split_bf16": "bf16x3", "split_f16": "f16x3", "split_f16_fine": "f16x3"}.get(args.precision, "f32"),
             "data": "synthetic",
             "config": {"workload": args.workload, "populations": P, "samples": panel.n_ind, "snps": M,
                        "blocks": B, "precision": args.precision, "l2": "inputs larger than L2 (no flush)",

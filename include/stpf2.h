@@ -41,7 +41,10 @@ typedef enum stp_status {
 typedef enum stp_precision {
     STP_PREC_FP32_SIMT = 0,  /* plain FP32 CUDA-core contraction, FP64 combine */
     STP_PREC_SPLIT_BF16 = 1, /* tcgen05 split-BF16 (hi+lo, 3 products), FP32 TMEM, FP64 drain */
-    STP_PREC_SPLIT_F16 = 2   /* tcgen05 split-FP16 (scaled hi+lo, 3 products), same pipeline */
+    STP_PREC_SPLIT_F16 = 2,  /* tcgen05 split-FP16 (scaled hi+lo, 3 products), same pipeline;
+                                FP32 sums over 64-SNP chunks (max rel f2 error ~8e-7) */
+    STP_PREC_SPLIT_F16_FINE = 3 /* split-FP16 with FP32 sums over 32-SNP chunks (~4.5e-7,
+                                   ~15% slower contraction) */
 } stp_precision;
 
 /* steppe::ExtractPloidy (include/steppe/extract.hpp) */

@@ -35,6 +35,7 @@ STATUS_NAMES = {
 PREC_FP32_SIMT = 0
 PREC_SPLIT_BF16 = 1
 PREC_SPLIT_F16 = 2
+PREC_SPLIT_F16_FINE = 3
 
 PLOIDY_AUTO = 0
 PLOIDY_PSEUDO = 1

@@ -23,8 +23,10 @@ PRECISIONS = {
     "fp32": L.PREC_FP32_SIMT, "fp32_simt": L.PREC_FP32_SIMT, "simt": L.PREC_FP32_SIMT,
     "bf16x3": L.PREC_SPLIT_BF16, "split_bf16": L.PREC_SPLIT_BF16, "bf16": L.PREC_SPLIT_BF16,
     "f16x3": L.PREC_SPLIT_F16, "split_f16": L.PREC_SPLIT_F16, "fp16": L.PREC_SPLIT_F16,
+    "split_f16_fine": L.PREC_SPLIT_F16_FINE, "f16x3_fine": L.PREC_SPLIT_F16_FINE,
 }
-PRECISION_TAGS = {L.PREC_FP32_SIMT: "fp32_simt", L.PREC_SPLIT_BF16: "split_bf16", L.PREC_SPLIT_F16: "split_f16"}
+PRECISION_TAGS = {L.PREC_FP32_SIMT: "fp32_simt", L.PREC_SPLIT_BF16: "split_bf16", L.PREC_SPLIT_F16: "split_f16",
+                  L.PREC_SPLIT_F16_FINE: "split_f16_fine"}
 DEFAULT_PRECISION = "split_f16"
 
 PLOIDY = {"auto": L.PLOIDY_AUTO, "1": L.PLOIDY_PSEUDO, "pseudo": L.PLOIDY_PSEUDO,

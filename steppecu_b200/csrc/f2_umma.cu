@@ -37,7 +37,7 @@ namespace {
 constexpr int kTile = 128;
 constexpr int kStageK = 32;        // SNP columns per pipeline stage
 constexpr int kStages = 2;
-constexpr int kNumBufs = 3;        // FP32 chunk buffers in TMEM (one 32-SNP stage each)
+constexpr int kNumBufs = 3;        // FP32 chunk buffers in TMEM
 constexpr uint32_t kVpCol = kNumBufs * 128u;
 constexpr int kPlanes = 5;
 constexpr uint32_t kTile16 = kTile * kStageK * 2;                 // 8 KiB
@@ -279,6 +279,7 @@ abort:
         wait_bounded(&ctl->full[k % kStages], (k / kStages) & 1u, ctl, a.err, false);
 }
 
+template <int kChunkStages>
 __device__ void mma_issuer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl, uint32_t tmem) {
     uint32_t g = 0, cs = 0, is = 0;
     for (uint32_t gi = 0;; ++gi) {
@@ -291,10 +292,13 @@ __device__ void mma_issuer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl, uint3
         const bool diag = w.ti == w.tj;
         {
             const uint32_t d_vp = tmem + kVpCol;
-            for (int st = 0; st < nst; ++st, ++g, ++cs) {
+            for (int st = 0; st < nst; ++st, ++g) {
+                const int sc = st % kChunkStages;  // stage within the chunk
                 const int nb = static_cast<int>(cs % kNumBufs);
-                if (!wait_bounded(&ctl->acc_empty[nb], ((cs / kNumBufs) & 1u) ^ 1u, ctl, a.err)) goto done;
-                tc_fence_after();
+                if (sc == 0) {
+                    if (!wait_bounded(&ctl->acc_empty[nb], ((cs / kNumBufs) & 1u) ^ 1u, ctl, a.err)) goto done;
+                    tc_fence_after();
+                }
                 const uint32_t d_num = tmem + static_cast<uint32_t>(nb) * 128u;
                 const int slot = static_cast<int>(g % kStages);
                 if (!wait_bounded(&ctl->full[slot], (g / kStages) & 1u, ctl, a.err)) goto done;
@@ -314,7 +318,7 @@ __device__ void mma_issuer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl, uint3
                     const uint64_t bAh = smem_desc(sb + 2 * kTile16 + ko, 512, 4);
                     const uint64_t bAl = smem_desc(sb + 3 * kTile16 + ko, 512, 4);
                     const uint64_t bM = smem_desc(sb + 4 * kTile16 + ko, 512, 4);
-                    const uint32_t first = k == 0 ? 0u : 1u;
+                    const uint32_t first = (sc == 0 && k == 0) ? 0u : 1u;
                     // Large terms first and interleaved in sign, the lo corrections last.
                     mma_f16(d_num, aAh, bM, a.idesc_am, first);
                     mma_f16(d_num, aPh, bPh, a.idesc_pp, 1u);
@@ -331,7 +335,10 @@ __device__ void mma_issuer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl, uint3
                 mma_i8(d_vp, smem_desc(sa + kPlanes * kTile16, 256, 6), smem_desc(sb + kPlanes * kTile16, 256, 6),
                        a.idesc_i8, st > 0 ? 1u : 0u);
                 mma_commit(&ctl->empty[slot]);
-                mma_commit(&ctl->acc_full[nb]);
+                if (sc == kChunkStages - 1 || st == nst - 1) {
+                    mma_commit(&ctl->acc_full[nb]);
+                    ++cs;
+                }
             }
             mma_commit(&ctl->vp_full);
             ++is;
@@ -343,6 +350,7 @@ done:
     wait_bounded(&ctl->drain, 0u, ctl, a.err, false);
 }
 
+template <int kChunkStages>
 __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int warp, int lane, double* stage) {
     const int e = warp - kEpiWarp0;
     const int q = warp & 3;                 // TMEM lane quarter this warp may access
@@ -379,8 +387,9 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
         }
 #pragma unroll
         for (int c = 0; c < kCols; ++c) acc[c] = 0.0;
-        for (int ch = 0; ch < nst; ch += 2) {
-            const bool pair = ch + 1 < nst;
+        const int nch = (nst + kChunkStages - 1) / kChunkStages;
+        for (int ch = 0; ch < nch; ch += 2) {
+            const bool pair = ch + 1 < nch;
             const int nb0 = static_cast<int>(cs % kNumBufs), nb1 = static_cast<int>((cs + 1) % kNumBufs);
             bool ok = true;
             if (lane == 0) {
@@ -473,6 +482,10 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
     }
 }
 
+// kChunkStages: pipeline stages of 32 SNPs accumulated into one FP32 TMEM chunk before the
+// epilogue moves it to FP64 (1: 32-SNP chunks, 2: 64-SNP chunks; longer chunks halve the
+// epilogue's conversions and lengthen the FP32 sums).
+template <int kChunkStages>
 __global__ void __maxnreg__(96)
 f2_umma_kernel(const __grid_constant__ UmmaArgs a) {
     extern __shared__ uint8_t smem_raw[];
@@ -513,9 +526,9 @@ f2_umma_kernel(const __grid_constant__ UmmaArgs a) {
 
     if (warp < kEpiWarp0) {
         if (warp == 0 && lane == 0) producer(a, smem, ctl);
-        if (warp == 1 && lane == 0) mma_issuer(a, smem, ctl, tmem);
+        if (warp == 1 && lane == 0) mma_issuer<kChunkStages>(a, smem, ctl, tmem);
     } else {
-        epilogue(a, ctl, tmem, warp, lane,
+        epilogue<kChunkStages>(a, ctl, tmem, warp, lane,
                  reinterpret_cast<double*>(smem + kStages * kStageBytes + kCtlBytes) + (warp - kEpiWarp0) * kStageDoubles);
     }
 
@@ -550,15 +563,18 @@ struct UmmaPlan {
     int P = 0;
     OpFmt fmt = OpFmt::BF16;
     double num_scale = 2.0;
+    int chunk_stages = 2;
 };
 
 int umma_tile() { return kTile; }
 
-UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L) {
+UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L, int chunk_stages) {
     if (op.fmt == OpFmt::F32) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs split 16-bit planes");
     auto p = std::make_unique<UmmaPlan>();
+    if (chunk_stages != 1 && chunk_stages != 2) fail(STP_INVALID_ARGUMENT, "chunk stages must be 1 or 2");
     p->P = op.P;
     p->fmt = op.fmt;
+    p->chunk_stages = chunk_stages;
     p->num_scale = 2.0 * op.scale_inv;
     const std::vector<WorkItem> items = make_work_items(L, op.P, kTile);
     p->n_items = static_cast<int>(items.size());
@@ -592,7 +608,9 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
     if (op.n_rt <= 0 || op.n_ck <= 0) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs tiled planes");
     p->images = static_cast<const uint8_t*>(op.planes);
     p->n_ck = op.n_ck;
-    STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(kSmemBytes)));
+    STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kSmemBytes)));
     return p.release();
 }
@@ -643,11 +661,12 @@ void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, 
     a.idesc_am = idesc_f16(bf16, false);
     a.idesc_i8 = idesc_u8_s32();
     const int grid = std::min(c.sm_count, n_items);
-    f2_umma_kernel<<<grid, kThreads, kSmemBytes, s>>>(a);
+    if (p->chunk_stages == 1) f2_umma_kernel<1><<<grid, kThreads, kSmemBytes, s>>>(a);
+    else f2_umma_kernel<2><<<grid, kThreads, kSmemBytes, s>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         cudaFuncAttributes fa{};
-        cudaFuncGetAttributes(&fa, f2_umma_kernel);
+        cudaFuncGetAttributes(&fa, f2_umma_kernel<2>);
         fail(STP_CUDA_ERROR, std::string("f2_umma_kernel launch: ") + cudaGetErrorString(e) + " (regs " +
                                  std::to_string(fa.numRegs) + ", max threads " + std::to_string(fa.maxThreadsPerBlock) +
                                  ", dyn smem " + std::to_string(kSmemBytes) + ", max dyn smem " +

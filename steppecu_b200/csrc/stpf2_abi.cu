@@ -302,7 +302,7 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
         p->n_items = static_cast<int>(items.size());
         upload(p->items, items, s);
     } else if (r.n_pop > 0 && r.n_block > 0) {
-        p->umma = umma_plan_create(c, p->op, p->L);
+        p->umma = umma_plan_create(c, p->op, p->L, chunk_stages_of(r.precision));
     }
     return p;
 }
@@ -791,7 +791,7 @@ stp_status stp_f2_from_qvn(stp_ctx* ctx, const double* Q, const double* V, const
             launch_f2_simt(*ctx, d_items.as<WorkItem>(), static_cast<int>(items.size()), d_blocks.as<BlockInfo>(), op,
                            d_f2.as<double>(), d_vp.as<double>(), s);
         } else {
-            UmmaPlan* up = umma_plan_create(*ctx, op, L);
+            UmmaPlan* up = umma_plan_create(*ctx, op, L, chunk_stages_of(precision));
             try {
                 launch_f2_umma(*ctx, up, d_f2.as<double>(), d_vp.as<double>(), s);
             } catch (...) {

@@ -121,6 +121,7 @@ inline OpFmt fmt_of(int precision) {
         case STP_PREC_FP32_SIMT: return OpFmt::F32;
         case STP_PREC_SPLIT_BF16: return OpFmt::BF16;
         case STP_PREC_SPLIT_F16: return OpFmt::F16;
+        case STP_PREC_SPLIT_F16_FINE: return OpFmt::F16;
     }
     fail(STP_INVALID_ARGUMENT, "unknown precision mode " + std::to_string(precision));
 }
@@ -221,7 +222,10 @@ void launch_f2_simt(Ctx& c, const WorkItem* items, int n_items, const BlockInfo*
 
 // tcgen05 contraction; returns false if the device cannot run it.
 struct UmmaPlan;
-UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L);
+// chunk_stages: 32-SNP stages per FP32 TMEM chunk (1 or 2).
+UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L, int chunk_stages);
+// 32-SNP stages per FP32 chunk for a tensor-core precision mode.
+inline int chunk_stages_of(int precision) { return precision == STP_PREC_SPLIT_F16_FINE ? 1 : 2; }
 void umma_plan_destroy(UmmaPlan* p);
 // per_block: one launch per jackknife block instead of one persistent launch over all
 // blocks (the comparison form of the grouped schedule).

@@ -22,9 +22,10 @@ pytestmark = pytest.mark.gpu
 TOL = {
     "fp32": (5e-6, 5e-8),
     "split_f16": (5e-6, 2e-7),
+    "split_f16_fine": (5e-6, 2e-7),
     "split_bf16": (3e-4, 3e-6),
 }
-MODES = ["fp32", "split_bf16", "split_f16"]
+MODES = ["fp32", "split_bf16", "split_f16", "split_f16_fine"]
 TC_DEFAULT = "split_f16"
 
 
