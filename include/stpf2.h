@@ -171,10 +171,22 @@ stp_status stp_f2_from_qvn(stp_ctx* ctx, const double* Q, const double* V, const
  * -> FP64 F2BlockTensor (src/app/extract_f2_core.cpp:93-407, Resident tier). */
 stp_status stp_f2_extract_blocks(stp_ctx* ctx, const stp_f2_request* req, stp_f2_output* out);
 
-/* Many independent requests (each its own populations and block map) over shared or
- * separate genotype matrices, batched into one grouped decode and one grouped contraction. */
+/* Many independent requests (each its own populations and block map). The reference runs
+ * requests one at a time (run_extract_f2 per request, src/app/extract_f2_core.cpp:93-407);
+ * it has no batch entry. Tensor-core requests that read the same panel (same geno view)
+ * with the same arithmetic run as one group: one ploidy pass and one canonical transpose
+ * over the union of their samples, a decode per request into its own operand images, and
+ * one persistent contraction launch over every request's (block, tile pair) items. FP32
+ * SIMT and empty requests run one by one. Outputs and errors are per request as in
+ * stp_f2_extract_blocks. */
 stp_status stp_f2_extract_batch(stp_ctx* ctx, const stp_f2_request* reqs, int32_t n_req,
                                 stp_f2_output* outs);
+
+/* Completion time of each request of this context's last stp_f2_extract_batch call, in ms
+ * from the start of its group's device work (%globaltimer stamps written by the last work
+ * item of each request); NaN for requests that ran on their own. No counterpart in the
+ * reference. */
+stp_status stp_last_batch_times(stp_ctx* ctx, double* ms, int32_t n);
 
 /* Block jackknife over per-block values (cpu_backend.cpp:2674-2720, :2273-2306), FP64 on
  * the device: x[k + m*b] with m = P*P -> est[m], var[m]. Host pointers. */

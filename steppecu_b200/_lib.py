@@ -102,6 +102,7 @@ SIGNATURES = {
     "stp_f2_from_qvn": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int64, _P, C.c_int32, C.c_int32, _P, _P, _P]),
     "stp_f2_extract_blocks": (C.c_int, [_P, C.POINTER(F2Request), C.POINTER(F2Output)]),
     "stp_f2_extract_batch": (C.c_int, [_P, C.POINTER(F2Request), C.c_int32, C.POINTER(F2Output)]),
+    "stp_last_batch_times": (C.c_int, [_P, _P, C.c_int32]),
     "stp_f2_jackknife": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, _P, _P]),
     "stp_plan_create": (_P, [_P, C.POINTER(F2Request), C.POINTER(C.c_int)]),
     "stp_plan_run": (C.c_int, [_P, _P, _P, _P, _P]),

@@ -214,6 +214,36 @@ class Context:
         t = F2Tensor(f2, vp, bs, P, n_block) if not on_dev else (f2, vp, bs)
         return (t, ploidy_out) if return_ploidy else t
 
+    def extract_batch(self, records, n_ind: int, requests, precision=None, out=None) -> list:
+        """Many requests over one panel in one call (stp_f2_extract_batch). requests: a sequence
+        of dicts with sel_rows, pop_offsets, block_id, n_block and optionally sample_ploidy /
+        ploidy. out: optional list of (f2, vpair) buffers per request (numpy host or torch
+        CUDA). Returns one F2Tensor (host outputs) or (f2, vpair, block_sizes) per request."""
+        reqs = (L.F2Request * max(len(requests), 1))()
+        outs = (L.F2Output * max(len(requests), 1))()
+        keep, results = [], []
+        for k, q in enumerate(requests):
+            r = self._request(records, n_ind, q["sel_rows"], q["pop_offsets"], q["block_id"], int(q["n_block"]),
+                              precision, q.get("sample_ploidy"), q.get("ploidy", "auto"))
+            reqs[k] = r
+            P = r.n_pop
+            n = P * P * int(q["n_block"])
+            f2, vp = (np.zeros(n), np.zeros(n)) if out is None else out[k]
+            bs = np.zeros(max(int(q["n_block"]), 0), np.int32)
+            on_dev = _is_torch_cuda(f2)
+            outs[k] = L.F2Output(_data_ptr(f2), _data_ptr(vp), L.ptr(bs), 1 if on_dev else 0, None)
+            keep.append((r, f2, vp, bs))
+            results.append(F2Tensor(f2, vp, bs, P, int(q["n_block"])) if not on_dev else (f2, vp, bs))
+        L.check(L.lib().stp_f2_extract_batch(self._h, reqs, len(requests), outs))
+        return results
+
+    def last_batch_times(self, n: int) -> np.ndarray:
+        """Per-request completion times (ms from the start of the group's device work) of the
+        last extract_batch call; NaN for requests that ran on their own."""
+        ms = np.zeros(max(n, 0))
+        L.check(L.lib().stp_last_batch_times(self._h, L.ptr(ms), n))
+        return ms
+
     def jackknife(self, x, block_sizes, m: int, n_block: int) -> tuple[np.ndarray, np.ndarray]:
         x = np.ascontiguousarray(x, dtype=np.float64)
         bs = _i32(block_sizes)

@@ -407,19 +407,52 @@ __device__ __forceinline__ void spill_counts(uint32_t* cnt, bool add, uint32_t (
     }
 }
 
-template <OpFmt F>
+// Columns r .. r+31 of the 64-column stream w0 | w1 (canonical words: column c of a word at
+// byte c/4, bits 7-2(c%4)), 0 <= r < 32: a byte shift, then a 2-bit shift inside each byte
+// taking the top columns from the next byte.
+__device__ __forceinline__ uint64_t window_cols(uint64_t w0, uint64_t w1, int r) {
+    if (r == 0) return w0;
+    const int rb = r >> 2, rs = r & 3;
+    const uint64_t A = rb == 0 ? w0 : (w0 >> (8 * rb)) | (w1 << (64 - 8 * rb));
+    if (rs == 0) return A;
+    const uint64_t B = rb == 7 ? w1 : (w0 >> (8 * rb + 8)) | (w1 << (56 - 8 * rb));
+    const uint64_t mhi = 0x0101010101010101ull * ((0xFFu << (2 * rs)) & 0xFFu);
+    const uint64_t mlo = 0x0101010101010101ull * (0xFFu >> (8 - 2 * rs));
+    return ((A << (2 * rs)) & mhi) | ((B >> (8 - 2 * rs)) & mlo);
+}
+
+// Bits of columns nv .. 31 of a canonical word set (code 3, missing).
+__device__ __forceinline__ uint64_t missing_from(int nv) {
+    if (nv >= 32) return 0;
+    const int kb = nv >> 2, js = nv & 3;
+    uint64_t m = kb + 1 < 8 ? (~0ull << (8 * (kb + 1))) : 0ull;
+    return m | (static_cast<uint64_t>(0xFFu >> (2 * js)) << (8 * kb));
+}
+
+template <OpFmt F, bool kUnion>
 __global__ void __launch_bounds__(kDecThreads2, 4)
 decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t n_sel,
                     const uint32_t* __restrict__ sel, const int32_t* __restrict__ pop_off, int P,
                     const double* __restrict__ center, const double* __restrict__ rec_n,
                     const double* __restrict__ rec_nm1, const int32_t* __restrict__ col_snp, int64_t col_base,
-                    OperandPlanes op, int32_t* __restrict__ cnt_ac2, int32_t* __restrict__ cnt_n) {
+                    OperandPlanes op, int32_t* __restrict__ cnt_ac2, int32_t* __restrict__ cnt_n,
+                    const int32_t* __restrict__ umap, const TileInfo* __restrict__ tiles, int64_t n_utiles,
+                    const double* __restrict__ center_snp) {
     extern __shared__ uint32_t s_cnt[];
     __shared__ double s_center[4 * kCenterPitch];
     const int64_t q = blockIdx.x;
     for (int c = threadIdx.x; c < 4 * kTileCols; c += blockDim.x) {
         const int64_t col = q * 4 * kTileCols + c;
-        s_center[(c / kTileCols) * kCenterPitch + c % kTileCols] = col < n_tiles * kTileCols ? __ldg(center + col) : 0.5;
+        double cv = 0.5;
+        if (col < n_tiles * kTileCols) {
+            if constexpr (kUnion) {
+                const int32_t s = __ldg(col_snp + col);
+                if (s >= 0) cv = __ldg(center_snp + s);
+            } else {
+                cv = __ldg(center + col);
+            }
+        }
+        s_center[(c / kTileCols) * kCenterPitch + c % kTileCols] = cv;
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     {
@@ -434,13 +467,39 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
             bool spilled = false;
             int it = 0;
             const uint64_t* col = canon + q * n_sel * 4 + sub;
+            // Shared-canonical mode: the union words holding this tile's 32-SNP window.
+            const uint64_t* col0 = nullptr;
+            const uint64_t* col1 = nullptr;
+            int shift = 0;
+            uint64_t miss = ~0ull;
+            if constexpr (kUnion) {
+                const TileInfo ti = tiles[4 * q + sub];
+                if (ti.nvalid > 0) {
+                    const int64_t ut = ti.snp0 >> 5;
+                    shift = ti.snp0 & 31;
+                    miss = missing_from(ti.nvalid);
+                    col0 = canon + (ut >> 2) * n_sel * 4 + (ut & 3);
+                    if (shift != 0 && ut + 1 < n_utiles) col1 = canon + ((ut + 1) >> 2) * n_sel * 4 + ((ut + 1) & 3);
+                }
+            }
+            auto load = [&](int gg) -> uint64_t {
+                if constexpr (kUnion) {
+                    if (!col0) return ~0ull;  // a padding tile: every column missing
+                    const int64_t uidx = static_cast<int64_t>(__ldg(umap + gg)) * 4;
+                    const uint64_t w0 = __ldg(col0 + uidx);
+                    const uint64_t w1 = shift == 0 ? 0ull : (col1 ? __ldg(col1 + uidx) : ~0ull);
+                    return window_cols(w0, w1, shift) | miss;
+                } else {
+                    return __ldg(col + static_cast<int64_t>(gg) * 4);
+                }
+            };
             int g = g0;
             for (; g + kDecUnroll <= g1; g += kDecUnroll) {
                 uint64_t x[kDecUnroll];
                 uint32_t pl[kDecUnroll];
 #pragma unroll
                 for (int u = 0; u < kDecUnroll; ++u) {
-                    x[u] = __ldg(col + static_cast<int64_t>(g + u) * 4);
+                    x[u] = load(g + u);
                     pl[u] = __ldg(sel + g + u) & 3u;
                 }
 #pragma unroll
@@ -457,7 +516,7 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
 #pragma unroll
                 for (int u = 0; u < kDecUnroll - 1; ++u) {
                     const bool ok = g + u < g1;
-                    x[u] = ok ? __ldg(col + static_cast<int64_t>(g + u) * 4) : ~0ull;
+                    x[u] = ok ? load(g + u) : ~0ull;
                     pl[u] = ok ? (__ldg(sel + g + u) & 3u) : 0u;
                 }
 #pragma unroll
@@ -653,15 +712,37 @@ void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t
     c.launches++;
 }
 
+namespace {
+__global__ void copy_union_ploidy_kernel(uint32_t* __restrict__ desc, const int32_t* __restrict__ umap, int64_t n_sel,
+                                         const uint32_t* __restrict__ desc_u) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g < n_sel) desc[g] = (desc[g] & ~3u) | (desc_u[umap[g]] & 3u);
+}
+}  // namespace
+
+void launch_copy_union_ploidy(Ctx& c, uint32_t* desc, const int32_t* umap, int64_t n_sel, const uint32_t* desc_u,
+                              cudaStream_t s) {
+    if (n_sel <= 0) return;
+    copy_union_ploidy_kernel<<<static_cast<unsigned>((n_sel + 255) / 256), 256, 0, s>>>(desc, umap, n_sel, desc_u);
+    STPF2_CUDA(cudaGetLastError());
+    c.launches++;
+}
+
 void launch_decode_canon(Ctx& c, const CanonDecodeArgs& a, cudaStream_t s) {
     if (a.P <= 0 || a.n_tiles <= 0) return;
     const dim3 grid(static_cast<unsigned>((a.n_tiles + 3) / 4), static_cast<unsigned>((a.P + kDecPops - 1) / kDecPops));
-#define STPF2_DECODE_ARGS a.canon, a.n_tiles, a.n_sel, a.sel, a.pop_off, a.P, a.center, a.rec_n, a.rec_nm1, a.col_snp, a.col_base, a.op, a.cnt_ac2, a.cnt_n
+#define STPF2_DECODE_ARGS a.canon, a.n_tiles, a.n_sel, a.sel, a.pop_off, a.P, a.center, a.rec_n, a.rec_nm1, a.col_snp, \
+                          a.col_base, a.op, a.cnt_ac2, a.cnt_n, a.umap, a.tiles, a.n_utiles, a.center_snp
+#define STPF2_DECODE_LAUNCH(F)                                                                      \
+    (a.umap ? decode_canon_kernel<F, true><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS) \
+            : decode_canon_kernel<F, false><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS))
+    if (a.umap && (!a.tiles || !a.center_snp)) fail(STP_INVALID_ARGUMENT, "shared-canonical decode needs tiles and centres");
     switch (a.op.fmt) {
-        case OpFmt::F32: decode_canon_kernel<OpFmt::F32><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS); break;
-        case OpFmt::BF16: decode_canon_kernel<OpFmt::BF16><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS); break;
-        case OpFmt::F16: decode_canon_kernel<OpFmt::F16><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS); break;
+        case OpFmt::F32: STPF2_DECODE_LAUNCH(OpFmt::F32); break;
+        case OpFmt::BF16: STPF2_DECODE_LAUNCH(OpFmt::BF16); break;
+        case OpFmt::F16: STPF2_DECODE_LAUNCH(OpFmt::F16); break;
     }
+#undef STPF2_DECODE_LAUNCH
 #undef STPF2_DECODE_ARGS
     STPF2_CUDA(cudaGetLastError());
     c.launches++;

@@ -26,7 +26,9 @@
 // kernel raises an error flag the host turns into STP_DEVICE_TIMEOUT, lets its copies and
 // MMAs finish, frees TMEM and returns.
 #include <algorithm>
+#include <climits>
 #include <memory>
+#include <vector>
 
 #include "stpf2_internal.cuh"
 
@@ -75,6 +77,14 @@ struct UmmaArgs {
     int* err;
     int* next_item;    // work-item counter, zero at launch
     uint32_t idesc_pp, idesc_am, idesc_i8;
+    // Grouped launch (a batch of requests): per-request images and outputs, indexed by
+    // BlockInfo::grp; null for one request (images, n_ck, P, f2, vpair above). Optional
+    // completion stamps: grp_done counts finished (item, epilogue warp) pairs per request,
+    // and the last one writes %globaltimer to grp_ns.
+    const GroupInfo* groups;
+    int* grp_done;
+    unsigned long long* grp_ns;
+    const int* grp_items;
 };
 
 constexpr int kItemRing = 4;  // work items handed from the producer to the other roles
@@ -218,6 +228,7 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo_bytes,
 // ---- roles -------------------------------------------------------------------------------
 
 __device__ __forceinline__ int stages_of(int k) { return (k + kStageK - 1) / kStageK; }
+inline int stages_of_host(int k) { return (k + kStageK - 1) / kStageK; }
 
 // Work items are handed out dynamically, in list order (costliest block first, a block's
 // tile pairs together): the producer takes the next item from a global counter and
@@ -244,6 +255,7 @@ __device__ __forceinline__ int read_item(const UmmaArgs& a, SmemCtl* ctl, uint32
     return it;
 }
 
+template <bool kGrouped>
 __device__ void producer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl) {
     uint32_t g = 0;
     for (uint32_t gi = 0;; ++gi) {
@@ -255,6 +267,12 @@ __device__ void producer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl) {
         const BlockInfo bi = a.blocks[w.blk];
         const int nst = stages_of(bi.k);
         const bool diag = w.ti == w.tj;
+        const uint8_t* images = a.images;
+        int64_t n_ck = a.n_ck;
+        if constexpr (kGrouped) {
+            images = a.groups[bi.grp].images;
+            n_ck = a.groups[bi.grp].n_ck;
+        }
         for (int st = 0; st < nst; ++st, ++g) {
             const int slot = static_cast<int>(g % kStages);
             const uint32_t ph = (g / kStages) & 1u;
@@ -263,11 +281,11 @@ __device__ void producer(const UmmaArgs& a, uint8_t* smem, SmemCtl* ctl) {
                 uint8_t* sb = smem + slot * kStageBytes;
                 mbar_expect_tx(&ctl->full[slot], diag ? kSideBytes : kStageBytes);
                 const int64_t chunk = bi.col / kStageK + st;
-                const int64_t ta = static_cast<int64_t>(w.ti) * a.n_ck + chunk;
-                bulk_load(sb, a.images + ta * kSideBytes, kSideBytes, &ctl->full[slot]);
+                const int64_t ta = static_cast<int64_t>(w.ti) * n_ck + chunk;
+                bulk_load(sb, images + ta * kSideBytes, kSideBytes, &ctl->full[slot]);
                 if (!diag) {
-                    const int64_t tb = static_cast<int64_t>(w.tj) * a.n_ck + chunk;
-                    bulk_load(sb + kSideBytes, a.images + tb * kSideBytes, kSideBytes, &ctl->full[slot]);
+                    const int64_t tb = static_cast<int64_t>(w.tj) * n_ck + chunk;
+                    bulk_load(sb + kSideBytes, images + tb * kSideBytes, kSideBytes, &ctl->full[slot]);
                 }
             }
         }
@@ -350,7 +368,54 @@ done:
     wait_bounded(&ctl->drain, 0u, ctl, a.err, false);
 }
 
-template <int kChunkStages>
+// The output side of a work item for this epilogue thread (row r of the tile, column
+// part h): its request's P and slabs, the slab offset, the thread's row i and first column
+// j0, and the first row i0 of its warp.
+struct ItemOut {
+    double* f2;
+    double* vp;
+    int64_t slab;
+    int P, i, j0, i0, grp;
+    bool diag;
+};
+
+template <bool kGrouped>
+__device__ __forceinline__ ItemOut item_out(const UmmaArgs& a, int it, int r, int h) {
+    const WorkItem w = a.items[it];
+    const BlockInfo bi = a.blocks[w.blk];
+    ItemOut o;
+    o.grp = bi.grp;
+    o.P = a.P;
+    o.f2 = a.f2;
+    o.vp = a.vpair;
+    if constexpr (kGrouped) {
+        const GroupInfo& gr = a.groups[bi.grp];
+        o.P = gr.P;
+        o.f2 = gr.f2;
+        o.vp = gr.vpair;
+    }
+    o.diag = w.ti == w.tj;
+    o.i = w.ti * kTile + r;
+    o.i0 = w.ti * kTile + (r & ~31);
+    o.j0 = w.tj * kTile + h * kCols;
+    o.slab = static_cast<int64_t>(o.P) * o.P * bi.b;
+    return o;
+}
+
+// Completion stamp of a grouped launch: the last (item, epilogue warp) of a request records
+// the time.
+template <bool kGrouped>
+__device__ __forceinline__ void stamp(const UmmaArgs& a, int grp, int lane) {
+    if (!kGrouped || !a.grp_done) return;
+    __syncwarp();
+    if (lane == 0) {
+        __threadfence();
+        const int d = atomicAdd(a.grp_done + grp, 1);
+        if (d == a.grp_items[grp] * kEpiWarps - 1) a.grp_ns[grp] = globaltimer();
+    }
+}
+
+template <int kChunkStages, bool kGrouped>
 __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int warp, int lane, double* stage) {
     const int e = warp - kEpiWarp0;
     const int q = warp & 3;                 // TMEM lane quarter this warp may access
@@ -358,7 +423,6 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
     const int r = q * 32 + lane;            // tile row (TMEM lane)
     const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
     const uint32_t col_addr = static_cast<uint32_t>(h * kCols);
-    const int P = a.P;
     uint32_t cs = 0, is = 0;
     double acc[kCols];  // FP64 running numerator per column
     for (uint32_t gi = 0;; ++gi) {
@@ -366,23 +430,21 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
         if (lane == 0) it = read_item(a, ctl, gi);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it < 0) return;
-        const WorkItem w = a.items[it];
-        const BlockInfo bi = a.blocks[w.blk];
-        const int nst = stages_of(bi.k);
-        const bool diag = w.ti == w.tj;
-        const int i = w.ti * kTile + r;
-        const int j0 = w.tj * kTile + h * kCols;
-        const int64_t slab = static_cast<int64_t>(P) * P * bi.b;
+        // Only the stage count lives through the drain; the output side of the item is
+        // read again at its end (fewer registers held across the chunk loop).
+        const int nst = stages_of(a.blocks[a.items[it].blk].k);
         if (nst == 0) {  // an empty block id: zeros (cpu_backend.cpp:234)
-            if (i < P)
+            const ItemOut o = item_out<kGrouped>(a, it, r, h);
+            if (o.i < o.P)
                 for (int c = 0; c < kCols; ++c) {
-                    const int j = j0 + c;
-                    if (j >= P || (diag && j < i)) continue;
-                    a.f2[slab + i + static_cast<int64_t>(P) * j] = 0.0;
-                    a.vpair[slab + i + static_cast<int64_t>(P) * j] = 0.0;
-                    a.f2[slab + j + static_cast<int64_t>(P) * i] = 0.0;
-                    a.vpair[slab + j + static_cast<int64_t>(P) * i] = 0.0;
+                    const int j = o.j0 + c;
+                    if (j >= o.P || (o.diag && j < o.i)) continue;
+                    o.f2[o.slab + o.i + static_cast<int64_t>(o.P) * j] = 0.0;
+                    o.vp[o.slab + o.i + static_cast<int64_t>(o.P) * j] = 0.0;
+                    o.f2[o.slab + j + static_cast<int64_t>(o.P) * o.i] = 0.0;
+                    o.vp[o.slab + j + static_cast<int64_t>(o.P) * o.i] = 0.0;
                 }
+            stamp<kGrouped>(a, o.grp, lane);
             continue;
         }
 #pragma unroll
@@ -432,9 +494,11 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
         // Output: (i, j) straight from registers (32 consecutive i per store: full sectors);
         // (j, i) through this warp's staging tile, so each store covers 4 rows x 8
         // consecutive j (64-byte segments) instead of 32 scattered 8-byte pieces.
-        const int i0 = w.ti * kTile + q * 32;
-        const int64_t row_i = slab + i;                              // (i, j) at row_i + P*j
-        const int64_t row_j0 = slab + static_cast<int64_t>(P) * i0;  // (j, i0 + rr) at row_j0 + P*rr + j
+        const ItemOut o = item_out<kGrouped>(a, it, r, h);
+        const int P = o.P, i = o.i, i0 = o.i0, j0 = o.j0;
+        const bool diag = o.diag;
+        const int64_t row_i = o.slab + i;                              // (i, j) at row_i + P*j
+        const int64_t row_j0 = o.slab + static_cast<int64_t>(P) * i0;  // (j, i0 + rr) at row_j0 + P*rr + j
 #pragma unroll
         for (int q8 = 0; q8 < kCols / 8; ++q8) {
             uint32_t v[8];
@@ -458,14 +522,14 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
                 fv[c] = vk > 0 ? acc[col] * a.num_scale * __ldg(a.rcp + vk) : 0.0;
                 if (i < P && j < P && !(diag && j < i)) {
                     const int64_t ij = row_i + static_cast<int64_t>(P) * j;
-                    __stcs(a.f2 + ij, fv[c]);  // output is never re-read: evict-first
-                    __stcs(a.vpair + ij, vv[c]);
+                    __stcs(o.f2 + ij, fv[c]);  // output is never re-read: evict-first
+                    __stcs(o.vp + ij, vv[c]);
                 }
             }
             const int jj = j0 + q8 * 8 + (lane & 7);
 #pragma unroll
             for (int part = 0; part < 2; ++part) {
-                double* out = part == 0 ? a.f2 : a.vpair;
+                double* out = part == 0 ? o.f2 : o.vp;
 #pragma unroll
                 for (int c = 0; c < 8; ++c) stage[lane * kStagePitch + c] = part == 0 ? fv[c] : vv[c];
                 __syncwarp();
@@ -478,6 +542,7 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
                 __syncwarp();
             }
         }
+        stamp<kGrouped>(a, o.grp, lane);
         ++is;
     }
 }
@@ -485,7 +550,7 @@ __device__ void epilogue(const UmmaArgs& a, SmemCtl* ctl, uint32_t tmem, int war
 // kChunkStages: pipeline stages of 32 SNPs accumulated into one FP32 TMEM chunk before the
 // epilogue moves it to FP64 (1: 32-SNP chunks, 2: 64-SNP chunks; longer chunks halve the
 // epilogue's conversions and lengthen the FP32 sums).
-template <int kChunkStages>
+template <int kChunkStages, bool kGrouped>
 __global__ void __maxnreg__(96)
 f2_umma_kernel(const __grid_constant__ UmmaArgs a) {
     extern __shared__ uint8_t smem_raw[];
@@ -525,10 +590,10 @@ f2_umma_kernel(const __grid_constant__ UmmaArgs a) {
     const uint32_t tmem = ctl->tmem_base;
 
     if (warp < kEpiWarp0) {
-        if (warp == 0 && lane == 0) producer(a, smem, ctl);
+        if (warp == 0 && lane == 0) producer<kGrouped>(a, smem, ctl);
         if (warp == 1 && lane == 0) mma_issuer<kChunkStages>(a, smem, ctl, tmem);
     } else {
-        epilogue<kChunkStages>(a, ctl, tmem, warp, lane,
+        epilogue<kChunkStages, kGrouped>(a, ctl, tmem, warp, lane,
                  reinterpret_cast<double*>(smem + kStages * kStageBytes + kCtlBytes) + (warp - kEpiWarp0) * kStageDoubles);
     }
 
@@ -550,6 +615,24 @@ uint32_t idesc_u8_s32() { return (2u << 4) | (0u << 7) | (0u << 10) | ((kTile >>
 
 constexpr size_t kSmemBytes = kStages * kStageBytes + kCtlBytes + kEpiWarps * kStageDoubles * sizeof(double) + 1024;
 static_assert(sizeof(SmemCtl) <= kCtlBytes, "barrier block overflows its slot");
+
+void set_umma_smem() {
+    const int b = static_cast<int>(kSmemBytes);
+    STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+}
+
+void launch_kernel(int chunk_stages, bool grouped, int grid, const UmmaArgs& a, cudaStream_t s) {
+    if (chunk_stages == 1) {
+        if (grouped) f2_umma_kernel<1, true><<<grid, kThreads, kSmemBytes, s>>>(a);
+        else f2_umma_kernel<1, false><<<grid, kThreads, kSmemBytes, s>>>(a);
+    } else {
+        if (grouped) f2_umma_kernel<2, true><<<grid, kThreads, kSmemBytes, s>>>(a);
+        else f2_umma_kernel<2, false><<<grid, kThreads, kSmemBytes, s>>>(a);
+    }
+}
 
 }  // namespace
 
@@ -608,10 +691,7 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
     if (op.n_rt <= 0 || op.n_ck <= 0) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs tiled planes");
     p->images = static_cast<const uint8_t*>(op.planes);
     p->n_ck = op.n_ck;
-    STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(kSmemBytes)));
-    STPF2_CUDA(cudaFuncSetAttribute(f2_umma_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(kSmemBytes)));
+    set_umma_smem();
     return p.release();
 }
 
@@ -661,18 +741,123 @@ void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, 
     a.idesc_am = idesc_f16(bf16, false);
     a.idesc_i8 = idesc_u8_s32();
     const int grid = std::min(c.sm_count, n_items);
-    if (p->chunk_stages == 1) f2_umma_kernel<1><<<grid, kThreads, kSmemBytes, s>>>(a);
-    else f2_umma_kernel<2><<<grid, kThreads, kSmemBytes, s>>>(a);
+    launch_kernel(p->chunk_stages, false, grid, a, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         cudaFuncAttributes fa{};
-        cudaFuncGetAttributes(&fa, f2_umma_kernel<2>);
+        cudaFuncGetAttributes(&fa, f2_umma_kernel<2, false>);
         fail(STP_CUDA_ERROR, std::string("f2_umma_kernel launch: ") + cudaGetErrorString(e) + " (regs " +
                                  std::to_string(fa.numRegs) + ", max threads " + std::to_string(fa.maxThreadsPerBlock) +
                                  ", dyn smem " + std::to_string(kSmemBytes) + ", max dyn smem " +
                                  std::to_string(fa.maxDynamicSharedSizeBytes) + ", local " +
                                  std::to_string(fa.localSizeBytes) + ")");
     }
+    c.launches++;
+}
+
+void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stages, const std::vector<GroupSpec>& groups,
+                            cudaStream_t s, std::vector<unsigned long long>* stamps) {
+    if (fmt == OpFmt::F32) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs split 16-bit planes");
+    if (chunk_stages != 1 && chunk_stages != 2) fail(STP_INVALID_ARGUMENT, "chunk stages must be 1 or 2");
+    const int G = static_cast<int>(groups.size());
+    if (stamps) stamps->assign(static_cast<size_t>(G), 0ull);
+    // Requests in ascending order of work (shortest first: lower median completion), each
+    // request's items costliest-first and its tile pairs together.
+    std::vector<double> cost(static_cast<size_t>(G), 0.0);
+    for (int g = 0; g < G; ++g) {
+        const int T = (groups[g].info.P + kTile - 1) / kTile;
+        for (const BlockInfo& b : groups[g].L->blocks) cost[g] += static_cast<double>(stages_of_host(b.k)) * T * (T + 1) / 2;
+    }
+    std::vector<int> ord(static_cast<size_t>(G));
+    for (int g = 0; g < G; ++g) ord[g] = g;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return cost[x] < cost[y]; });
+    std::vector<BlockInfo> blocks;
+    std::vector<WorkItem> items;
+    std::vector<int> n_items(static_cast<size_t>(G), 0);
+    std::vector<GroupInfo> info(static_cast<size_t>(G));
+    int max_k = 0;
+    for (int g : ord) {
+        const BlockLayout& L = *groups[g].L;
+        info[g] = groups[g].info;
+        const int base = static_cast<int>(blocks.size());
+        for (BlockInfo b : L.blocks) {
+            b.grp = g;
+            blocks.push_back(b);
+            max_k = std::max(max_k, b.k);
+        }
+        if (info[g].P <= 0) continue;
+        for (WorkItem w : make_work_items(L, info[g].P, kTile)) {
+            w.blk += base;
+            items.push_back(w);
+            n_items[g]++;
+        }
+    }
+    if (items.empty()) return;
+    if (items.size() > static_cast<size_t>(INT_MAX)) fail(STP_RUNTIME_ERROR, "too many work items in one batch");
+    std::vector<double> rcp(static_cast<size_t>(max_k) + 1, 0.0);
+    for (int k = 1; k <= max_k; ++k) rcp[k] = 1.0 / static_cast<double>(k);
+    DevBuf d_items, d_blocks, d_info, d_rcp, d_nitems, d_done, d_ns, d_err, d_counter;
+    auto up = [&](DevBuf& b, const void* h, size_t n) {
+        b.reserve(std::max<size_t>(n, 16));
+        STPF2_CUDA(cudaMemcpyAsync(b.ptr, h, n, cudaMemcpyHostToDevice, s));
+    };
+    up(d_items, items.data(), items.size() * sizeof(WorkItem));
+    up(d_blocks, blocks.data(), blocks.size() * sizeof(BlockInfo));
+    up(d_info, info.data(), info.size() * sizeof(GroupInfo));
+    up(d_rcp, rcp.data(), rcp.size() * sizeof(double));
+    up(d_nitems, n_items.data(), n_items.size() * sizeof(int));
+    d_done.reserve(std::max<size_t>(static_cast<size_t>(G) * sizeof(int), 16));
+    d_ns.reserve(std::max<size_t>(static_cast<size_t>(G) * sizeof(unsigned long long), 16));
+    d_err.reserve(16);
+    d_counter.reserve(16);
+    STPF2_CUDA(cudaMemsetAsync(d_done.ptr, 0, d_done.bytes, s));
+    STPF2_CUDA(cudaMemsetAsync(d_ns.ptr, 0, d_ns.bytes, s));
+    STPF2_CUDA(cudaMemsetAsync(d_err.ptr, 0, 16, s));
+    STPF2_CUDA(cudaMemsetAsync(d_counter.ptr, 0, 16, s));
+    set_umma_smem();
+
+    UmmaArgs a{};
+    a.images = info[ord[0]].images;
+    a.n_ck = info[ord[0]].n_ck;
+    a.P = info[ord[0]].P;
+    a.f2 = info[ord[0]].f2;
+    a.vpair = info[ord[0]].vpair;
+    a.items = d_items.as<WorkItem>();
+    a.n_items = static_cast<int>(items.size());
+    a.next_item = d_counter.as<int>();
+    a.blocks = d_blocks.as<BlockInfo>();
+    a.num_scale = 2.0 * scale_inv;
+    a.rcp = d_rcp.as<double>();
+    a.rcp_max = max_k;
+    a.err = d_err.as<int>();
+    const bool bf16 = fmt == OpFmt::BF16;
+    a.idesc_pp = idesc_f16(bf16, true);
+    a.idesc_am = idesc_f16(bf16, false);
+    a.idesc_i8 = idesc_u8_s32();
+    a.groups = d_info.as<GroupInfo>();
+    a.grp_done = d_done.as<int>();
+    a.grp_ns = d_ns.as<unsigned long long>();
+    a.grp_items = d_nitems.as<int>();
+    const int grid = std::min(c.sm_count, a.n_items);
+    launch_kernel(chunk_stages, true, grid, a, s);
+    STPF2_CUDA(cudaGetLastError());
+    c.launches++;
+    int err = 0;
+    STPF2_CUDA(cudaMemcpyAsync(&err, d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (stamps)
+        STPF2_CUDA(cudaMemcpyAsync(stamps->data(), d_ns.ptr, static_cast<size_t>(G) * sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToHost, s));
+    STPF2_CUDA(cudaStreamSynchronize(s));
+    if (err) fail(STP_DEVICE_TIMEOUT, "grouped tensor-core contraction: a bounded device wait expired; results are invalid");
+}
+
+namespace {
+__global__ void timestamp_kernel(unsigned long long* dst) { *dst = globaltimer(); }
+}  // namespace
+
+void launch_timestamp(Ctx& c, unsigned long long* dst, cudaStream_t s) {
+    timestamp_kernel<<<1, 1, 0, s>>>(dst);
+    STPF2_CUDA(cudaGetLastError());
     c.launches++;
 }
 

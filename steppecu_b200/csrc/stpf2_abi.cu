@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <array>
 #include <climits>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -188,8 +189,13 @@ struct Plan {
 namespace {
 
 // Validates a request and builds its plan. planes_base != nullptr borrows operand
-// storage (at least operand_plane_bytes) instead of allocating it.
-std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch, void* planes_base) {
+// storage (at least operand_plane_bytes) instead of allocating it. A batch member (a
+// request of a grouped batch) gets only its descriptors, block layout and tile tables:
+// the batch owns the records, the shared canonical genotypes and the contraction, and its
+// planes need no clearing (every column of rows < P is written by the decode, and rows
+// >= P of the last row tile only reach accumulator rows that are never stored).
+std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch, void* planes_base,
+                                 bool batch_member = false) {
     need(r.n_pop >= 0 && r.geno.n_snp >= 0 && r.n_block >= 0, "negative extent");
     need(r.geno.bytes_per_record > 0 || r.geno.n_snp == 0, "bytes_per_record is 0");
     need(r.pop_offsets != nullptr || r.n_pop == 0, "pop_offsets is NULL");
@@ -242,7 +248,7 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
         need(slot < 0, "a sample is selected more than once");
         slot = static_cast<int32_t>(g);
     }
-    upload(p->pos, pos, s);
+    if (!batch_member) upload(p->pos, pos, s);
 
     // 1/n and 1/max(n-1, 1) for every called-allele count a population can reach.
     const int64_t n_max = 2 * max_pop + 1;
@@ -272,16 +278,19 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
     upload(p->tiles, tiles, s);
     upload(p->col_snp, col_snp, s);
     p->n_sel_pad = (n_sel + 3) / 4 * 4;
-    p->canon.reserve(std::max<size_t>(static_cast<size_t>((p->n_tiles + 3) / 4) * p->n_sel_pad * 32, 64));
-    p->center.reserve(std::max<size_t>(static_cast<size_t>(p->L.ld) * 8, 64));
+    if (!batch_member) {
+        p->canon.reserve(std::max<size_t>(static_cast<size_t>((p->n_tiles + 3) / 4) * p->n_sel_pad * 32, 64));
+        p->center.reserve(std::max<size_t>(static_cast<size_t>(p->L.ld) * 8, 64));
+    }
 
     // The transpose reads records with 4-byte (16-byte when aligned so) copies: records of
     // a pitch that is not a multiple of 4 are copied once per run into a 16-byte pitch.
     p->bpr = r.geno.bytes_per_record;
     p->src_pitch = pitch;
     const uint64_t need_bytes = static_cast<uint64_t>((r.geno.n_ind + 63) / 64) * 16;
-    p->repitch = (pitch % 4 != 0) || pitch < static_cast<uint64_t>((r.geno.n_ind + 3) / 4) ||
-                 (r.geno.on_device && reinterpret_cast<uintptr_t>(r.geno.records) % 4 != 0);
+    p->repitch = !batch_member &&
+                 ((pitch % 4 != 0) || pitch < static_cast<uint64_t>((r.geno.n_ind + 3) / 4) ||
+                  (r.geno.on_device && reinterpret_cast<uintptr_t>(r.geno.records) % 4 != 0));
     if (p->repitch) {
         p->pitch = (std::max<uint64_t>(r.geno.bytes_per_record, need_bytes) + 15) / 16 * 16;
         p->repitched.reserve(std::max<size_t>(static_cast<size_t>(p->pitch) * r.geno.n_snp, 64));
@@ -294,10 +303,11 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
         planes_base = p->own_planes.ptr;
     }
     // Padding columns must read as zero; decode only ever writes real SNP columns.
-    STPF2_CUDA(cudaMemsetAsync(planes_base, 0, ob, s));
+    if (!batch_member) STPF2_CUDA(cudaMemsetAsync(planes_base, 0, ob, s));
     bind_operand_planes(p->op, fmt, r.n_pop, p->L.ld, planes_base);
 
-    if (r.precision == STP_PREC_FP32_SIMT) {
+    if (batch_member) {
+    } else if (r.precision == STP_PREC_FP32_SIMT) {
         const std::vector<WorkItem> items = make_work_items(p->L, r.n_pop, simt_tile());
         p->n_items = static_cast<int>(items.size());
         upload(p->items, items, s);
@@ -512,6 +522,196 @@ void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
     }
     STPF2_CUDA(cudaStreamSynchronize(s));
     umma_check(p->umma);
+}
+
+// ---- grouped batch ----------------------------------------------------------------------
+
+// Requests that read the same genotype panel, so a batch can share one upload, one ploidy
+// pass and one canonical transpose.
+bool same_panel(const stp_geno_view& a, const stp_geno_view& b) {
+    return a.records == b.records && a.bytes_per_record == b.bytes_per_record && a.pitch == b.pitch &&
+           a.n_snp == b.n_snp && a.n_ind == b.n_ind && a.on_device == b.on_device;
+}
+
+// A batch of requests over one panel, all on the tensor cores with one arithmetic: the
+// union of their samples goes through one ploidy pass and one transpose into canonical
+// genotypes in contiguous SNP tiles; each request's decode reads its samples and its
+// blocks' 32-SNP windows from that copy into its own operand images; and one persistent
+// launch contracts every request's (block, tile pair) items. Requests whose images do not
+// fit in free device memory together run in consecutive waves of the same form.
+// done_ms[k] receives request idx[k]'s completion time from the start of the group.
+void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* outs, const std::vector<int>& idx,
+                           std::vector<double>& done_ms) {
+    cudaStream_t s = c.stream;
+    const stp_geno_view& g = reqs[idx[0]].geno;
+    const int64_t M = g.n_snp, n_ind = g.n_ind;
+    need(g.records != nullptr, "records is NULL");
+    need(n_ind > 0, "n_ind must be positive");
+    uint64_t pitch = g.pitch ? g.pitch : g.bytes_per_record;
+    need(pitch >= g.bytes_per_record, "pitch < bytes_per_record");
+    const int prec = reqs[idx[0]].precision;
+    const OpFmt fmt = fmt_of(prec);
+
+    // Records on the device at a pitch the transpose reads (a multiple of 4 bytes).
+    const uint8_t* d_rec = g.records;
+    DevBuf repitched;
+    if (!g.on_device) {
+        const uint64_t dp = device_pitch(g);
+        c.ws_records.reserve(static_cast<size_t>(dp) * M);
+        upload_rows(g, c.ws_records.as<uint8_t>(), dp, 0, M, s);
+        d_rec = c.ws_records.as<uint8_t>();
+        pitch = dp;
+    } else if (pitch % 4 != 0 || pitch < static_cast<uint64_t>((n_ind + 3) / 4) ||
+               reinterpret_cast<uintptr_t>(g.records) % 4 != 0) {
+        const uint64_t need_bytes = static_cast<uint64_t>((n_ind + 63) / 64) * 16;
+        const uint64_t dp = (std::max<uint64_t>(g.bytes_per_record, need_bytes) + 15) / 16 * 16;
+        repitched.reserve(static_cast<size_t>(dp) * M);
+        STPF2_CUDA(cudaMemcpy2DAsync(repitched.ptr, dp, g.records, pitch, g.bytes_per_record, static_cast<size_t>(M),
+                                     cudaMemcpyDeviceToDevice, s));
+        d_rec = repitched.as<uint8_t>();
+        pitch = dp;
+    }
+
+    // The union of the selected samples, in file order.
+    std::vector<int32_t> pos_u(static_cast<size_t>(n_ind), -1);
+    bool any_auto = false;
+    for (int k : idx) {
+        const stp_f2_request& r = reqs[k];
+        need(r.pop_offsets != nullptr, "pop_offsets is NULL");
+        const int64_t n_sel = r.pop_offsets[r.n_pop];
+        need(n_sel == 0 || r.sel_rows != nullptr, "sel_rows is NULL");
+        for (int64_t q = 0; q < n_sel; ++q) {
+            need(r.sel_rows[q] >= 0 && r.sel_rows[q] < n_ind, "sel_rows entry outside [0, n_ind)");
+            pos_u[static_cast<size_t>(r.sel_rows[q])] = 0;
+        }
+        any_auto = any_auto || (r.sample_ploidy == nullptr && r.ploidy_mode == STP_PLOIDY_AUTO);
+    }
+    std::vector<uint32_t> desc_u;
+    for (int64_t row = 0; row < n_ind; ++row)
+        if (pos_u[static_cast<size_t>(row)] == 0) {
+            pos_u[static_cast<size_t>(row)] = static_cast<int32_t>(desc_u.size());
+            desc_u.push_back(pack_sel(row, 0));
+        }
+    const int64_t n_u = static_cast<int64_t>(desc_u.size());
+    const int64_t n_u_pad = (n_u + 3) / 4 * 4;
+    const int64_t n_utiles = (M + kTileK - 1) / kTileK;
+    std::vector<TileInfo> tiles_u(static_cast<size_t>(n_utiles));
+    for (int64_t t = 0; t < n_utiles; ++t)
+        tiles_u[t] = TileInfo{static_cast<int32_t>(t * kTileK), static_cast<int32_t>(std::min<int64_t>(kTileK, M - t * kTileK))};
+    DevBuf d_pos_u, d_desc_u, d_tiles_u, d_canon_u, d_center_u, d_t0;
+    upload(d_pos_u, pos_u, s);
+    upload(d_desc_u, desc_u, s);
+    upload(d_tiles_u, tiles_u, s);
+    d_canon_u.reserve(std::max<size_t>(static_cast<size_t>((n_utiles + 3) / 4) * n_u_pad * 32, 64));
+    d_center_u.reserve(std::max<size_t>(static_cast<size_t>(n_utiles) * kTileK * 8, 64));
+    d_t0.reserve(16);
+
+    launch_timestamp(c, d_t0.as<unsigned long long>(), s);
+    if (any_auto) launch_detect_ploidy_pa(c, d_rec, pitch, M, d_desc_u.as<uint32_t>(), n_u, s);
+    launch_transpose_pa(c, d_rec, pitch, n_ind, d_tiles_u.as<TileInfo>(), n_utiles, d_pos_u.as<int32_t>(), n_u_pad,
+                        d_canon_u.as<uint64_t>(), d_center_u.as<double>(), s);
+
+    // Waves of requests whose operand images (and device-side outputs) fit together.
+    std::vector<size_t> img_bytes(idx.size()), out_bytes(idx.size());
+    for (size_t m = 0; m < idx.size(); ++m) {
+        const stp_f2_request& r = reqs[idx[m]];
+        const BlockLayout probe = make_block_layout(r.block_id, M, r.n_block);
+        img_bytes[m] = align256(operand_plane_bytes(fmt, r.n_pop, probe.ld));
+        const size_t elems = static_cast<size_t>(r.n_pop) * r.n_pop * r.n_block;
+        out_bytes[m] = outs[idx[m]].on_device ? 0 : 2 * align256(elems * sizeof(double));
+    }
+    STPF2_CUDA(cudaStreamSynchronize(s));
+    size_t free_b = 0, total_b = 0;
+    STPF2_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t held = c.ws_batch.bytes + c.ws_f2.bytes;
+    const size_t budget = (free_b + held) > (size_t(2) << 30) ? (free_b + held - (size_t(2) << 30)) * 9 / 10 : 0;
+    std::vector<std::vector<size_t>> waves(1);
+    size_t acc = 0;
+    for (size_t m = 0; m < idx.size(); ++m) {
+        const size_t b = img_bytes[m] + out_bytes[m];
+        if (!waves.back().empty() && acc + b > budget) {
+            waves.emplace_back();
+            acc = 0;
+        }
+        waves.back().push_back(m);
+        acc += b;
+    }
+    unsigned long long t0 = 0;
+    for (const auto& wave : waves) {
+        size_t img_total = 0, out_total = 0;
+        for (size_t m : wave) {
+            img_total += img_bytes[m];
+            out_total += out_bytes[m] / 2;
+        }
+        c.ws_batch.reserve(std::max<size_t>(img_total, 256));
+        if (out_total) {
+            c.ws_f2.reserve(out_total);
+            c.ws_vpair.reserve(out_total);
+        }
+        std::vector<std::unique_ptr<Plan>> plans;
+        std::vector<DevBuf> umaps(wave.size());
+        std::vector<GroupSpec> specs(wave.size());
+        size_t io = 0, oo = 0;
+        for (size_t w = 0; w < wave.size(); ++w) {
+            const int k = idx[wave[w]];
+            const stp_f2_request& r = reqs[k];
+            plans.push_back(build_plan(c, r, pitch, c.ws_batch.as<uint8_t>() + io, true));
+            Plan& p = *plans.back();
+            io += img_bytes[wave[w]];
+            std::vector<int32_t> umap(static_cast<size_t>(p.n_sel));
+            for (int64_t q = 0; q < p.n_sel; ++q) umap[q] = pos_u[static_cast<size_t>(r.sel_rows[q])];
+            upload(umaps[w], umap, s);
+            if (p.detect) launch_copy_union_ploidy(c, p.sel.as<uint32_t>(), umaps[w].as<int32_t>(), p.n_sel, d_desc_u.as<uint32_t>(), s);
+            CanonDecodeArgs a;
+            a.canon = d_canon_u.as<uint64_t>();
+            a.n_tiles = p.n_tiles;
+            a.n_sel = n_u_pad;
+            a.sel = p.sel.as<uint32_t>();
+            a.pop_off = p.pop_off.as<int32_t>();
+            a.P = p.P;
+            a.rec_n = p.rec_n.as<double>();
+            a.rec_nm1 = p.rec_nm1.as<double>();
+            a.col_snp = p.col_snp.as<int32_t>();
+            a.op = p.op;
+            a.umap = umaps[w].as<int32_t>();
+            a.tiles = p.tiles.as<TileInfo>();
+            a.n_utiles = n_utiles;
+            a.center_snp = d_center_u.as<double>();
+            launch_decode_canon(c, a, s);
+            const stp_f2_output& o = outs[k];
+            double* f2 = o.f2;
+            double* vp = o.vpair;
+            if (!o.on_device) {
+                f2 = reinterpret_cast<double*>(c.ws_f2.as<uint8_t>() + oo);
+                vp = reinterpret_cast<double*>(c.ws_vpair.as<uint8_t>() + oo);
+                oo += out_bytes[wave[w]] / 2;
+            }
+            specs[w].L = &p.L;
+            specs[w].info = GroupInfo{static_cast<const uint8_t*>(p.op.planes), f2, vp, p.op.n_ck, p.P, 0};
+            if (o.block_sizes) copy_block_sizes(p.L, o.block_sizes);
+        }
+        std::vector<unsigned long long> stamps;
+        launch_f2_umma_grouped(c, fmt, plans[0]->op.scale_inv, chunk_stages_of(prec), specs, s, &stamps);
+        if (t0 == 0) STPF2_CUDA(cudaMemcpy(&t0, d_t0.ptr, sizeof(t0), cudaMemcpyDeviceToHost));
+        for (size_t w = 0; w < wave.size(); ++w) {
+            const int k = idx[wave[w]];
+            done_ms[wave[w]] = stamps[w] >= t0 ? static_cast<double>(stamps[w] - t0) * 1e-6 : 0.0;
+            const stp_f2_output& o = outs[k];
+            const Plan& p = *plans[w];
+            const size_t elems = static_cast<size_t>(p.P) * p.P * p.L.n_block;
+            if (!o.on_device && elems) {
+                STPF2_CUDA(cudaMemcpyAsync(o.f2, specs[w].info.f2, elems * sizeof(double), cudaMemcpyDeviceToHost, s));
+                STPF2_CUDA(cudaMemcpyAsync(o.vpair, specs[w].info.vpair, elems * sizeof(double), cudaMemcpyDeviceToHost, s));
+            }
+            if (o.ploidy_out && p.n_sel > 0) {
+                std::vector<uint32_t> sel(static_cast<size_t>(p.n_sel));
+                STPF2_CUDA(cudaMemcpyAsync(sel.data(), p.sel.ptr, sel.size() * 4, cudaMemcpyDeviceToHost, s));
+                STPF2_CUDA(cudaStreamSynchronize(s));
+                for (size_t q = 0; q < sel.size(); ++q) o.ploidy_out[q] = static_cast<int32_t>(sel[q] & 3u);
+            }
+        }
+        STPF2_CUDA(cudaStreamSynchronize(s));
+    }
 }
 
 }  // namespace
@@ -828,12 +1028,46 @@ stp_status stp_f2_extract_batch(stp_ctx* ctx, const stp_f2_request* reqs, int32_
     return guarded([&] {
         need(ctx && (reqs || n_req == 0) && (outs || n_req == 0), "null argument");
         use_device(*ctx);
+        ctx->last_batch_ms.assign(static_cast<size_t>(std::max(n_req, 0)), std::nan(""));
+        // Tensor-core requests over the same panel with the same arithmetic run as one
+        // grouped batch; the rest (FP32 SIMT, empty requests) run one by one.
+        std::vector<std::vector<int>> groups;
         for (int32_t k = 0; k < n_req; ++k) {
-            if (reqs[k].n_block > 0 && outs[k].block_sizes)
-                std::fill(outs[k].block_sizes, outs[k].block_sizes + reqs[k].n_block, 0);
-            if (reqs[k].n_pop <= 0 || reqs[k].n_block <= 0) continue;
-            extract_one(*ctx, reqs[k], outs[k]);
+            const stp_f2_request& r = reqs[k];
+            if (r.n_block > 0 && outs[k].block_sizes)
+                std::fill(outs[k].block_sizes, outs[k].block_sizes + r.n_block, 0);
+            if (r.n_pop <= 0 || r.n_block <= 0) continue;
+            need(outs[k].f2 != nullptr && outs[k].vpair != nullptr, "output f2 / vpair is NULL");
+            fmt_of(r.precision);  // validates the mode
+            if (r.precision == STP_PREC_FP32_SIMT || r.geno.n_snp <= 0) {
+                extract_one(*ctx, r, outs[k]);
+                continue;
+            }
+            bool placed = false;
+            for (auto& grp : groups) {
+                const stp_f2_request& h = reqs[grp[0]];
+                if (same_panel(h.geno, r.geno) && h.precision == r.precision) {
+                    grp.push_back(k);
+                    placed = true;
+                    break;
+                }
+            }
+            if (!placed) groups.push_back({k});
         }
+        for (const auto& grp : groups) {
+            std::vector<double> done(grp.size(), 0.0);
+            extract_batch_grouped(*ctx, reqs, outs, grp, done);
+            for (size_t m = 0; m < grp.size(); ++m) ctx->last_batch_ms[static_cast<size_t>(grp[m])] = done[m];
+        }
+    });
+}
+
+stp_status stp_last_batch_times(stp_ctx* ctx, double* ms, int32_t n) {
+    return guarded([&] {
+        need(ctx != nullptr, "null context");
+        need(ms != nullptr || n <= 0, "null argument");
+        for (int32_t k = 0; k < n; ++k)
+            ms[k] = static_cast<size_t>(k) < ctx->last_batch_ms.size() ? ctx->last_batch_ms[static_cast<size_t>(k)] : std::nan("");
     });
 }
 

@@ -74,6 +74,10 @@ struct Ctx {
     // Grow-only scratch reused across calls of the host-buffer entry points, so repeated
     // extractions do not pay cudaMalloc each time.
     DevBuf ws_records, ws_f2, ws_vpair, ws_misc;
+    DevBuf ws_batch;  // operand images of a grouped batch
+    // Completion time of each request of the last stp_f2_extract_batch call, in ms from the
+    // start of its group's device work (NaN for requests that ran on their own).
+    std::vector<double> last_batch_ms;
 };
 
 // ---- block layout ---------------------------------------------------------------------
@@ -84,9 +88,21 @@ struct Ctx {
 constexpr int kColAlign = 64;
 
 struct BlockInfo {  // device-visible, one per jackknife block
-    int64_t col;    // first padded column
-    int32_t k;      // SNPs in the block
-    int32_t b;      // block id (slab index of the output)
+    int64_t col;      // first padded column
+    int32_t k;        // SNPs in the block
+    int32_t b;        // block id (slab index of the output)
+    int32_t grp = 0;  // request of a batch (index into the GroupInfo table)
+    int32_t pad_ = 0;
+};
+
+// One request of a grouped contraction: its operand images and its output slabs.
+struct GroupInfo {
+    const uint8_t* images;  // (row tile t, chunk c) at (t * n_ck + c) * kImageBytes
+    double* f2;             // [P x P x n_block]
+    double* vpair;
+    int64_t n_ck;
+    int32_t P;
+    int32_t pad_;
 };
 
 struct BlockLayout {
@@ -201,6 +217,17 @@ struct CanonDecodeArgs {
     OperandPlanes op;                  // planes == nullptr: counts only
     int32_t* cnt_ac2 = nullptr;        // optional [P x n_snp] column-major counts
     int32_t* cnt_n = nullptr;
+    // Shared-canonical mode (umap != nullptr), for a batch of requests over one panel:
+    // canon holds the union of every request's samples in contiguous SNP tiles (tile u =
+    // SNPs 32u .. 32u+31, n_sel = the union's padded count, n_utiles tiles). Sample g of
+    // this request is union sample umap[g]; the request's own tile t reads the 32-SNP
+    // window starting at tiles[t].snp0 (two union words, shifted) with columns from
+    // tiles[t].nvalid on read as missing; centres come per SNP from center_snp through
+    // col_snp (center unused).
+    const int32_t* umap = nullptr;
+    const TileInfo* tiles = nullptr;
+    int64_t n_utiles = 0;
+    const double* center_snp = nullptr;
 };
 
 void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_snp,
@@ -222,6 +249,23 @@ void launch_f2_simt(Ctx& c, const WorkItem* items, int n_items, const BlockInfo*
 
 // tcgen05 contraction; returns false if the device cannot run it.
 struct UmmaPlan;
+// One request of a grouped contraction (a batch over one panel): its block layout and its
+// images / outputs.
+struct GroupSpec {
+    const BlockLayout* L = nullptr;
+    GroupInfo info{};
+};
+// Contracts every request of a batch in one persistent launch over all their (block, tile
+// pair) items, requests in ascending order of work. stamps (optional) receives each
+// request's completion time (%globaltimer, ns). Synchronises s; timeouts raise.
+void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stages, const std::vector<GroupSpec>& groups,
+                            cudaStream_t s, std::vector<unsigned long long>* stamps);
+// %globaltimer of the device when the stream reaches this point, written to *dst.
+void launch_timestamp(Ctx& c, unsigned long long* dst, cudaStream_t s);
+// desc[g] takes the ploidy bits of union sample umap[g] (a batch's shared ploidy pass).
+void launch_copy_union_ploidy(Ctx& c, uint32_t* desc, const int32_t* umap, int64_t n_sel, const uint32_t* desc_u,
+                              cudaStream_t s);
+
 // chunk_stages: 32-SNP stages per FP32 TMEM chunk (1 or 2).
 UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L, int chunk_stages);
 // 32-SNP stages per FP32 chunk for a tensor-core precision mode.
