@@ -215,6 +215,85 @@ def run_e2e(args, ctx, rec, panel, sel, po, bpr, n_out, barrier, dist, dev, P, M
     return e2e
 
 
+def run_batched(dev: str, steps: int = 3, n_req: int = 64) -> dict:
+    """Many requests over one shared panel (8,000 samples x 1.15M SNPs, 64 requests of
+    4-300 populations, each with its own 5 cM block map): one grouped stp_f2_extract_batch
+    call against the same requests extracted one after another (plain FP32 SIMT and
+    split-F16). Records and outputs stay in HBM; each call is synchronous and timed on the
+    host around it (its planning is part of the cost); per-request completion times of the
+    grouped call come from device stamps."""
+    import numpy as np
+    import torch
+
+    import steppecu_b200 as sb
+    from steppecu_b200 import synth
+
+    panel = synth.generate("c5", seed=20261203 + 5, device=dev)
+    reqs = synth.batch_requests(panel, n_req=n_req)
+    M = panel.n_snp
+    bpr = panel.bytes_per_record
+    pitch = (bpr + 15) // 16 * 16
+    rec = torch.zeros((M, pitch), dtype=torch.uint8, device=dev)
+    rec[:, :bpr] = panel.records
+    panel.records = None
+    Ps = [len(q["pop_offsets"]) - 1 for q in reqs]
+    total_units = sum(units(P, M) for P in Ps)
+    outs = []
+    for q, P in zip(reqs, Ps):
+        n = P * P * q["n_block"]
+        outs.append((torch.empty(n, dtype=torch.float64, device=dev), torch.empty(n, dtype=torch.float64, device=dev)))
+    ctx = sb.Context(int(dev.split(":")[1]) if ":" in dev else 0)
+
+    def grouped():
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ctx.extract_batch(rec, panel.n_ind, reqs, precision="split_f16", out=outs)
+        return time.perf_counter() - t
+
+    grouped()  # warm-up (allocates the batch workspace)
+    l0 = ctx.launches
+    wall = [grouped() for _ in range(steps)]
+    launches = (ctx.launches - l0) / steps
+    done = ctx.last_batch_times(len(reqs))
+    ref = [(f2.clone(), vp.clone()) for f2, vp in outs]
+
+    def serial(precision: str):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        comp = []
+        for q, (f2, vp) in zip(reqs, outs):
+            ctx.extract_blocks(rec, panel.n_ind, q["sel_rows"], q["pop_offsets"], q["block_id"], q["n_block"],
+                               precision=precision, out=(f2, vp))
+            comp.append((time.perf_counter() - t0) * 1e3)
+        return comp
+
+    serial("split_f16")  # warm-up
+    ser_f16 = serial("split_f16")
+    same = all(torch.equal(a, c) and torch.equal(b, d) for (a, b), (c, d) in zip(ref, outs))
+    serial("fp32")
+    ser_f32 = serial("fp32")
+    ctx.close()
+    med = float(np.median(wall))
+
+    def pct(x, p):
+        return float(np.percentile(np.asarray(x), p))
+
+    return {
+        "workload": "c5: 64 requests over one panel of 8,000 samples (400 pops x 20) x 1.15M SNPs",
+        "requests": len(reqs), "populations_per_request": {"min": min(Ps), "max": max(Ps), "sum_sq": int(sum(P * P for P in Ps))},
+        "units": total_units,
+        "grouped": {"value": total_units / med, "unit": UNIT, "ms_per_call": med * 1e3, "calls": steps,
+                    "device_span_ms": float(np.nanmax(done)), "completion_ms_p50": pct(done, 50),
+                    "completion_ms_p99": pct(done, 99), "gpu_launches": launches,
+                    "equals_serial_split_f16": bool(same)},
+        "serial_split_f16": {"value": total_units / (ser_f16[-1] / 1e3), "ms_total": ser_f16[-1],
+                             "completion_ms_p50": pct(ser_f16, 50), "completion_ms_p99": pct(ser_f16, 99)},
+        "serial_fp32": {"value": total_units / (ser_f32[-1] / 1e3), "ms_total": ser_f32[-1],
+                        "completion_ms_p50": pct(ser_f32, 50), "completion_ms_p99": pct(ser_f32, 99)},
+        "timing": "host wall clock around each synchronous call; completion of grouped requests from device stamps",
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -231,6 +310,8 @@ def main():
     ap.add_argument("--cpu-threads", type=int, default=None)
     ap.add_argument("--snps", type=int, default=None, help="override the workload's SNP count (smaller cases)")
     ap.add_argument("--quick", action="store_true", help="headline timing only: no other arithmetics, e2e or CPU leg")
+    ap.add_argument("--no-batched", dest="batched", action="store_false",
+                    help="skip the many-requests (grouped batch) measurement")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -382,6 +463,15 @@ def main():
         modes = [args.precision] + [m for m in ("split_f16_fine", "split_bf16", "fp32") if m != args.precision]
         precision = {"against": f"{kind} CPU f2 on the cpu_baseline sample", **precision_report(ctx, sample, modes)}
 
+    batched = None
+    if world == 1 and not args.quick and args.batched:
+        plan.close()
+        ctx.close()
+        del rec, f2, vp, plan, ctx
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        batched = run_batched(dev)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -397,10 +487,12 @@ def main():
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "other_arithmetics": others,
             "per_block_launches": per_block,
+            "batched_requests": batched,
         }
         print(json.dumps(line), flush=True)
-    plan.close()
-    ctx.close()
+    if batched is None:
+        plan.close()
+        ctx.close()
     if dist is not None:
         dist.destroy_process_group()
 

@@ -720,6 +720,43 @@ __global__ void copy_union_ploidy_kernel(uint32_t* __restrict__ desc, const int3
 }
 }  // namespace
 
+namespace {
+// Column c of the padded space belongs to the last block whose first column is <= c (empty
+// blocks share their successor's first column and cover nothing).
+__global__ void layout_tables_kernel(const BlockInfo* __restrict__ blocks, const int64_t* __restrict__ snp_begin,
+                                     int n_block, int64_t ld, int32_t* __restrict__ col_snp,
+                                     TileInfo* __restrict__ tiles) {
+    const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c >= ld) return;
+    int lo = 0, hi = n_block;  // first block with col > c
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (blocks[mid].col <= c) lo = mid + 1;
+        else hi = mid;
+    }
+    const int b = lo - 1;
+    int64_t off = -1, k = 0, s0 = 0;
+    if (b >= 0) {
+        off = c - blocks[b].col;
+        k = blocks[b].k;
+        s0 = snp_begin[b];
+    }
+    const bool real = b >= 0 && off < k;
+    col_snp[c] = real ? static_cast<int32_t>(s0 + off) : -1;
+    if ((c & 31) == 0)
+        tiles[c >> 5] = real ? TileInfo{static_cast<int32_t>(s0 + off), static_cast<int32_t>(k - off < 32 ? k - off : 32)}
+                             : TileInfo{0, 0};
+}
+}  // namespace
+
+void launch_layout_tables(Ctx& c, const BlockInfo* blocks, const int64_t* snp_begin, int n_block, int64_t ld,
+                          int32_t* col_snp, TileInfo* tiles, cudaStream_t s) {
+    if (ld <= 0) return;
+    layout_tables_kernel<<<static_cast<unsigned>((ld + 255) / 256), 256, 0, s>>>(blocks, snp_begin, n_block, ld, col_snp, tiles);
+    STPF2_CUDA(cudaGetLastError());
+    c.launches++;
+}
+
 void launch_copy_union_ploidy(Ctx& c, uint32_t* desc, const int32_t* umap, int64_t n_sel, const uint32_t* desc_u,
                               cudaStream_t s) {
     if (n_sel <= 0) return;

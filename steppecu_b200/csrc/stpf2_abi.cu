@@ -7,6 +7,9 @@
 // launches the kernels in decode.cu, f2_simt.cu, f2_umma.cu and jackknife.cu. There is
 // no CPU fallback: without a CUDA device every entry point returns STP_NO_DEVICE.
 #include <algorithm>
+#include <thread>
+#include <exception>
+#include <atomic>
 #include <array>
 #include <climits>
 #include <cmath>
@@ -64,7 +67,7 @@ void upload(DevBuf& b, const std::vector<T>& h, cudaStream_t s) {
 
 // ---- layout ---------------------------------------------------------------------------
 
-BlockLayout make_block_layout(const int32_t* block_id, int64_t n_snp, int n_block) {
+BlockLayout make_block_layout(const int32_t* block_id, int64_t n_snp, int n_block, bool with_snp_col) {
     BlockLayout L;
     L.n_block = n_block;
     L.n_snp = n_snp;
@@ -97,6 +100,7 @@ BlockLayout make_block_layout(const int32_t* block_id, int64_t n_snp, int n_bloc
     L.ld = std::max<int64_t>(col, kColAlign);
     if (L.ld > INT_MAX)
         fail(STP_RUNTIME_ERROR, "padded SNP axis exceeds INT_MAX columns (M > INT_MAX)");
+    if (!with_snp_col) return L;
     L.snp_col.resize(static_cast<size_t>(n_snp));
     for (int64_t s = 0; s < n_snp; ++s) {
         const int b = block_id[s];
@@ -189,13 +193,8 @@ struct Plan {
 namespace {
 
 // Validates a request and builds its plan. planes_base != nullptr borrows operand
-// storage (at least operand_plane_bytes) instead of allocating it. A batch member (a
-// request of a grouped batch) gets only its descriptors, block layout and tile tables:
-// the batch owns the records, the shared canonical genotypes and the contraction, and its
-// planes need no clearing (every column of rows < P is written by the decode, and rows
-// >= P of the last row tile only reach accumulator rows that are never stored).
-std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch, void* planes_base,
-                                 bool batch_member = false) {
+// storage (at least operand_plane_bytes) instead of allocating it.
+std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch, void* planes_base) {
     need(r.n_pop >= 0 && r.geno.n_snp >= 0 && r.n_block >= 0, "negative extent");
     need(r.geno.bytes_per_record > 0 || r.geno.n_snp == 0, "bytes_per_record is 0");
     need(r.pop_offsets != nullptr || r.n_pop == 0, "pop_offsets is NULL");
@@ -248,7 +247,7 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
         need(slot < 0, "a sample is selected more than once");
         slot = static_cast<int32_t>(g);
     }
-    if (!batch_member) upload(p->pos, pos, s);
+    upload(p->pos, pos, s);
 
     // 1/n and 1/max(n-1, 1) for every called-allele count a population can reach.
     const int64_t n_max = 2 * max_pop + 1;
@@ -278,19 +277,16 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
     upload(p->tiles, tiles, s);
     upload(p->col_snp, col_snp, s);
     p->n_sel_pad = (n_sel + 3) / 4 * 4;
-    if (!batch_member) {
-        p->canon.reserve(std::max<size_t>(static_cast<size_t>((p->n_tiles + 3) / 4) * p->n_sel_pad * 32, 64));
-        p->center.reserve(std::max<size_t>(static_cast<size_t>(p->L.ld) * 8, 64));
-    }
+    p->canon.reserve(std::max<size_t>(static_cast<size_t>((p->n_tiles + 3) / 4) * p->n_sel_pad * 32, 64));
+    p->center.reserve(std::max<size_t>(static_cast<size_t>(p->L.ld) * 8, 64));
 
     // The transpose reads records with 4-byte (16-byte when aligned so) copies: records of
     // a pitch that is not a multiple of 4 are copied once per run into a 16-byte pitch.
     p->bpr = r.geno.bytes_per_record;
     p->src_pitch = pitch;
     const uint64_t need_bytes = static_cast<uint64_t>((r.geno.n_ind + 63) / 64) * 16;
-    p->repitch = !batch_member &&
-                 ((pitch % 4 != 0) || pitch < static_cast<uint64_t>((r.geno.n_ind + 3) / 4) ||
-                  (r.geno.on_device && reinterpret_cast<uintptr_t>(r.geno.records) % 4 != 0));
+    p->repitch = (pitch % 4 != 0) || pitch < static_cast<uint64_t>((r.geno.n_ind + 3) / 4) ||
+                 (r.geno.on_device && reinterpret_cast<uintptr_t>(r.geno.records) % 4 != 0);
     if (p->repitch) {
         p->pitch = (std::max<uint64_t>(r.geno.bytes_per_record, need_bytes) + 15) / 16 * 16;
         p->repitched.reserve(std::max<size_t>(static_cast<size_t>(p->pitch) * r.geno.n_snp, 64));
@@ -303,11 +299,10 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
         planes_base = p->own_planes.ptr;
     }
     // Padding columns must read as zero; decode only ever writes real SNP columns.
-    if (!batch_member) STPF2_CUDA(cudaMemsetAsync(planes_base, 0, ob, s));
+    STPF2_CUDA(cudaMemsetAsync(planes_base, 0, ob, s));
     bind_operand_planes(p->op, fmt, r.n_pop, p->L.ld, planes_base);
 
-    if (batch_member) {
-    } else if (r.precision == STP_PREC_FP32_SIMT) {
+    if (r.precision == STP_PREC_FP32_SIMT) {
         const std::vector<WorkItem> items = make_work_items(p->L, r.n_pop, simt_tile());
         p->n_items = static_cast<int>(items.size());
         upload(p->items, items, s);
@@ -533,13 +528,105 @@ bool same_panel(const stp_geno_view& a, const stp_geno_view& b) {
            a.n_snp == b.n_snp && a.n_ind == b.n_ind && a.on_device == b.on_device;
 }
 
+// One request of a grouped batch: what the host prepares (in parallel with the others)
+// and the device tables it uploads.
+struct BatchMember {
+    int k = 0;  // index of the request
+    int P = 0;
+    int64_t n_sel = 0;
+    bool detect = false;
+    BlockLayout L;
+    std::vector<uint32_t> sel;
+    std::vector<int32_t> pop_off, umap;
+    std::vector<double> rn, rnm1;
+    size_t img_bytes = 0, out_bytes = 0;
+    DevBuf d_sel, d_pop_off, d_umap, d_rn, d_rnm1, d_blocks, d_snp_begin, d_col_snp, d_tiles;
+    OperandPlanes op;
+};
+
+// Validates request r (the same rules as build_plan) and fills m's host tables. Host only,
+// safe to run for several members at once.
+void prepare_member(const stp_f2_request& r, const stp_f2_output& o, const std::vector<int32_t>& pos_u, OpFmt fmt,
+                    BatchMember& m) {
+    need(r.n_pop > 0 && r.n_block > 0, "empty request in a batch");
+    need(r.pop_offsets != nullptr, "pop_offsets is NULL");
+    need(r.pop_offsets[0] == 0, "pop_offsets[0] must be 0");
+    for (int i = 0; i < r.n_pop; ++i) need(r.pop_offsets[i + 1] >= r.pop_offsets[i], "pop_offsets must be non-decreasing");
+    const int64_t n_sel = r.pop_offsets[r.n_pop];
+    need(n_sel == 0 || r.sel_rows != nullptr, "sel_rows is NULL");
+    need(n_sel < INT_MAX, "too many selected samples");
+    need(r.block_id != nullptr, "block_id is NULL");
+    m.P = r.n_pop;
+    m.n_sel = n_sel;
+    const bool auto_ploidy = r.sample_ploidy == nullptr && r.ploidy_mode == STP_PLOIDY_AUTO;
+    m.detect = auto_ploidy;
+    m.sel.resize(static_cast<size_t>(n_sel));
+    m.umap.resize(static_cast<size_t>(n_sel));
+    std::vector<char> seen(pos_u.size(), 0);
+    for (int64_t g = 0; g < n_sel; ++g) {
+        const int64_t row = r.sel_rows[g];
+        need(row >= 0 && row < static_cast<int64_t>(pos_u.size()), "sel_rows entry outside [0, n_ind)");
+        need(static_cast<uint64_t>(row / 4) < r.geno.bytes_per_record, "sel_rows entry beyond the record");
+        need(!seen[static_cast<size_t>(row)], "a sample is selected more than once");
+        seen[static_cast<size_t>(row)] = 1;
+        int pl = 0;
+        if (r.sample_ploidy) pl = r.sample_ploidy[g];
+        else if (r.ploidy_mode == STP_PLOIDY_PSEUDO) pl = 1;
+        else if (r.ploidy_mode == STP_PLOIDY_DIPLOID) pl = 2;
+        else need(auto_ploidy, "unknown ploidy_mode");
+        if (pl != 1 && pl != 2) pl = 0;  // a bad ploidy contributes nothing (decode_af.hpp:58-65)
+        m.sel[g] = pack_sel(row, pl);
+        m.umap[g] = pos_u[static_cast<size_t>(row)];
+    }
+    m.pop_off.assign(static_cast<size_t>(r.n_pop) + 1, 0);
+    int64_t max_pop = 0;
+    for (int i = 0; i <= r.n_pop; ++i) m.pop_off[i] = static_cast<int32_t>(r.pop_offsets[i]);
+    for (int i = 0; i < r.n_pop; ++i) max_pop = std::max<int64_t>(max_pop, r.pop_offsets[i + 1] - r.pop_offsets[i]);
+    need(max_pop <= 16383, "a population has more than 16383 samples");
+    const int64_t n_max = 2 * max_pop + 1;
+    m.rn.assign(static_cast<size_t>(n_max) + 1, 0.0);
+    m.rnm1.assign(static_cast<size_t>(n_max) + 1, 1.0);
+    for (int64_t n = 1; n <= n_max; ++n) {
+        m.rn[n] = 1.0 / static_cast<double>(n);
+        m.rnm1[n] = 1.0 / std::max(static_cast<double>(n) - 1.0, 1.0);
+    }
+    m.L = make_block_layout(r.block_id, r.geno.n_snp, r.n_block, false);
+    m.img_bytes = align256(operand_plane_bytes(fmt, r.n_pop, m.L.ld));
+    const size_t elems = static_cast<size_t>(r.n_pop) * r.n_pop * r.n_block;
+    m.out_bytes = o.on_device ? 0 : 2 * align256(elems * sizeof(double));
+}
+
+// Runs f(i) for i in [0, n) on up to hardware_concurrency threads; rethrows the first error.
+template <class F>
+void parallel_for(int n, F&& f) {
+    const int nt = std::max(1, std::min<int>(n, static_cast<int>(std::thread::hardware_concurrency())));
+    std::atomic<int> next{0};
+    std::vector<std::exception_ptr> errs(static_cast<size_t>(nt));
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            try {
+                for (int i = next++; i < n; i = next++) f(i);
+            } catch (...) {
+                errs[t] = std::current_exception();
+            }
+        });
+    for (auto& x : th) x.join();
+    for (auto& e : errs)
+        if (e) std::rethrow_exception(e);
+}
+
 // A batch of requests over one panel, all on the tensor cores with one arithmetic: the
 // union of their samples goes through one ploidy pass and one transpose into canonical
 // genotypes in contiguous SNP tiles; each request's decode reads its samples and its
 // blocks' 32-SNP windows from that copy into its own operand images; and one persistent
-// launch contracts every request's (block, tile pair) items. Requests whose images do not
-// fit in free device memory together run in consecutive waves of the same form.
-// done_ms[k] receives request idx[k]'s completion time from the start of the group.
+// launch contracts every request's (block, tile pair) items. The requests' host tables are
+// prepared in parallel while the device runs the shared passes; their column and tile maps
+// are built on the device. Requests whose images do not fit in free device memory together
+// run in consecutive waves of the same form. The images are not cleared: the decode writes
+// every column of rows < P, and rows >= P of a request's last row tile only reach
+// accumulator rows that are never stored. done_ms[m] receives request idx[m]'s completion
+// time from the start of the group.
 void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* outs, const std::vector<int>& idx,
                            std::vector<double>& done_ms) {
     cudaStream_t s = c.stream;
@@ -547,6 +634,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
     const int64_t M = g.n_snp, n_ind = g.n_ind;
     need(g.records != nullptr, "records is NULL");
     need(n_ind > 0, "n_ind must be positive");
+    need(g.bytes_per_record > 0, "bytes_per_record is 0");
     uint64_t pitch = g.pitch ? g.pitch : g.bytes_per_record;
     need(pitch >= g.bytes_per_record, "pitch < bytes_per_record");
     const int prec = reqs[idx[0]].precision;
@@ -611,24 +699,23 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
     launch_transpose_pa(c, d_rec, pitch, n_ind, d_tiles_u.as<TileInfo>(), n_utiles, d_pos_u.as<int32_t>(), n_u_pad,
                         d_canon_u.as<uint64_t>(), d_center_u.as<double>(), s);
 
+    // Host tables of every request, in parallel, while the device runs the shared passes.
+    std::vector<BatchMember> mem(idx.size());
+    parallel_for(static_cast<int>(idx.size()), [&](int m) {
+        mem[m].k = idx[m];
+        prepare_member(reqs[idx[m]], outs[idx[m]], pos_u, fmt, mem[m]);
+    });
+
     // Waves of requests whose operand images (and device-side outputs) fit together.
-    std::vector<size_t> img_bytes(idx.size()), out_bytes(idx.size());
-    for (size_t m = 0; m < idx.size(); ++m) {
-        const stp_f2_request& r = reqs[idx[m]];
-        const BlockLayout probe = make_block_layout(r.block_id, M, r.n_block);
-        img_bytes[m] = align256(operand_plane_bytes(fmt, r.n_pop, probe.ld));
-        const size_t elems = static_cast<size_t>(r.n_pop) * r.n_pop * r.n_block;
-        out_bytes[m] = outs[idx[m]].on_device ? 0 : 2 * align256(elems * sizeof(double));
-    }
-    STPF2_CUDA(cudaStreamSynchronize(s));
     size_t free_b = 0, total_b = 0;
     STPF2_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t held = c.ws_batch.bytes + c.ws_f2.bytes;
-    const size_t budget = (free_b + held) > (size_t(2) << 30) ? (free_b + held - (size_t(2) << 30)) * 9 / 10 : 0;
+    const size_t held = c.ws_batch.bytes + c.ws_f2.bytes + c.ws_vpair.bytes;
+    const size_t avail = free_b + held;
+    const size_t budget = avail > (size_t(2) << 30) ? (avail - (size_t(2) << 30)) * 9 / 10 : 0;
     std::vector<std::vector<size_t>> waves(1);
     size_t acc = 0;
-    for (size_t m = 0; m < idx.size(); ++m) {
-        const size_t b = img_bytes[m] + out_bytes[m];
+    for (size_t m = 0; m < mem.size(); ++m) {
+        const size_t b = mem[m].img_bytes + mem[m].out_bytes;
         if (!waves.back().empty() && acc + b > budget) {
             waves.emplace_back();
             acc = 0;
@@ -640,64 +727,69 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
     for (const auto& wave : waves) {
         size_t img_total = 0, out_total = 0;
         for (size_t m : wave) {
-            img_total += img_bytes[m];
-            out_total += out_bytes[m] / 2;
+            img_total += mem[m].img_bytes;
+            out_total += mem[m].out_bytes / 2;
         }
         c.ws_batch.reserve(std::max<size_t>(img_total, 256));
         if (out_total) {
             c.ws_f2.reserve(out_total);
             c.ws_vpair.reserve(out_total);
         }
-        std::vector<std::unique_ptr<Plan>> plans;
-        std::vector<DevBuf> umaps(wave.size());
         std::vector<GroupSpec> specs(wave.size());
         size_t io = 0, oo = 0;
         for (size_t w = 0; w < wave.size(); ++w) {
-            const int k = idx[wave[w]];
-            const stp_f2_request& r = reqs[k];
-            plans.push_back(build_plan(c, r, pitch, c.ws_batch.as<uint8_t>() + io, true));
-            Plan& p = *plans.back();
-            io += img_bytes[wave[w]];
-            std::vector<int32_t> umap(static_cast<size_t>(p.n_sel));
-            for (int64_t q = 0; q < p.n_sel; ++q) umap[q] = pos_u[static_cast<size_t>(r.sel_rows[q])];
-            upload(umaps[w], umap, s);
-            if (p.detect) launch_copy_union_ploidy(c, p.sel.as<uint32_t>(), umaps[w].as<int32_t>(), p.n_sel, d_desc_u.as<uint32_t>(), s);
+            BatchMember& p = mem[wave[w]];
+            const stp_f2_output& o = outs[p.k];
+            upload(p.d_sel, p.sel, s);
+            upload(p.d_pop_off, p.pop_off, s);
+            upload(p.d_umap, p.umap, s);
+            upload(p.d_rn, p.rn, s);
+            upload(p.d_rnm1, p.rnm1, s);
+            upload(p.d_blocks, p.L.blocks, s);
+            upload(p.d_snp_begin, p.L.snp_begin, s);
+            const int64_t n_tiles = p.L.ld / kTileK;
+            p.d_col_snp.reserve(static_cast<size_t>(p.L.ld) * 4);
+            p.d_tiles.reserve(std::max<size_t>(static_cast<size_t>(n_tiles) * sizeof(TileInfo), 16));
+            launch_layout_tables(c, p.d_blocks.as<BlockInfo>(), p.d_snp_begin.as<int64_t>(), p.L.n_block, p.L.ld,
+                                 p.d_col_snp.as<int32_t>(), p.d_tiles.as<TileInfo>(), s);
+            bind_operand_planes(p.op, fmt, p.P, p.L.ld, c.ws_batch.as<uint8_t>() + io);
+            io += p.img_bytes;
+            if (p.detect)
+                launch_copy_union_ploidy(c, p.d_sel.as<uint32_t>(), p.d_umap.as<int32_t>(), p.n_sel, d_desc_u.as<uint32_t>(), s);
             CanonDecodeArgs a;
             a.canon = d_canon_u.as<uint64_t>();
-            a.n_tiles = p.n_tiles;
+            a.n_tiles = n_tiles;
             a.n_sel = n_u_pad;
-            a.sel = p.sel.as<uint32_t>();
-            a.pop_off = p.pop_off.as<int32_t>();
+            a.sel = p.d_sel.as<uint32_t>();
+            a.pop_off = p.d_pop_off.as<int32_t>();
             a.P = p.P;
-            a.rec_n = p.rec_n.as<double>();
-            a.rec_nm1 = p.rec_nm1.as<double>();
-            a.col_snp = p.col_snp.as<int32_t>();
+            a.rec_n = p.d_rn.as<double>();
+            a.rec_nm1 = p.d_rnm1.as<double>();
+            a.col_snp = p.d_col_snp.as<int32_t>();
             a.op = p.op;
-            a.umap = umaps[w].as<int32_t>();
-            a.tiles = p.tiles.as<TileInfo>();
+            a.umap = p.d_umap.as<int32_t>();
+            a.tiles = p.d_tiles.as<TileInfo>();
             a.n_utiles = n_utiles;
             a.center_snp = d_center_u.as<double>();
             launch_decode_canon(c, a, s);
-            const stp_f2_output& o = outs[k];
             double* f2 = o.f2;
             double* vp = o.vpair;
             if (!o.on_device) {
                 f2 = reinterpret_cast<double*>(c.ws_f2.as<uint8_t>() + oo);
                 vp = reinterpret_cast<double*>(c.ws_vpair.as<uint8_t>() + oo);
-                oo += out_bytes[wave[w]] / 2;
+                oo += p.out_bytes / 2;
             }
             specs[w].L = &p.L;
             specs[w].info = GroupInfo{static_cast<const uint8_t*>(p.op.planes), f2, vp, p.op.n_ck, p.P, 0};
             if (o.block_sizes) copy_block_sizes(p.L, o.block_sizes);
         }
         std::vector<unsigned long long> stamps;
-        launch_f2_umma_grouped(c, fmt, plans[0]->op.scale_inv, chunk_stages_of(prec), specs, s, &stamps);
+        launch_f2_umma_grouped(c, fmt, mem[wave[0]].op.scale_inv, chunk_stages_of(prec), specs, s, &stamps);
         if (t0 == 0) STPF2_CUDA(cudaMemcpy(&t0, d_t0.ptr, sizeof(t0), cudaMemcpyDeviceToHost));
         for (size_t w = 0; w < wave.size(); ++w) {
-            const int k = idx[wave[w]];
+            BatchMember& p = mem[wave[w]];
             done_ms[wave[w]] = stamps[w] >= t0 ? static_cast<double>(stamps[w] - t0) * 1e-6 : 0.0;
-            const stp_f2_output& o = outs[k];
-            const Plan& p = *plans[w];
+            const stp_f2_output& o = outs[p.k];
             const size_t elems = static_cast<size_t>(p.P) * p.P * p.L.n_block;
             if (!o.on_device && elems) {
                 STPF2_CUDA(cudaMemcpyAsync(o.f2, specs[w].info.f2, elems * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -705,7 +797,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
             }
             if (o.ploidy_out && p.n_sel > 0) {
                 std::vector<uint32_t> sel(static_cast<size_t>(p.n_sel));
-                STPF2_CUDA(cudaMemcpyAsync(sel.data(), p.sel.ptr, sel.size() * 4, cudaMemcpyDeviceToHost, s));
+                STPF2_CUDA(cudaMemcpyAsync(sel.data(), p.d_sel.ptr, sel.size() * 4, cudaMemcpyDeviceToHost, s));
                 STPF2_CUDA(cudaStreamSynchronize(s));
                 for (size_t q = 0; q < sel.size(); ++q) o.ploidy_out[q] = static_cast<int32_t>(sel[q] & 3u);
             }

@@ -116,7 +116,8 @@ struct BlockLayout {
 
 // Validates a contiguous non-decreasing partition (core::block_ranges,
 // src/core/domain/block_partition_rule.hpp:56-96) and builds the padded column map.
-BlockLayout make_block_layout(const int32_t* block_id, int64_t n_snp, int n_block);
+// with_snp_col = false skips the per-SNP column map (only the Q/V/N feeder reads it).
+BlockLayout make_block_layout(const int32_t* block_id, int64_t n_snp, int n_block, bool with_snp_col = true);
 
 // Work item of the contraction: tile pair (ti <= tj) of one block.
 struct WorkItem {
@@ -262,6 +263,10 @@ void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stage
                             cudaStream_t s, std::vector<unsigned long long>* stamps);
 // %globaltimer of the device when the stream reaches this point, written to *dst.
 void launch_timestamp(Ctx& c, unsigned long long* dst, cudaStream_t s);
+// The column -> SNP map (ld entries, -1 for padding) and the 32-column tile table (ld / 32)
+// of a block layout, built on the device from its blocks and their first SNPs.
+void launch_layout_tables(Ctx& c, const BlockInfo* blocks, const int64_t* snp_begin, int n_block, int64_t ld,
+                          int32_t* col_snp, TileInfo* tiles, cudaStream_t s);
 // desc[g] takes the ploidy bits of union sample umap[g] (a batch's shared ploidy pass).
 void launch_copy_union_ploidy(Ctx& c, uint32_t* desc, const int32_t* umap, int64_t n_sel, const uint32_t* desc_u,
                               cudaStream_t s);

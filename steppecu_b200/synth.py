@@ -50,6 +50,9 @@ WORKLOADS = {
     # 1000 pops of lognormal size (1-60), lognormal block sizes (median 1500, 50-6000)
     "c4": Workload("c4", 1000, None, 1_150_000, HUMAN_CM, "beta23", 0.5, (0.01, 0.15),
                    block_sizes_lognormal=True),
+    # The shared panel of the many-requests workload: 8,000 samples (400 pops x 20), 1.15M
+    # SNPs, same sample model as c2; requests come from batch_requests().
+    "c5": Workload("c5", 400, 20, 1_150_000, HUMAN_CM, "beta23", 0.5, (0.01, 0.15)),
 }
 
 
@@ -203,3 +206,24 @@ def write_eigenstrat(panel: Panel, prefix: str | Path) -> None:
     with open(prefix + ".ind", "w") as f:
         for g in range(panel.n_ind):
             f.write(f"I{g} U {panel.pop_labels[panel.ind_pop[g]]}\n")
+
+
+def batch_requests(panel: Panel, n_req: int = 64, seed: int = 20261208, p_min: int = 4, p_max: int = 300,
+                   blgsize: float = 0.05) -> list[dict]:
+    """Independent extraction requests over one panel: each selects P_r populations, P_r
+    log-uniform on [p_min, p_max], a random subset in ascending order, and has its own 5 cM
+    block map (the panel's genetic map scaled by a per-request factor in [0.9, 1.1], i.e. a
+    different recombination map, then the AT2 block walk)."""
+    rng = np.random.default_rng(seed)
+    p_max = min(p_max, panel.n_pop)
+    out = []
+    for _ in range(n_req):
+        P = int(round(math.exp(rng.uniform(math.log(p_min), math.log(p_max)))))
+        P = max(1, min(P, panel.n_pop))
+        pops = np.sort(rng.choice(panel.n_pop, size=P, replace=False)).tolist()
+        sel, po = panel.selection(pops)
+        scale = rng.uniform(0.9, 1.1)
+        bid, nb = assign_blocks(panel.chrom, panel.genpos * scale, blgsize, panel.physpos)
+        out.append({"pops": pops, "sel_rows": sel, "pop_offsets": po, "block_id": np.asarray(bid, np.int32),
+                    "n_block": int(nb)})
+    return out
