@@ -407,26 +407,30 @@ __device__ __forceinline__ void spill_counts(uint32_t* cnt, bool add, uint32_t (
     }
 }
 
-// Columns r .. r+31 of the 64-column stream w0 | w1 (canonical words: column c of a word at
-// byte c/4, bits 7-2(c%4)), 0 <= r < 32: a byte shift, then a 2-bit shift inside each byte
-// taking the top columns from the next byte.
-__device__ __forceinline__ uint64_t window_cols(uint64_t w0, uint64_t w1, int r) {
-    if (r == 0) return w0;
-    const int rb = r >> 2, rs = r & 3;
-    const uint64_t A = rb == 0 ? w0 : (w0 >> (8 * rb)) | (w1 << (64 - 8 * rb));
-    if (rs == 0) return A;
-    const uint64_t B = rb == 7 ? w1 : (w0 >> (8 * rb + 8)) | (w1 << (56 - 8 * rb));
-    const uint64_t mhi = 0x0101010101010101ull * ((0xFFu << (2 * rs)) & 0xFFu);
-    const uint64_t mlo = 0x0101010101010101ull * (0xFFu >> (8 - 2 * rs));
-    return ((A << (2 * rs)) & mhi) | ((B >> (8 - 2 * rs)) & mlo);
-}
-
-// Bits of columns nv .. 31 of a canonical word set (code 3, missing).
-__device__ __forceinline__ uint64_t missing_from(int nv) {
-    if (nv >= 32) return 0;
-    const int kb = nv >> 2, js = nv & 3;
-    uint64_t m = kb + 1 < 8 ? (~0ull << (8 * (kb + 1))) : 0ull;
-    return m | (static_cast<uint64_t>(0xFFu >> (2 * js)) << (8 * kb));
+// Operand terms of 8 columns from their packed counts (ac2 | n << 16) and centres: in FP64
+// (q from the exact counts), rounded once to FP32 for the planes; a2 -> double through the
+// 2^52 trick (an FP64 add, no conversion unit).
+__device__ __forceinline__ Terms8 terms8_from_counts(const uint32_t (&v)[8], const double* cen,
+                                                     const double* __restrict__ rec_n,
+                                                     const double* __restrict__ rec_nm1) {
+    Terms8 tm;
+    tm.mbits = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const uint32_t n = v[c] >> 16, a2 = v[c] & 0xFFFFu;
+        double pt = 0.0, ah = 0.0;
+        if (n > 0) {
+            const double a2d = __hiloint2double(0x43300000, static_cast<int>(a2)) - 4503599627370496.0;
+            const double qf = a2d * 0.5 * __ldg(rec_n + n);
+            const double h = qf * (1.0 - qf) * __ldg(rec_nm1 + n);
+            pt = qf - cen[c];
+            ah = 0.5 * (pt * pt - h);
+            tm.mbits |= 1u << c;
+        }
+        tm.pt[c] = static_cast<float>(pt);
+        tm.ah[c] = static_cast<float>(ah);
+    }
+    return tm;
 }
 
 template <OpFmt F, bool kUnion>
@@ -436,8 +440,8 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
                     const double* __restrict__ center, const double* __restrict__ rec_n,
                     const double* __restrict__ rec_nm1, const int32_t* __restrict__ col_snp, int64_t col_base,
                     OperandPlanes op, int32_t* __restrict__ cnt_ac2, int32_t* __restrict__ cnt_n,
-                    const int32_t* __restrict__ umap, const TileInfo* __restrict__ tiles, int64_t n_utiles,
-                    const double* __restrict__ center_snp) {
+                    const int32_t* __restrict__ umap, const double* __restrict__ center_snp,
+                    uint32_t* __restrict__ cnt_packed, int64_t cnt_ld) {
     extern __shared__ uint32_t s_cnt[];
     __shared__ double s_center[4 * kCenterPitch];
     const int64_t q = blockIdx.x;
@@ -467,31 +471,10 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
             bool spilled = false;
             int it = 0;
             const uint64_t* col = canon + q * n_sel * 4 + sub;
-            // Shared-canonical mode: the union words holding this tile's 32-SNP window.
-            const uint64_t* col0 = nullptr;
-            const uint64_t* col1 = nullptr;
-            int shift = 0;
-            uint64_t miss = ~0ull;
-            if constexpr (kUnion) {
-                const TileInfo ti = tiles[4 * q + sub];
-                if (ti.nvalid > 0) {
-                    const int64_t ut = ti.snp0 >> 5;
-                    shift = ti.snp0 & 31;
-                    miss = missing_from(ti.nvalid);
-                    col0 = canon + (ut >> 2) * n_sel * 4 + (ut & 3);
-                    if (shift != 0 && ut + 1 < n_utiles) col1 = canon + ((ut + 1) >> 2) * n_sel * 4 + ((ut + 1) & 3);
-                }
-            }
+            // Shared-canonical mode: selected sample gg is canonical sample umap[gg].
             auto load = [&](int gg) -> uint64_t {
-                if constexpr (kUnion) {
-                    if (!col0) return ~0ull;  // a padding tile: every column missing
-                    const int64_t uidx = static_cast<int64_t>(__ldg(umap + gg)) * 4;
-                    const uint64_t w0 = __ldg(col0 + uidx);
-                    const uint64_t w1 = shift == 0 ? 0ull : (col1 ? __ldg(col1 + uidx) : ~0ull);
-                    return window_cols(w0, w1, shift) | miss;
-                } else {
-                    return __ldg(col + static_cast<int64_t>(gg) * 4);
-                }
+                if constexpr (kUnion) return __ldg(col + static_cast<int64_t>(__ldg(umap + gg)) * 4);
+                else return __ldg(col + static_cast<int64_t>(gg) * 4);
             };
             int g = g0;
             for (; g + kDecUnroll <= g1; g += kDecUnroll) {
@@ -549,28 +532,18 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
                 }
             }
         }
-        if (!op.planes) continue;
-        Terms8 tm;
-        tm.mbits = 0;
+        if (cnt_packed) {
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const uint32_t v = cnt[c * kCntCol];
-            const uint32_t n = v >> 16, a2 = v & 0xFFFFu;
-            // Terms in FP64 (q from the exact counts), rounded once to FP32 for the planes.
-            // a2 -> double through the 2^52 trick (an FP64 add, no conversion unit).
-            double pt = 0.0, ah = 0.0;
-            if (n > 0) {
-                const double a2d = __hiloint2double(0x43300000, static_cast<int>(a2)) - 4503599627370496.0;
-                const double qf = a2d * 0.5 * __ldg(rec_n + n);
-                const double h = qf * (1.0 - qf) * __ldg(rec_nm1 + n);
-                pt = qf - cen[c];
-                ah = 0.5 * (pt * pt - h);
-                tm.mbits |= 1u << c;
+            for (int c = 0; c < 8; ++c) {
+                const int32_t s = __ldg(col_snp + col0 + c);
+                if (s >= 0) cnt_packed[static_cast<int64_t>(i) * cnt_ld + s] = cnt[c * kCntCol];
             }
-            tm.pt[c] = static_cast<float>(pt);
-            tm.ah[c] = static_cast<float>(ah);
         }
-        emit8<F>(op, i, col_base + col0, tm);
+        if (!op.planes) continue;
+        uint32_t v[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] = cnt[c * kCntCol];
+        emit8<F>(op, i, col_base + col0, terms8_from_counts(v, cen, rec_n, rec_nm1));
     }
 }
 
@@ -713,10 +686,44 @@ void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t
 }
 
 namespace {
+// Operand images of one request from packed per-population counts (pop-major, row u at
+// counts + u * cnt_ld, SNP s at column s): its population i reads row upop[i], its padded
+// column c SNP col_snp[c]. One CTA per (64 populations, quad of 4 column tiles); lane =
+// (population, 8-column chunk), as in the decode's emit phase, with the same terms.
+template <OpFmt F>
+__global__ void __launch_bounds__(kDecThreads2)
+emit_counts_kernel(const uint32_t* __restrict__ counts, int64_t cnt_ld, const int32_t* __restrict__ upop, int P,
+                   int64_t n_tiles, const int32_t* __restrict__ col_snp, const double* __restrict__ center_snp,
+                   const double* __restrict__ rec_n, const double* __restrict__ rec_nm1, OperandPlanes op) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int r = lane & 7, chunk = lane >> 3;
+    const int i = blockIdx.y * kDecPops + warp * 8 + r;
+    if (i >= P) return;
+    const uint32_t* row = counts + static_cast<int64_t>(__ldg(upop + i)) * cnt_ld;
+    const int64_t q = blockIdx.x;
+#pragma unroll 1
+    for (int sub = 0; sub < 4; ++sub) {
+        const int64_t t = 4 * q + sub;
+        if (t >= n_tiles) break;
+        const int64_t col0 = t * kTileCols + 8 * chunk;
+        uint32_t v[8];
+        double cen[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int32_t s = __ldg(col_snp + col0 + c);
+            v[c] = s >= 0 ? __ldg(row + s) : 0u;
+            cen[c] = s >= 0 ? __ldg(center_snp + s) : 0.5;
+        }
+        emit8<F>(op, i, col0, terms8_from_counts(v, cen, rec_n, rec_nm1));
+    }
+}
+}  // namespace
+
+namespace {
 __global__ void copy_union_ploidy_kernel(uint32_t* __restrict__ desc, const int32_t* __restrict__ umap, int64_t n_sel,
                                          const uint32_t* __restrict__ desc_u) {
     const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (g < n_sel) desc[g] = (desc[g] & ~3u) | (desc_u[umap[g]] & 3u);
+    if (g < n_sel && (desc[g] & 3u) == 3u) desc[g] = (desc[g] & ~3u) | (desc_u[umap[g]] & 3u);
 }
 }  // namespace
 
@@ -757,6 +764,20 @@ void launch_layout_tables(Ctx& c, const BlockInfo* blocks, const int64_t* snp_be
     c.launches++;
 }
 
+void launch_emit_counts(Ctx& c, const uint32_t* counts, int64_t cnt_ld, const int32_t* upop, int P, int64_t n_tiles,
+                        const int32_t* col_snp, const double* center_snp, const double* rec_n, const double* rec_nm1,
+                        const OperandPlanes& op, cudaStream_t s) {
+    if (P <= 0 || n_tiles <= 0) return;
+    const dim3 grid(static_cast<unsigned>((n_tiles + 3) / 4), static_cast<unsigned>((P + kDecPops - 1) / kDecPops));
+    switch (op.fmt) {
+        case OpFmt::F32: emit_counts_kernel<OpFmt::F32><<<grid, kDecThreads2, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
+        case OpFmt::BF16: emit_counts_kernel<OpFmt::BF16><<<grid, kDecThreads2, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
+        case OpFmt::F16: emit_counts_kernel<OpFmt::F16><<<grid, kDecThreads2, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
+    }
+    STPF2_CUDA(cudaGetLastError());
+    c.launches++;
+}
+
 void launch_copy_union_ploidy(Ctx& c, uint32_t* desc, const int32_t* umap, int64_t n_sel, const uint32_t* desc_u,
                               cudaStream_t s) {
     if (n_sel <= 0) return;
@@ -769,11 +790,11 @@ void launch_decode_canon(Ctx& c, const CanonDecodeArgs& a, cudaStream_t s) {
     if (a.P <= 0 || a.n_tiles <= 0) return;
     const dim3 grid(static_cast<unsigned>((a.n_tiles + 3) / 4), static_cast<unsigned>((a.P + kDecPops - 1) / kDecPops));
 #define STPF2_DECODE_ARGS a.canon, a.n_tiles, a.n_sel, a.sel, a.pop_off, a.P, a.center, a.rec_n, a.rec_nm1, a.col_snp, \
-                          a.col_base, a.op, a.cnt_ac2, a.cnt_n, a.umap, a.tiles, a.n_utiles, a.center_snp
+                          a.col_base, a.op, a.cnt_ac2, a.cnt_n, a.umap, a.center_snp, a.cnt_packed, a.cnt_ld
 #define STPF2_DECODE_LAUNCH(F)                                                                      \
     (a.umap ? decode_canon_kernel<F, true><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS) \
             : decode_canon_kernel<F, false><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS))
-    if (a.umap && (!a.tiles || !a.center_snp)) fail(STP_INVALID_ARGUMENT, "shared-canonical decode needs tiles and centres");
+    if (a.umap && !a.center_snp) fail(STP_INVALID_ARGUMENT, "shared-canonical decode needs per-SNP centres");
     switch (a.op.fmt) {
         case OpFmt::F32: STPF2_DECODE_LAUNCH(OpFmt::F32); break;
         case OpFmt::BF16: STPF2_DECODE_LAUNCH(OpFmt::BF16); break;

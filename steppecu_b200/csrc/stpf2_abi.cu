@@ -14,6 +14,7 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <new>
 #include <string>
@@ -529,25 +530,25 @@ bool same_panel(const stp_geno_view& a, const stp_geno_view& b) {
 }
 
 // One request of a grouped batch: what the host prepares (in parallel with the others)
-// and the device tables it uploads.
+// and the device tables it uploads. A population is identified by its samples and their
+// ploidy (key: sorted row * 4 + ploidy code, code 3 = detect), so requests that select the
+// same population share its decoded counts.
 struct BatchMember {
     int k = 0;  // index of the request
     int P = 0;
     int64_t n_sel = 0;
-    bool detect = false;
     BlockLayout L;
-    std::vector<uint32_t> sel;
-    std::vector<int32_t> pop_off, umap;
-    std::vector<double> rn, rnm1;
+    std::vector<std::vector<int64_t>> keys;  // per population
+    std::vector<int32_t> plcode;             // per selected sample: 0/1/2, or 3 = detect
+    std::vector<int32_t> upop;               // population -> batch population
     size_t img_bytes = 0, out_bytes = 0;
-    DevBuf d_sel, d_pop_off, d_umap, d_rn, d_rnm1, d_blocks, d_snp_begin, d_col_snp, d_tiles;
+    DevBuf d_upop, d_blocks, d_snp_begin, d_col_snp, d_tiles;
     OperandPlanes op;
 };
 
-// Validates request r (the same rules as build_plan) and fills m's host tables. Host only,
+// Validates request r (the rules of build_plan) and fills m's host tables. Host only,
 // safe to run for several members at once.
-void prepare_member(const stp_f2_request& r, const stp_f2_output& o, const std::vector<int32_t>& pos_u, OpFmt fmt,
-                    BatchMember& m) {
+void prepare_member(const stp_f2_request& r, const stp_f2_output& o, int64_t n_ind, OpFmt fmt, BatchMember& m) {
     need(r.n_pop > 0 && r.n_block > 0, "empty request in a batch");
     need(r.pop_offsets != nullptr, "pop_offsets is NULL");
     need(r.pop_offsets[0] == 0, "pop_offsets[0] must be 0");
@@ -559,36 +560,30 @@ void prepare_member(const stp_f2_request& r, const stp_f2_output& o, const std::
     m.P = r.n_pop;
     m.n_sel = n_sel;
     const bool auto_ploidy = r.sample_ploidy == nullptr && r.ploidy_mode == STP_PLOIDY_AUTO;
-    m.detect = auto_ploidy;
-    m.sel.resize(static_cast<size_t>(n_sel));
-    m.umap.resize(static_cast<size_t>(n_sel));
-    std::vector<char> seen(pos_u.size(), 0);
+    m.plcode.resize(static_cast<size_t>(n_sel));
+    std::vector<char> seen(static_cast<size_t>(n_ind), 0);
     for (int64_t g = 0; g < n_sel; ++g) {
         const int64_t row = r.sel_rows[g];
-        need(row >= 0 && row < static_cast<int64_t>(pos_u.size()), "sel_rows entry outside [0, n_ind)");
+        need(row >= 0 && row < n_ind, "sel_rows entry outside [0, n_ind)");
         need(static_cast<uint64_t>(row / 4) < r.geno.bytes_per_record, "sel_rows entry beyond the record");
         need(!seen[static_cast<size_t>(row)], "a sample is selected more than once");
         seen[static_cast<size_t>(row)] = 1;
-        int pl = 0;
+        int pl = 3;
         if (r.sample_ploidy) pl = r.sample_ploidy[g];
         else if (r.ploidy_mode == STP_PLOIDY_PSEUDO) pl = 1;
         else if (r.ploidy_mode == STP_PLOIDY_DIPLOID) pl = 2;
         else need(auto_ploidy, "unknown ploidy_mode");
-        if (pl != 1 && pl != 2) pl = 0;  // a bad ploidy contributes nothing (decode_af.hpp:58-65)
-        m.sel[g] = pack_sel(row, pl);
-        m.umap[g] = pos_u[static_cast<size_t>(row)];
+        if (!auto_ploidy && pl != 1 && pl != 2) pl = 0;  // a bad ploidy contributes nothing (decode_af.hpp:58-65)
+        m.plcode[g] = pl;
     }
-    m.pop_off.assign(static_cast<size_t>(r.n_pop) + 1, 0);
-    int64_t max_pop = 0;
-    for (int i = 0; i <= r.n_pop; ++i) m.pop_off[i] = static_cast<int32_t>(r.pop_offsets[i]);
-    for (int i = 0; i < r.n_pop; ++i) max_pop = std::max<int64_t>(max_pop, r.pop_offsets[i + 1] - r.pop_offsets[i]);
-    need(max_pop <= 16383, "a population has more than 16383 samples");
-    const int64_t n_max = 2 * max_pop + 1;
-    m.rn.assign(static_cast<size_t>(n_max) + 1, 0.0);
-    m.rnm1.assign(static_cast<size_t>(n_max) + 1, 1.0);
-    for (int64_t n = 1; n <= n_max; ++n) {
-        m.rn[n] = 1.0 / static_cast<double>(n);
-        m.rnm1[n] = 1.0 / std::max(static_cast<double>(n) - 1.0, 1.0);
+    m.keys.resize(static_cast<size_t>(r.n_pop));
+    for (int i = 0; i < r.n_pop; ++i) {
+        const int64_t g0 = r.pop_offsets[i], g1 = r.pop_offsets[i + 1];
+        need(g1 - g0 <= 16383, "a population has more than 16383 samples");
+        auto& key = m.keys[i];
+        key.reserve(static_cast<size_t>(g1 - g0));
+        for (int64_t g = g0; g < g1; ++g) key.push_back(r.sel_rows[g] * 4 + m.plcode[g]);
+        std::sort(key.begin(), key.end());
     }
     m.L = make_block_layout(r.block_id, r.geno.n_snp, r.n_block, false);
     m.img_bytes = align256(operand_plane_bytes(fmt, r.n_pop, m.L.ld));
@@ -616,17 +611,20 @@ void parallel_for(int n, F&& f) {
         if (e) std::rethrow_exception(e);
 }
 
-// A batch of requests over one panel, all on the tensor cores with one arithmetic: the
-// union of their samples goes through one ploidy pass and one transpose into canonical
-// genotypes in contiguous SNP tiles; each request's decode reads its samples and its
-// blocks' 32-SNP windows from that copy into its own operand images; and one persistent
-// launch contracts every request's (block, tile pair) items. The requests' host tables are
-// prepared in parallel while the device runs the shared passes; their column and tile maps
-// are built on the device. Requests whose images do not fit in free device memory together
-// run in consecutive waves of the same form. The images are not cleared: the decode writes
-// every column of rows < P, and rows >= P of a request's last row tile only reach
-// accumulator rows that are never stored. done_ms[m] receives request idx[m]'s completion
-// time from the start of the group.
+// A batch of requests over one panel, all on the tensor cores with one arithmetic:
+//   1. the union of their samples goes through one ploidy pass and one transpose into
+//      canonical genotypes in contiguous SNP tiles;
+//   2. every distinct population of the batch is decoded once from that copy into packed
+//      exact counts (ac2 | n << 16, population-major);
+//   3. each request's operand images are emitted from its populations' counts through its
+//      own block layout (column and tile maps built on the device), with the arithmetic of
+//      the one-request decode, so results are bit-identical to it;
+//   4. one persistent launch contracts every request's (block, tile pair) items.
+// The requests' host tables are prepared in parallel while the device runs steps 1-2.
+// Requests whose images do not fit in free device memory together run in consecutive
+// waves of steps 3-4. The images are not cleared: step 3 writes every column of rows < P,
+// and rows >= P of a request's last row tile only reach accumulator rows that are never
+// stored. done_ms[m] receives request idx[m]'s completion time from the start of the group.
 void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* outs, const std::vector<int>& idx,
                            std::vector<double>& done_ms) {
     cudaStream_t s = c.stream;
@@ -635,6 +633,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
     need(g.records != nullptr, "records is NULL");
     need(n_ind > 0, "n_ind must be positive");
     need(g.bytes_per_record > 0, "bytes_per_record is 0");
+    need(M < INT_MAX, "too many SNPs");
     uint64_t pitch = g.pitch ? g.pitch : g.bytes_per_record;
     need(pitch >= g.bytes_per_record, "pitch < bytes_per_record");
     const int prec = reqs[idx[0]].precision;
@@ -683,18 +682,23 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
     const int64_t n_u = static_cast<int64_t>(desc_u.size());
     const int64_t n_u_pad = (n_u + 3) / 4 * 4;
     const int64_t n_utiles = (M + kTileK - 1) / kTileK;
-    std::vector<TileInfo> tiles_u(static_cast<size_t>(n_utiles));
-    for (int64_t t = 0; t < n_utiles; ++t)
-        tiles_u[t] = TileInfo{static_cast<int32_t>(t * kTileK), static_cast<int32_t>(std::min<int64_t>(kTileK, M - t * kTileK))};
-    DevBuf d_pos_u, d_desc_u, d_tiles_u, d_canon_u, d_center_u, d_t0;
+    // The contiguous SNP layout of the shared copy: one block of every SNP.
+    std::vector<BlockInfo> one_block{BlockInfo{0, static_cast<int32_t>(M), 0}};
+    std::vector<int64_t> zero{0};
+    DevBuf d_pos_u, d_desc_u, d_tiles_u, d_cols_u, d_one, d_zero, d_canon_u, d_center_u, d_t0;
     upload(d_pos_u, pos_u, s);
     upload(d_desc_u, desc_u, s);
-    upload(d_tiles_u, tiles_u, s);
+    upload(d_one, one_block, s);
+    upload(d_zero, zero, s);
+    d_tiles_u.reserve(std::max<size_t>(static_cast<size_t>(n_utiles) * sizeof(TileInfo), 16));
+    d_cols_u.reserve(std::max<size_t>(static_cast<size_t>(n_utiles) * kTileK * 4, 16));
     d_canon_u.reserve(std::max<size_t>(static_cast<size_t>((n_utiles + 3) / 4) * n_u_pad * 32, 64));
     d_center_u.reserve(std::max<size_t>(static_cast<size_t>(n_utiles) * kTileK * 8, 64));
     d_t0.reserve(16);
 
     launch_timestamp(c, d_t0.as<unsigned long long>(), s);
+    launch_layout_tables(c, d_one.as<BlockInfo>(), d_zero.as<int64_t>(), 1, n_utiles * kTileK, d_cols_u.as<int32_t>(),
+                         d_tiles_u.as<TileInfo>(), s);
     if (any_auto) launch_detect_ploidy_pa(c, d_rec, pitch, M, d_desc_u.as<uint32_t>(), n_u, s);
     launch_transpose_pa(c, d_rec, pitch, n_ind, d_tiles_u.as<TileInfo>(), n_utiles, d_pos_u.as<int32_t>(), n_u_pad,
                         d_canon_u.as<uint64_t>(), d_center_u.as<double>(), s);
@@ -703,10 +707,70 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
     std::vector<BatchMember> mem(idx.size());
     parallel_for(static_cast<int>(idx.size()), [&](int m) {
         mem[m].k = idx[m];
-        prepare_member(reqs[idx[m]], outs[idx[m]], pos_u, fmt, mem[m]);
+        prepare_member(reqs[idx[m]], outs[idx[m]], n_ind, fmt, mem[m]);
     });
 
+    // The batch's distinct populations, decoded once into packed counts.
+    std::map<std::vector<int64_t>, int32_t> pop_index;
+    std::vector<const std::vector<int64_t>*> pops;
+    for (BatchMember& m : mem) {
+        m.upop.resize(static_cast<size_t>(m.P));
+        for (int i = 0; i < m.P; ++i) {
+            auto it = pop_index.emplace(m.keys[i], static_cast<int32_t>(pops.size()));
+            if (it.second) pops.push_back(&it.first->first);
+            m.upop[i] = it.first->second;
+        }
+    }
+    const int UP = static_cast<int>(pops.size());
+    std::vector<uint32_t> sel_up;
+    std::vector<int32_t> umap_up, off_up{0};
+    int64_t max_pop = 0;
+    for (const auto* key : pops) {
+        for (int64_t e : *key) {
+            sel_up.push_back(pack_sel(e >> 2, static_cast<int>(e & 3)));
+            umap_up.push_back(pos_u[static_cast<size_t>(e >> 2)]);
+        }
+        off_up.push_back(static_cast<int32_t>(sel_up.size()));
+        max_pop = std::max<int64_t>(max_pop, static_cast<int64_t>(key->size()));
+    }
+    const int64_t n_max = 2 * max_pop + 1;
+    std::vector<double> rn(static_cast<size_t>(n_max) + 1, 0.0), rnm1(static_cast<size_t>(n_max) + 1, 1.0);
+    for (int64_t n = 1; n <= n_max; ++n) {
+        rn[n] = 1.0 / static_cast<double>(n);
+        rnm1[n] = 1.0 / std::max(static_cast<double>(n) - 1.0, 1.0);
+    }
+    DevBuf d_sel_up, d_umap_up, d_off_up, d_rn, d_rnm1, d_counts;
+    upload(d_sel_up, sel_up, s);
+    upload(d_umap_up, umap_up, s);
+    upload(d_off_up, off_up, s);
+    upload(d_rn, rn, s);
+    upload(d_rnm1, rnm1, s);
+    d_counts.reserve(std::max<size_t>(static_cast<size_t>(UP) * static_cast<size_t>(M) * 4, 16));
+    if (any_auto)
+        launch_copy_union_ploidy(c, d_sel_up.as<uint32_t>(), d_umap_up.as<int32_t>(), static_cast<int64_t>(sel_up.size()),
+                                 d_desc_u.as<uint32_t>(), s);
+    {
+        CanonDecodeArgs a;
+        a.canon = d_canon_u.as<uint64_t>();
+        a.n_tiles = n_utiles;
+        a.n_sel = n_u_pad;
+        a.sel = d_sel_up.as<uint32_t>();
+        a.pop_off = d_off_up.as<int32_t>();
+        a.P = UP;
+        a.rec_n = d_rn.as<double>();
+        a.rec_nm1 = d_rnm1.as<double>();
+        a.col_snp = d_cols_u.as<int32_t>();
+        a.op.fmt = fmt;
+        a.op.planes = nullptr;  // counts only
+        a.umap = d_umap_up.as<int32_t>();
+        a.center_snp = d_center_u.as<double>();
+        a.cnt_packed = d_counts.as<uint32_t>();
+        a.cnt_ld = M;
+        launch_decode_canon(c, a, s);
+    }
+
     // Waves of requests whose operand images (and device-side outputs) fit together.
+    STPF2_CUDA(cudaStreamSynchronize(s));
     size_t free_b = 0, total_b = 0;
     STPF2_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t held = c.ws_batch.bytes + c.ws_f2.bytes + c.ws_vpair.bytes;
@@ -723,6 +787,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
         waves.back().push_back(m);
         acc += b;
     }
+    std::vector<uint32_t> desc_h;  // detected ploidy of the union samples, for ploidy_out
     unsigned long long t0 = 0;
     for (const auto& wave : waves) {
         size_t img_total = 0, out_total = 0;
@@ -740,11 +805,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
         for (size_t w = 0; w < wave.size(); ++w) {
             BatchMember& p = mem[wave[w]];
             const stp_f2_output& o = outs[p.k];
-            upload(p.d_sel, p.sel, s);
-            upload(p.d_pop_off, p.pop_off, s);
-            upload(p.d_umap, p.umap, s);
-            upload(p.d_rn, p.rn, s);
-            upload(p.d_rnm1, p.rnm1, s);
+            upload(p.d_upop, p.upop, s);
             upload(p.d_blocks, p.L.blocks, s);
             upload(p.d_snp_begin, p.L.snp_begin, s);
             const int64_t n_tiles = p.L.ld / kTileK;
@@ -754,24 +815,9 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
                                  p.d_col_snp.as<int32_t>(), p.d_tiles.as<TileInfo>(), s);
             bind_operand_planes(p.op, fmt, p.P, p.L.ld, c.ws_batch.as<uint8_t>() + io);
             io += p.img_bytes;
-            if (p.detect)
-                launch_copy_union_ploidy(c, p.d_sel.as<uint32_t>(), p.d_umap.as<int32_t>(), p.n_sel, d_desc_u.as<uint32_t>(), s);
-            CanonDecodeArgs a;
-            a.canon = d_canon_u.as<uint64_t>();
-            a.n_tiles = n_tiles;
-            a.n_sel = n_u_pad;
-            a.sel = p.d_sel.as<uint32_t>();
-            a.pop_off = p.d_pop_off.as<int32_t>();
-            a.P = p.P;
-            a.rec_n = p.d_rn.as<double>();
-            a.rec_nm1 = p.d_rnm1.as<double>();
-            a.col_snp = p.d_col_snp.as<int32_t>();
-            a.op = p.op;
-            a.umap = p.d_umap.as<int32_t>();
-            a.tiles = p.d_tiles.as<TileInfo>();
-            a.n_utiles = n_utiles;
-            a.center_snp = d_center_u.as<double>();
-            launch_decode_canon(c, a, s);
+            launch_emit_counts(c, d_counts.as<uint32_t>(), M, p.d_upop.as<int32_t>(), p.P, n_tiles,
+                               p.d_col_snp.as<int32_t>(), d_center_u.as<double>(), d_rn.as<double>(),
+                               d_rnm1.as<double>(), p.op, s);
             double* f2 = o.f2;
             double* vp = o.vpair;
             if (!o.on_device) {
@@ -796,10 +842,16 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
                 STPF2_CUDA(cudaMemcpyAsync(o.vpair, specs[w].info.vpair, elems * sizeof(double), cudaMemcpyDeviceToHost, s));
             }
             if (o.ploidy_out && p.n_sel > 0) {
-                std::vector<uint32_t> sel(static_cast<size_t>(p.n_sel));
-                STPF2_CUDA(cudaMemcpyAsync(sel.data(), p.d_sel.ptr, sel.size() * 4, cudaMemcpyDeviceToHost, s));
-                STPF2_CUDA(cudaStreamSynchronize(s));
-                for (size_t q = 0; q < sel.size(); ++q) o.ploidy_out[q] = static_cast<int32_t>(sel[q] & 3u);
+                if (desc_h.empty()) {
+                    desc_h.resize(desc_u.size());
+                    STPF2_CUDA(cudaMemcpyAsync(desc_h.data(), d_desc_u.ptr, desc_h.size() * 4, cudaMemcpyDeviceToHost, s));
+                    STPF2_CUDA(cudaStreamSynchronize(s));
+                }
+                const stp_f2_request& r = reqs[p.k];
+                for (int64_t q = 0; q < p.n_sel; ++q)
+                    o.ploidy_out[q] = p.plcode[q] == 3
+                                          ? static_cast<int32_t>(desc_h[static_cast<size_t>(pos_u[static_cast<size_t>(r.sel_rows[q])])] & 3u)
+                                          : p.plcode[q];
             }
         }
         STPF2_CUDA(cudaStreamSynchronize(s));

@@ -218,17 +218,16 @@ struct CanonDecodeArgs {
     OperandPlanes op;                  // planes == nullptr: counts only
     int32_t* cnt_ac2 = nullptr;        // optional [P x n_snp] column-major counts
     int32_t* cnt_n = nullptr;
-    // Shared-canonical mode (umap != nullptr), for a batch of requests over one panel:
-    // canon holds the union of every request's samples in contiguous SNP tiles (tile u =
-    // SNPs 32u .. 32u+31, n_sel = the union's padded count, n_utiles tiles). Sample g of
-    // this request is union sample umap[g]; the request's own tile t reads the 32-SNP
-    // window starting at tiles[t].snp0 (two union words, shifted) with columns from
-    // tiles[t].nvalid on read as missing; centres come per SNP from center_snp through
-    // col_snp (center unused).
+    // Shared-canonical mode (umap != nullptr), for a batch over one panel: canon holds a
+    // set of canonical samples (n_sel = its padded count) in the same tiles as this
+    // decode, and selected sample g is canonical sample umap[g]; centres come per SNP from
+    // center_snp through col_snp (center unused).
     const int32_t* umap = nullptr;
-    const TileInfo* tiles = nullptr;
-    int64_t n_utiles = 0;
     const double* center_snp = nullptr;
+    // Optional packed counts (ac2 | n << 16), population-major: population i, SNP s at
+    // cnt_packed[i * cnt_ld + s].
+    uint32_t* cnt_packed = nullptr;
+    int64_t cnt_ld = 0;
 };
 
 void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_snp,
@@ -267,7 +266,13 @@ void launch_timestamp(Ctx& c, unsigned long long* dst, cudaStream_t s);
 // of a block layout, built on the device from its blocks and their first SNPs.
 void launch_layout_tables(Ctx& c, const BlockInfo* blocks, const int64_t* snp_begin, int n_block, int64_t ld,
                           int32_t* col_snp, TileInfo* tiles, cudaStream_t s);
-// desc[g] takes the ploidy bits of union sample umap[g] (a batch's shared ploidy pass).
+// Operand images of one request (P populations, n_tiles padded tiles) from packed
+// per-population counts: population i reads counts row upop[i], column c SNP col_snp[c].
+void launch_emit_counts(Ctx& c, const uint32_t* counts, int64_t cnt_ld, const int32_t* upop, int P, int64_t n_tiles,
+                        const int32_t* col_snp, const double* center_snp, const double* rec_n, const double* rec_nm1,
+                        const OperandPlanes& op, cudaStream_t s);
+// Entries of desc marked 3 (ploidy to be detected) take the ploidy bits of union sample
+// umap[g] (a batch's shared ploidy pass).
 void launch_copy_union_ploidy(Ctx& c, uint32_t* desc, const int32_t* umap, int64_t n_sel, const uint32_t* desc_u,
                               cudaStream_t s);
 
