@@ -215,7 +215,7 @@ def run_e2e(args, ctx, rec, panel, sel, po, bpr, n_out, barrier, dist, dev, P, M
     return e2e
 
 
-def run_batched(dev: str, steps: int = 3, n_req: int = 64) -> dict:
+def run_batched(dev: str, steps: int = 3, n_req: int = 64, serial_baselines: bool = True) -> dict:
     """Many requests over one shared panel (8,000 samples x 1.15M SNPs, 64 requests of
     4-300 populations, each with its own 5 cM block map): one grouped stp_f2_extract_batch
     call against the same requests extracted one after another (plain FP32 SIMT and
@@ -242,7 +242,32 @@ def run_batched(dev: str, steps: int = 3, n_req: int = 64) -> dict:
     for q, P in zip(reqs, Ps):
         n = P * P * q["n_block"]
         outs.append((torch.empty(n, dtype=torch.float64, device=dev), torch.empty(n, dtype=torch.float64, device=dev)))
-    ctx = sb.Context(int(dev.split(":")[1]) if ":" in dev else 0)
+    ordinal = int(dev.split(":")[1]) if ":" in dev else 0
+
+    def serial(ctx, precision: str):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        comp = []
+        for q, (f2, vp) in zip(reqs, outs):
+            ctx.extract_blocks(rec, panel.n_ind, q["sel_rows"], q["pop_offsets"], q["block_id"], q["n_block"],
+                               precision=precision, out=(f2, vp))
+            comp.append((time.perf_counter() - t0) * 1e3)
+        return comp
+
+    # Serial baselines first, each on a fresh context (no workspace of another form held).
+    ser_f32 = ser_f16 = ref = None
+    if serial_baselines:
+        ctx = sb.Context(ordinal)
+        serial(ctx, "fp32")  # warm-up
+        ser_f32 = serial(ctx, "fp32")
+        ctx.close()
+        ctx = sb.Context(ordinal)
+        serial(ctx, "split_f16")  # warm-up
+        ser_f16 = serial(ctx, "split_f16")
+        ref = [(f2.clone(), vp.clone()) for f2, vp in outs]
+        ctx.close()
+
+    ctx = sb.Context(ordinal)
 
     def grouped():
         torch.cuda.synchronize()
@@ -255,23 +280,7 @@ def run_batched(dev: str, steps: int = 3, n_req: int = 64) -> dict:
     wall = [grouped() for _ in range(steps)]
     launches = (ctx.launches - l0) / steps
     done = ctx.last_batch_times(len(reqs))
-    ref = [(f2.clone(), vp.clone()) for f2, vp in outs]
-
-    def serial(precision: str):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        comp = []
-        for q, (f2, vp) in zip(reqs, outs):
-            ctx.extract_blocks(rec, panel.n_ind, q["sel_rows"], q["pop_offsets"], q["block_id"], q["n_block"],
-                               precision=precision, out=(f2, vp))
-            comp.append((time.perf_counter() - t0) * 1e3)
-        return comp
-
-    serial("split_f16")  # warm-up
-    ser_f16 = serial("split_f16")
-    same = all(torch.equal(a, c) and torch.equal(b, d) for (a, b), (c, d) in zip(ref, outs))
-    serial("fp32")
-    ser_f32 = serial("fp32")
+    same = None if ref is None else all(torch.equal(a, c) and torch.equal(b, d) for (a, b), (c, d) in zip(ref, outs))
     ctx.close()
     med = float(np.median(wall))
 
@@ -283,13 +292,16 @@ def run_batched(dev: str, steps: int = 3, n_req: int = 64) -> dict:
         "requests": len(reqs), "populations_per_request": {"min": min(Ps), "max": max(Ps), "sum_sq": int(sum(P * P for P in Ps))},
         "units": total_units,
         "grouped": {"value": total_units / med, "unit": UNIT, "ms_per_call": med * 1e3, "calls": steps,
-                    "device_span_ms": float(np.nanmax(done)), "completion_ms_p50": pct(done, 50),
-                    "completion_ms_p99": pct(done, 99), "gpu_launches": launches,
-                    "equals_serial_split_f16": bool(same)},
-        "serial_split_f16": {"value": total_units / (ser_f16[-1] / 1e3), "ms_total": ser_f16[-1],
-                             "completion_ms_p50": pct(ser_f16, 50), "completion_ms_p99": pct(ser_f16, 99)},
-        "serial_fp32": {"value": total_units / (ser_f32[-1] / 1e3), "ms_total": ser_f32[-1],
-                        "completion_ms_p50": pct(ser_f32, 50), "completion_ms_p99": pct(ser_f32, 99)},
+                    "device_span_ms": float(np.nanmax(done)),
+                    "device_value": total_units / (float(np.nanmax(done)) / 1e3),
+                    "completion_ms_p50": pct(done, 50), "completion_ms_p99": pct(done, 99), "gpu_launches": launches,
+                    "equals_serial_split_f16": same},
+        "serial_split_f16": None if ser_f16 is None else {
+            "value": total_units / (ser_f16[-1] / 1e3), "ms_total": ser_f16[-1],
+            "completion_ms_p50": pct(ser_f16, 50), "completion_ms_p99": pct(ser_f16, 99)},
+        "serial_fp32": None if ser_f32 is None else {
+            "value": total_units / (ser_f32[-1] / 1e3), "ms_total": ser_f32[-1],
+            "completion_ms_p50": pct(ser_f32, 50), "completion_ms_p99": pct(ser_f32, 99)},
         "timing": "host wall clock around each synchronous call; completion of grouped requests from device stamps",
     }
 
@@ -300,7 +312,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c5: only the many-requests measurement (grouped batch vs serial)")
     ap.add_argument("--precision", default="split_f16")
     ap.add_argument("--also", default="split_bf16,split_f16_fine",
                     help="other tensor-core arithmetics timed beside the headline (comma-separated, or none)")
@@ -342,6 +355,19 @@ def main():
             dist.barrier()
 
     dev = f"cuda:{local}"
+    if args.workload == "c5":
+        b = run_batched(dev, steps=args.steps, serial_baselines=not args.quick)
+        if rank == 0:
+            print(json.dumps({
+                "metric": METRIC, "value": b["grouped"]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": 1, "ms_per_step": b["grouped"]["ms_per_call"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f16x3", "data": "synthetic",
+                "config": {"workload": "c5", "requests": b["requests"], "samples": 8000, "snps": 1150000,
+                           "precision": "split_f16", "parallelism": "1 GPU"},
+                "gpu_launches": b["grouped"]["gpu_launches"], "batched_requests": b}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     panel = make_panel(args.workload, rank, dev, n_snp=args.snps)
     sel, po = panel.selection()
     P, M, B = panel.n_pop, panel.n_snp, panel.n_block

@@ -27,6 +27,7 @@
 // MMAs finish, frees TMEM and returns.
 #include <algorithm>
 #include <climits>
+#include <cstring>
 #include <memory>
 #include <vector>
 
@@ -796,24 +797,29 @@ void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stage
     if (items.size() > static_cast<size_t>(INT_MAX)) fail(STP_RUNTIME_ERROR, "too many work items in one batch");
     std::vector<double> rcp(static_cast<size_t>(max_k) + 1, 0.0);
     for (int k = 1; k <= max_k; ++k) rcp[k] = 1.0 / static_cast<double>(k);
-    DevBuf d_items, d_blocks, d_info, d_rcp, d_nitems, d_done, d_ns, d_err, d_counter;
-    auto up = [&](DevBuf& b, const void* h, size_t n) {
-        b.reserve(std::max<size_t>(n, 16));
-        STPF2_CUDA(cudaMemcpyAsync(b.ptr, h, n, cudaMemcpyHostToDevice, s));
-    };
-    up(d_items, items.data(), items.size() * sizeof(WorkItem));
-    up(d_blocks, blocks.data(), blocks.size() * sizeof(BlockInfo));
-    up(d_info, info.data(), info.size() * sizeof(GroupInfo));
-    up(d_rcp, rcp.data(), rcp.size() * sizeof(double));
-    up(d_nitems, n_items.data(), n_items.size() * sizeof(int));
-    d_done.reserve(std::max<size_t>(static_cast<size_t>(G) * sizeof(int), 16));
-    d_ns.reserve(std::max<size_t>(static_cast<size_t>(G) * sizeof(unsigned long long), 16));
-    d_err.reserve(16);
-    d_counter.reserve(16);
-    STPF2_CUDA(cudaMemsetAsync(d_done.ptr, 0, d_done.bytes, s));
-    STPF2_CUDA(cudaMemsetAsync(d_ns.ptr, 0, d_ns.bytes, s));
-    STPF2_CUDA(cudaMemsetAsync(d_err.ptr, 0, 16, s));
-    STPF2_CUDA(cudaMemsetAsync(d_counter.ptr, 0, 16, s));
+    // Every table in one pinned staging buffer and one upload; counters cleared on device.
+    Packing pk;
+    const size_t o_items = pk.add(items.size() * sizeof(WorkItem));
+    const size_t o_blocks = pk.add(blocks.size() * sizeof(BlockInfo));
+    const size_t o_info = pk.add(info.size() * sizeof(GroupInfo));
+    const size_t o_rcp = pk.add(rcp.size() * sizeof(double));
+    const size_t o_nitems = pk.add(n_items.size() * sizeof(int));
+    const size_t staged = pk.end;
+    const size_t o_done = pk.add(static_cast<size_t>(G) * sizeof(int));
+    const size_t o_ns = pk.add(static_cast<size_t>(G) * sizeof(unsigned long long));
+    const size_t o_err = pk.add(16);
+    const size_t o_counter = pk.add(16);
+    c.pin_items.reserve(staged);
+    c.ws_items.reserve(pk.end);
+    uint8_t* h = c.pin_items.as<uint8_t>();
+    std::memcpy(h + o_items, items.data(), items.size() * sizeof(WorkItem));
+    std::memcpy(h + o_blocks, blocks.data(), blocks.size() * sizeof(BlockInfo));
+    std::memcpy(h + o_info, info.data(), info.size() * sizeof(GroupInfo));
+    std::memcpy(h + o_rcp, rcp.data(), rcp.size() * sizeof(double));
+    std::memcpy(h + o_nitems, n_items.data(), n_items.size() * sizeof(int));
+    uint8_t* d = c.ws_items.as<uint8_t>();
+    STPF2_CUDA(cudaMemcpyAsync(d, h, staged, cudaMemcpyHostToDevice, s));
+    STPF2_CUDA(cudaMemsetAsync(d + staged, 0, pk.end - staged, s));
     set_umma_smem();
 
     UmmaArgs a{};
@@ -822,30 +828,30 @@ void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stage
     a.P = info[ord[0]].P;
     a.f2 = info[ord[0]].f2;
     a.vpair = info[ord[0]].vpair;
-    a.items = d_items.as<WorkItem>();
+    a.items = reinterpret_cast<const WorkItem*>(d + o_items);
     a.n_items = static_cast<int>(items.size());
-    a.next_item = d_counter.as<int>();
-    a.blocks = d_blocks.as<BlockInfo>();
+    a.next_item = reinterpret_cast<int*>(d + o_counter);
+    a.blocks = reinterpret_cast<const BlockInfo*>(d + o_blocks);
     a.num_scale = 2.0 * scale_inv;
-    a.rcp = d_rcp.as<double>();
+    a.rcp = reinterpret_cast<const double*>(d + o_rcp);
     a.rcp_max = max_k;
-    a.err = d_err.as<int>();
+    a.err = reinterpret_cast<int*>(d + o_err);
     const bool bf16 = fmt == OpFmt::BF16;
     a.idesc_pp = idesc_f16(bf16, true);
     a.idesc_am = idesc_f16(bf16, false);
     a.idesc_i8 = idesc_u8_s32();
-    a.groups = d_info.as<GroupInfo>();
-    a.grp_done = d_done.as<int>();
-    a.grp_ns = d_ns.as<unsigned long long>();
-    a.grp_items = d_nitems.as<int>();
+    a.groups = reinterpret_cast<const GroupInfo*>(d + o_info);
+    a.grp_done = reinterpret_cast<int*>(d + o_done);
+    a.grp_ns = reinterpret_cast<unsigned long long*>(d + o_ns);
+    a.grp_items = reinterpret_cast<const int*>(d + o_nitems);
     const int grid = std::min(c.sm_count, a.n_items);
     launch_kernel(chunk_stages, true, grid, a, s);
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
     int err = 0;
-    STPF2_CUDA(cudaMemcpyAsync(&err, d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    STPF2_CUDA(cudaMemcpyAsync(&err, d + o_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (stamps)
-        STPF2_CUDA(cudaMemcpyAsync(stamps->data(), d_ns.ptr, static_cast<size_t>(G) * sizeof(unsigned long long),
+        STPF2_CUDA(cudaMemcpyAsync(stamps->data(), d + o_ns, static_cast<size_t>(G) * sizeof(unsigned long long),
                                    cudaMemcpyDeviceToHost, s));
     STPF2_CUDA(cudaStreamSynchronize(s));
     if (err) fail(STP_DEVICE_TIMEOUT, "grouped tensor-core contraction: a bounded device wait expired; results are invalid");

@@ -542,7 +542,6 @@ struct BatchMember {
     std::vector<int32_t> plcode;             // per selected sample: 0/1/2, or 3 = detect
     std::vector<int32_t> upop;               // population -> batch population
     size_t img_bytes = 0, out_bytes = 0;
-    DevBuf d_upop, d_blocks, d_snp_begin, d_col_snp, d_tiles;
     OperandPlanes op;
 };
 
@@ -682,26 +681,46 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
     const int64_t n_u = static_cast<int64_t>(desc_u.size());
     const int64_t n_u_pad = (n_u + 3) / 4 * 4;
     const int64_t n_utiles = (M + kTileK - 1) / kTileK;
-    // The contiguous SNP layout of the shared copy: one block of every SNP.
-    std::vector<BlockInfo> one_block{BlockInfo{0, static_cast<int32_t>(M), 0}};
-    std::vector<int64_t> zero{0};
-    DevBuf d_pos_u, d_desc_u, d_tiles_u, d_cols_u, d_one, d_zero, d_canon_u, d_center_u, d_t0;
-    upload(d_pos_u, pos_u, s);
-    upload(d_desc_u, desc_u, s);
-    upload(d_one, one_block, s);
-    upload(d_zero, zero, s);
-    d_tiles_u.reserve(std::max<size_t>(static_cast<size_t>(n_utiles) * sizeof(TileInfo), 16));
-    d_cols_u.reserve(std::max<size_t>(static_cast<size_t>(n_utiles) * kTileK * 4, 16));
-    d_canon_u.reserve(std::max<size_t>(static_cast<size_t>((n_utiles + 3) / 4) * n_u_pad * 32, 64));
-    d_center_u.reserve(std::max<size_t>(static_cast<size_t>(n_utiles) * kTileK * 8, 64));
-    d_t0.reserve(16);
+    // The contiguous SNP layout of the shared copy (one block of every SNP), the union's
+    // tables, its canonical genotypes and centres: one workspace, the host tables staged
+    // through pinned memory in one upload.
+    const BlockInfo one_block{0, static_cast<int32_t>(M), 0};
+    const int64_t zero = 0;
+    Packing pa;
+    const size_t o_pos = pa.add(pos_u.size() * 4);
+    const size_t o_desc = pa.add(desc_u.size() * 4);
+    const size_t o_one = pa.add(sizeof(BlockInfo));
+    const size_t o_zero = pa.add(sizeof(int64_t));
+    const size_t staged_a = pa.end;
+    const size_t o_tiles = pa.add(static_cast<size_t>(n_utiles) * sizeof(TileInfo));
+    const size_t o_cols = pa.add(static_cast<size_t>(n_utiles) * kTileK * 4);
+    const size_t o_canon = pa.add(static_cast<size_t>((n_utiles + 3) / 4) * n_u_pad * 32);
+    const size_t o_center = pa.add(static_cast<size_t>(n_utiles) * kTileK * 8);
+    const size_t o_t0 = pa.add(16);
+    c.pin_union.reserve(staged_a);
+    c.ws_union.reserve(pa.end);
+    {
+        uint8_t* h = c.pin_union.as<uint8_t>();
+        std::memcpy(h + o_pos, pos_u.data(), pos_u.size() * 4);
+        std::memcpy(h + o_desc, desc_u.data(), desc_u.size() * 4);
+        std::memcpy(h + o_one, &one_block, sizeof(BlockInfo));
+        std::memcpy(h + o_zero, &zero, sizeof(int64_t));
+        STPF2_CUDA(cudaMemcpyAsync(c.ws_union.ptr, h, staged_a, cudaMemcpyHostToDevice, s));
+    }
+    uint8_t* U = c.ws_union.as<uint8_t>();
+    auto* d_pos_u = reinterpret_cast<int32_t*>(U + o_pos);
+    auto* d_desc_u = reinterpret_cast<uint32_t*>(U + o_desc);
+    auto* d_tiles_u = reinterpret_cast<TileInfo*>(U + o_tiles);
+    auto* d_cols_u = reinterpret_cast<int32_t*>(U + o_cols);
+    auto* d_canon_u = reinterpret_cast<uint64_t*>(U + o_canon);
+    auto* d_center_u = reinterpret_cast<double*>(U + o_center);
+    auto* d_t0 = reinterpret_cast<unsigned long long*>(U + o_t0);
 
-    launch_timestamp(c, d_t0.as<unsigned long long>(), s);
-    launch_layout_tables(c, d_one.as<BlockInfo>(), d_zero.as<int64_t>(), 1, n_utiles * kTileK, d_cols_u.as<int32_t>(),
-                         d_tiles_u.as<TileInfo>(), s);
-    if (any_auto) launch_detect_ploidy_pa(c, d_rec, pitch, M, d_desc_u.as<uint32_t>(), n_u, s);
-    launch_transpose_pa(c, d_rec, pitch, n_ind, d_tiles_u.as<TileInfo>(), n_utiles, d_pos_u.as<int32_t>(), n_u_pad,
-                        d_canon_u.as<uint64_t>(), d_center_u.as<double>(), s);
+    launch_timestamp(c, d_t0, s);
+    launch_layout_tables(c, reinterpret_cast<BlockInfo*>(U + o_one), reinterpret_cast<int64_t*>(U + o_zero), 1,
+                         n_utiles * kTileK, d_cols_u, d_tiles_u, s);
+    if (any_auto) launch_detect_ploidy_pa(c, d_rec, pitch, M, d_desc_u, n_u, s);
+    launch_transpose_pa(c, d_rec, pitch, n_ind, d_tiles_u, n_utiles, d_pos_u, n_u_pad, d_canon_u, d_center_u, s);
 
     // Host tables of every request, in parallel, while the device runs the shared passes.
     std::vector<BatchMember> mem(idx.size());
@@ -739,41 +758,81 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
         rn[n] = 1.0 / static_cast<double>(n);
         rnm1[n] = 1.0 / std::max(static_cast<double>(n) - 1.0, 1.0);
     }
-    DevBuf d_sel_up, d_umap_up, d_off_up, d_rn, d_rnm1, d_counts;
-    upload(d_sel_up, sel_up, s);
-    upload(d_umap_up, umap_up, s);
-    upload(d_off_up, off_up, s);
-    upload(d_rn, rn, s);
-    upload(d_rnm1, rnm1, s);
-    d_counts.reserve(std::max<size_t>(static_cast<size_t>(UP) * static_cast<size_t>(M) * 4, 16));
+    // The batch populations' tables and every request's tables (staged in one upload), then
+    // the requests' device-built column and tile maps and the packed counts.
+    Packing pb;
+    const size_t o_sel = pb.add(sel_up.size() * 4);
+    const size_t o_umap = pb.add(umap_up.size() * 4);
+    const size_t o_off = pb.add(off_up.size() * 4);
+    const size_t o_rn = pb.add(rn.size() * 8);
+    const size_t o_rnm1 = pb.add(rn.size() * 8);
+    struct MemberOffsets {
+        size_t upop, blocks, begin, cols, tiles;
+    };
+    std::vector<MemberOffsets> mo(mem.size());
+    for (size_t m = 0; m < mem.size(); ++m) {
+        mo[m].upop = pb.add(mem[m].upop.size() * 4);
+        mo[m].blocks = pb.add(mem[m].L.blocks.size() * sizeof(BlockInfo));
+        mo[m].begin = pb.add(mem[m].L.snp_begin.size() * sizeof(int64_t));
+    }
+    const size_t staged_b = pb.end;
+    for (size_t m = 0; m < mem.size(); ++m) {
+        mo[m].cols = pb.add(static_cast<size_t>(mem[m].L.ld) * 4);
+        mo[m].tiles = pb.add(static_cast<size_t>(mem[m].L.ld / kTileK) * sizeof(TileInfo));
+    }
+    const size_t o_counts = pb.add(static_cast<size_t>(UP) * static_cast<size_t>(M) * 4);
+    c.pin_tables.reserve(staged_b);
+    c.ws_tables.reserve(pb.end);
+    {
+        uint8_t* h = c.pin_tables.as<uint8_t>();
+        std::memcpy(h + o_sel, sel_up.data(), sel_up.size() * 4);
+        std::memcpy(h + o_umap, umap_up.data(), umap_up.size() * 4);
+        std::memcpy(h + o_off, off_up.data(), off_up.size() * 4);
+        std::memcpy(h + o_rn, rn.data(), rn.size() * 8);
+        std::memcpy(h + o_rnm1, rnm1.data(), rnm1.size() * 8);
+        for (size_t m = 0; m < mem.size(); ++m) {
+            std::memcpy(h + mo[m].upop, mem[m].upop.data(), mem[m].upop.size() * 4);
+            std::memcpy(h + mo[m].blocks, mem[m].L.blocks.data(), mem[m].L.blocks.size() * sizeof(BlockInfo));
+            std::memcpy(h + mo[m].begin, mem[m].L.snp_begin.data(), mem[m].L.snp_begin.size() * sizeof(int64_t));
+        }
+        STPF2_CUDA(cudaMemcpyAsync(c.ws_tables.ptr, h, staged_b, cudaMemcpyHostToDevice, s));
+    }
+    uint8_t* T = c.ws_tables.as<uint8_t>();
+    auto* d_counts = reinterpret_cast<uint32_t*>(T + o_counts);
+    auto* d_rn = reinterpret_cast<const double*>(T + o_rn);
+    auto* d_rnm1 = reinterpret_cast<const double*>(T + o_rnm1);
     if (any_auto)
-        launch_copy_union_ploidy(c, d_sel_up.as<uint32_t>(), d_umap_up.as<int32_t>(), static_cast<int64_t>(sel_up.size()),
-                                 d_desc_u.as<uint32_t>(), s);
+        launch_copy_union_ploidy(c, reinterpret_cast<uint32_t*>(T + o_sel), reinterpret_cast<int32_t*>(T + o_umap),
+                                 static_cast<int64_t>(sel_up.size()), d_desc_u, s);
     {
         CanonDecodeArgs a;
-        a.canon = d_canon_u.as<uint64_t>();
+        a.canon = d_canon_u;
         a.n_tiles = n_utiles;
         a.n_sel = n_u_pad;
-        a.sel = d_sel_up.as<uint32_t>();
-        a.pop_off = d_off_up.as<int32_t>();
+        a.sel = reinterpret_cast<const uint32_t*>(T + o_sel);
+        a.pop_off = reinterpret_cast<const int32_t*>(T + o_off);
         a.P = UP;
-        a.rec_n = d_rn.as<double>();
-        a.rec_nm1 = d_rnm1.as<double>();
-        a.col_snp = d_cols_u.as<int32_t>();
+        a.rec_n = d_rn;
+        a.rec_nm1 = d_rnm1;
+        a.col_snp = d_cols_u;
         a.op.fmt = fmt;
         a.op.planes = nullptr;  // counts only
-        a.umap = d_umap_up.as<int32_t>();
-        a.center_snp = d_center_u.as<double>();
-        a.cnt_packed = d_counts.as<uint32_t>();
+        a.umap = reinterpret_cast<const int32_t*>(T + o_umap);
+        a.center_snp = d_center_u;
+        a.cnt_packed = d_counts;
         a.cnt_ld = M;
         launch_decode_canon(c, a, s);
     }
+    for (size_t m = 0; m < mem.size(); ++m)
+        launch_layout_tables(c, reinterpret_cast<const BlockInfo*>(T + mo[m].blocks),
+                             reinterpret_cast<const int64_t*>(T + mo[m].begin), mem[m].L.n_block, mem[m].L.ld,
+                             reinterpret_cast<int32_t*>(T + mo[m].cols), reinterpret_cast<TileInfo*>(T + mo[m].tiles), s);
 
     // Waves of requests whose operand images (and device-side outputs) fit together.
     STPF2_CUDA(cudaStreamSynchronize(s));
     size_t free_b = 0, total_b = 0;
     STPF2_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t held = c.ws_batch.bytes + c.ws_f2.bytes + c.ws_vpair.bytes;
+    const size_t held = c.ws_batch.bytes + c.ws_f2.bytes + c.ws_vpair.bytes;  // reusable for this batch's images
     const size_t avail = free_b + held;
     const size_t budget = avail > (size_t(2) << 30) ? (avail - (size_t(2) << 30)) * 9 / 10 : 0;
     std::vector<std::vector<size_t>> waves(1);
@@ -804,20 +863,12 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
         size_t io = 0, oo = 0;
         for (size_t w = 0; w < wave.size(); ++w) {
             BatchMember& p = mem[wave[w]];
+            const MemberOffsets& q = mo[wave[w]];
             const stp_f2_output& o = outs[p.k];
-            upload(p.d_upop, p.upop, s);
-            upload(p.d_blocks, p.L.blocks, s);
-            upload(p.d_snp_begin, p.L.snp_begin, s);
-            const int64_t n_tiles = p.L.ld / kTileK;
-            p.d_col_snp.reserve(static_cast<size_t>(p.L.ld) * 4);
-            p.d_tiles.reserve(std::max<size_t>(static_cast<size_t>(n_tiles) * sizeof(TileInfo), 16));
-            launch_layout_tables(c, p.d_blocks.as<BlockInfo>(), p.d_snp_begin.as<int64_t>(), p.L.n_block, p.L.ld,
-                                 p.d_col_snp.as<int32_t>(), p.d_tiles.as<TileInfo>(), s);
             bind_operand_planes(p.op, fmt, p.P, p.L.ld, c.ws_batch.as<uint8_t>() + io);
             io += p.img_bytes;
-            launch_emit_counts(c, d_counts.as<uint32_t>(), M, p.d_upop.as<int32_t>(), p.P, n_tiles,
-                               p.d_col_snp.as<int32_t>(), d_center_u.as<double>(), d_rn.as<double>(),
-                               d_rnm1.as<double>(), p.op, s);
+            launch_emit_counts(c, d_counts, M, reinterpret_cast<const int32_t*>(T + q.upop), p.P, p.L.ld / kTileK,
+                               reinterpret_cast<const int32_t*>(T + q.cols), d_center_u, d_rn, d_rnm1, p.op, s);
             double* f2 = o.f2;
             double* vp = o.vpair;
             if (!o.on_device) {
@@ -831,7 +882,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
         }
         std::vector<unsigned long long> stamps;
         launch_f2_umma_grouped(c, fmt, mem[wave[0]].op.scale_inv, chunk_stages_of(prec), specs, s, &stamps);
-        if (t0 == 0) STPF2_CUDA(cudaMemcpy(&t0, d_t0.ptr, sizeof(t0), cudaMemcpyDeviceToHost));
+        if (t0 == 0) STPF2_CUDA(cudaMemcpy(&t0, d_t0, sizeof(t0), cudaMemcpyDeviceToHost));
         for (size_t w = 0; w < wave.size(); ++w) {
             BatchMember& p = mem[wave[w]];
             done_ms[wave[w]] = stamps[w] >= t0 ? static_cast<double>(stamps[w] - t0) * 1e-6 : 0.0;
@@ -844,7 +895,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
             if (o.ploidy_out && p.n_sel > 0) {
                 if (desc_h.empty()) {
                     desc_h.resize(desc_u.size());
-                    STPF2_CUDA(cudaMemcpyAsync(desc_h.data(), d_desc_u.ptr, desc_h.size() * 4, cudaMemcpyDeviceToHost, s));
+                    STPF2_CUDA(cudaMemcpyAsync(desc_h.data(), d_desc_u, desc_h.size() * 4, cudaMemcpyDeviceToHost, s));
                     STPF2_CUDA(cudaStreamSynchronize(s));
                 }
                 const stp_f2_request& r = reqs[p.k];

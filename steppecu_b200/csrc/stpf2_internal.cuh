@@ -63,6 +63,36 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
 
+// Grow-only pinned host memory, for packing many small tables into one upload. Reserving
+// more drops the contents; the caller makes sure no copy from it is still in flight.
+struct PinnedBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    ~PinnedBuf() { if (ptr) cudaFreeHost(ptr); }
+    void reserve(size_t n) {
+        if (n <= bytes) return;
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        STPF2_CUDA(cudaMallocHost(&ptr, n));
+        bytes = n;
+    }
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Offsets of buffers packed into one allocation (each start 256-byte aligned).
+struct Packing {
+    size_t end = 0;
+    size_t add(size_t bytes) {
+        const size_t o = end;
+        end = (end + bytes + 255) & ~size_t(255);
+        return o;
+    }
+};
+
 // ---- context --------------------------------------------------------------------------
 
 struct Ctx {
@@ -74,7 +104,11 @@ struct Ctx {
     // Grow-only scratch reused across calls of the host-buffer entry points, so repeated
     // extractions do not pay cudaMalloc each time.
     DevBuf ws_records, ws_f2, ws_vpair, ws_misc;
-    DevBuf ws_batch;  // operand images of a grouped batch
+    // Grouped batches: operand images; the shared canonical copy and its tables; the batch
+    // populations' counts and every request's tables; the contraction's work lists; and
+    // the pinned staging of the tables.
+    DevBuf ws_batch, ws_union, ws_tables, ws_items;
+    PinnedBuf pin_union, pin_tables, pin_items;
     // Completion time of each request of the last stp_f2_extract_batch call, in ms from the
     // start of its group's device work (NaN for requests that ran on their own).
     std::vector<double> last_batch_ms;
