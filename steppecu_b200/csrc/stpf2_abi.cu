@@ -161,6 +161,8 @@ struct Plan {
     bool detect = false;
     BlockLayout L;
     DevBuf sel, pop_off, pos, tiles, col_snp, rec_n, rec_nm1, canon, center, blocks, items, own_planes, repitched;
+    uint64_t* canon_ptr = nullptr;  // canon's storage, or a context workspace (one-shot calls)
+    double* center_ptr = nullptr;
     int64_t n_ind = 0, n_tiles = 0, n_sel_pad = 0;
     int n_items = 0;
     bool repitch = false;
@@ -194,8 +196,11 @@ struct Plan {
 namespace {
 
 // Validates a request and builds its plan. planes_base != nullptr borrows operand
-// storage (at least operand_plane_bytes) instead of allocating it.
-std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch, void* planes_base) {
+// storage (at least operand_plane_bytes) instead of allocating it; borrow_ws takes the
+// canonical genotypes and centres from the context's grow-only workspace as well (for
+// one-shot calls, which finish before the next call on the context starts).
+std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch, void* planes_base,
+                                 bool borrow_ws = false) {
     need(r.n_pop >= 0 && r.geno.n_snp >= 0 && r.n_block >= 0, "negative extent");
     need(r.geno.bytes_per_record > 0 || r.geno.n_snp == 0, "bytes_per_record is 0");
     need(r.pop_offsets != nullptr || r.n_pop == 0, "pop_offsets is NULL");
@@ -278,8 +283,16 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
     upload(p->tiles, tiles, s);
     upload(p->col_snp, col_snp, s);
     p->n_sel_pad = (n_sel + 3) / 4 * 4;
-    p->canon.reserve(std::max<size_t>(static_cast<size_t>((p->n_tiles + 3) / 4) * p->n_sel_pad * 32, 64));
-    p->center.reserve(std::max<size_t>(static_cast<size_t>(p->L.ld) * 8, 64));
+    {
+        const size_t canon_bytes = std::max<size_t>(static_cast<size_t>((p->n_tiles + 3) / 4) * p->n_sel_pad * 32, 64);
+        const size_t center_bytes = std::max<size_t>(static_cast<size_t>(p->L.ld) * 8, 64);
+        DevBuf& cb = borrow_ws ? c.ws_canon : p->canon;
+        DevBuf& eb = borrow_ws ? c.ws_center : p->center;
+        cb.reserve(canon_bytes);
+        eb.reserve(center_bytes);
+        p->canon_ptr = cb.as<uint64_t>();
+        p->center_ptr = eb.as<double>();
+    }
 
     // The transpose reads records with 4-byte (16-byte when aligned so) copies: records of
     // a pitch that is not a multiple of 4 are copied once per run into a 16-byte pitch.
@@ -332,15 +345,15 @@ void launch_decode(Plan& p, const uint8_t* d_records, int32_t* cnt_ac2, int32_t*
     if (p.detect && detect) launch_detect_ploidy_pa(c, rec, p.pitch, p.n_snp, p.sel.as<uint32_t>(), p.n_sel, s);
     if (t1 <= t0) return;
     launch_transpose_pa(c, rec, p.pitch, p.n_ind, p.tiles.as<TileInfo>() + t0, t1 - t0, p.pos.as<int32_t>(),
-                        p.n_sel_pad, p.canon.as<uint64_t>(), p.center.as<double>() + t0 * kTileK, s);
+                        p.n_sel_pad, p.canon_ptr, p.center_ptr + t0 * kTileK, s);
     CanonDecodeArgs a;
-    a.canon = p.canon.as<uint64_t>();
+    a.canon = p.canon_ptr;
     a.n_tiles = t1 - t0;
     a.n_sel = p.n_sel_pad;
     a.sel = p.sel.as<uint32_t>();
     a.pop_off = p.pop_off.as<int32_t>();
     a.P = p.P;
-    a.center = p.center.as<double>() + t0 * kTileK;
+    a.center = p.center_ptr + t0 * kTileK;
     a.rec_n = p.rec_n.as<double>();
     a.rec_nm1 = p.rec_nm1.as<double>();
     a.col_snp = p.col_snp.as<int32_t>() + t0 * kTileK;
@@ -488,7 +501,7 @@ void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
         const BlockLayout probe = make_block_layout(r.block_id, r.geno.n_snp, r.n_block);
         c.ws_misc.reserve(operand_plane_bytes(fmt_of(r.precision), std::max(r.n_pop, 1), probe.ld));
     }
-    std::unique_ptr<Plan> p = build_plan(c, r, pitch, c.ws_misc.ptr);
+    std::unique_ptr<Plan> p = build_plan(c, r, pitch, c.ws_misc.ptr, true);
     if (o.block_sizes) copy_block_sizes(p->L, o.block_sizes);
     const size_t out_elems = static_cast<size_t>(std::max(r.n_pop, 0)) * std::max(r.n_pop, 0) * std::max(r.n_block, 0);
     double* d_f2 = o.f2;

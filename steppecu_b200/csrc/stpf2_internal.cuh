@@ -103,7 +103,7 @@ struct Ctx {
     cudaStream_t h2d = nullptr, d2h = nullptr;  // copy streams of the pipelined host-buffer path
     // Grow-only scratch reused across calls of the host-buffer entry points, so repeated
     // extractions do not pay cudaMalloc each time.
-    DevBuf ws_records, ws_f2, ws_vpair, ws_misc;
+    DevBuf ws_records, ws_f2, ws_vpair, ws_misc, ws_canon, ws_center;
     // Grouped batches: operand images; the shared canonical copy and its tables; the batch
     // populations' counts and every request's tables; the contraction's work lists; and
     // the pinned staging of the tables.
