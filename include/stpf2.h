@@ -182,6 +182,29 @@ stp_status stp_f2_extract_blocks(stp_ctx* ctx, const stp_f2_request* req, stp_f2
 stp_status stp_f2_extract_batch(stp_ctx* ctx, const stp_f2_request* reqs, int32_t n_req,
                                 stp_f2_output* outs);
 
+/* f-statistics from an F2BlockTensor and their block jackknife, FP64 on the device.
+ * Blocks where some pair is missing (vpair = 0) and another present are dropped
+ * (survivor_blocks, src/device/cpu/cpu_backend.cpp:124-151); per surviving block the
+ * statistic is assembled from f2 slabs (assemble_f4_quartets / assemble_f3_triples /
+ * assemble_f4, cpu_backend.cpp:2064-2216) and est / var are the block-size-weighted
+ * estimate and jackknife variance (compute_loo_and_total + jackknife_diag, :2674-2720,
+ * :2273-2306). kind STP_FSTAT_F4: idx holds n_stat quartets (p1, p2, p3, p4) ->
+ * (f2(p2,p3) + f2(p1,p4) - f2(p1,p3) - f2(p2,p4)) / 2; STP_FSTAT_F3: n_stat triples
+ * (c, a, b) -> (f2(c,a) + f2(c,b) - f2(a,b)) / 2; STP_FSTAT_F4_LEFT_RIGHT: idx holds the
+ * n_stat left indices then the n_idx - n_stat right ones, and statistic j + nr*i
+ * (nl = n_stat - 1, nr = n_idx - n_stat - 1) is (f2(Li,R0) + f2(L0,Rj) - f2(L0,R0) -
+ * f2(Li,Rj)) / 2. f2 / vpair: [P x P x n_block] (host, or device when on_device);
+ * block_sizes, idx, est, var: host. With no surviving block est = var = 0. */
+typedef enum stp_fstat_kind {
+    STP_FSTAT_F4 = 0,
+    STP_FSTAT_F3 = 1,
+    STP_FSTAT_F4_LEFT_RIGHT = 2
+} stp_fstat_kind;
+
+stp_status stp_fstats(stp_ctx* ctx, const double* f2, const double* vpair, const int32_t* block_sizes,
+                      int32_t P, int32_t n_block, int32_t on_device, int32_t kind, const int32_t* idx,
+                      int64_t n_idx, int64_t n_stat, double* est, double* var, int32_t* n_survivors);
+
 /* Completion time of each request of this context's last stp_f2_extract_batch call, in ms
  * from the start of its group's device work (%globaltimer stamps written by the last work
  * item of each request); NaN for requests that ran on their own. No counterpart in the

@@ -319,3 +319,68 @@ void or_block_jackknife(const double* x, const int32_t* block_sizes, long m, int
     }
     free(loo);
 }
+
+/* cpu_backend.cpp:124-151. */
+int or_survivor_blocks(const double* vpair, int P, int nb, int32_t* keep) {
+    const size_t slab = (size_t)P * (size_t)P;
+    int kept = 0;
+    for (int b = 0; b < nb; ++b) {
+        int any_missing = 0, any_present = 0;
+        for (size_t e = 0; e < slab; ++e) {
+            if (!(vpair[slab * (size_t)b + e] > 0.0)) any_missing = 1;
+            else any_present = 1;
+            if (any_missing && any_present) break;
+        }
+        keep[b] = !(any_missing && any_present);
+        kept += keep[b];
+    }
+    return kept;
+}
+
+/* cpu_backend.cpp:2064-2216 then 2674-2720 / 2273-2306. */
+int or_fstats(const double* f2, const double* vpair, const int32_t* block_sizes, int P, int nb, int kind,
+              const int32_t* idx, long n_idx, long n_stat, double* est, double* var, double* x_blocks) {
+    const size_t slab = (size_t)P * (size_t)P;
+    long m = 0, nl = 0, nr = 0;
+    if (kind == 0 || kind == 1) m = n_stat;
+    else {
+        nl = n_stat - 1;
+        nr = n_idx - n_stat - 1;
+        m = (nl > 0 && nr > 0) ? nl * nr : 0;
+    }
+    for (long k = 0; k < m; ++k) est[k] = var[k] = 0.0;
+    if (m <= 0 || nb <= 0) return 0;
+    int32_t* keep = (int32_t*)malloc((size_t)nb * sizeof(int32_t));
+    const int ns = or_survivor_blocks(vpair, P, nb, keep);
+    int32_t* bl = (int32_t*)malloc((size_t)(ns > 0 ? ns : 1) * sizeof(int32_t));
+    double* x = (double*)malloc((size_t)m * (size_t)(ns > 0 ? ns : 1) * sizeof(double));
+#define F2AT(i, j, b) f2[(size_t)(i) + (size_t)P * (size_t)(j) + slab * (size_t)(b)]
+    int bs = 0;
+    for (int b = 0; b < nb; ++b) {
+        if (!keep[b]) continue;
+        bl[bs] = block_sizes[b];
+        for (long k = 0; k < m; ++k) {
+            double v = 0.0;
+            if (kind == 0) {
+                const int p1 = idx[4 * k], p2 = idx[4 * k + 1], p3 = idx[4 * k + 2], p4 = idx[4 * k + 3];
+                v = 0.5 * (F2AT(p2, p3, b) + F2AT(p1, p4, b) - F2AT(p1, p3, b) - F2AT(p2, p4, b));
+            } else if (kind == 1) {
+                const int pc = idx[3 * k], pa = idx[3 * k + 1], pb = idx[3 * k + 2];
+                v = 0.5 * (F2AT(pc, pa, b) + F2AT(pc, pb, b) - F2AT(pa, pb, b));
+            } else {
+                const long i = k / nr, j = k % nr;  /* k = j + nr*i */
+                const int L0 = idx[0], R0 = idx[n_stat], Li = idx[1 + i], Rj = idx[n_stat + 1 + j];
+                v = 0.5 * (F2AT(Li, R0, b) + F2AT(L0, Rj, b) - F2AT(L0, R0, b) - F2AT(Li, Rj, b));
+            }
+            x[(size_t)k + (size_t)m * (size_t)bs] = v;
+        }
+        ++bs;
+    }
+#undef F2AT
+    if (x_blocks) memcpy(x_blocks, x, (size_t)m * (size_t)ns * sizeof(double));
+    if (ns > 0) or_block_jackknife(x, bl, m, ns, est, var);
+    free(keep);
+    free(bl);
+    free(x);
+    return ns;
+}

@@ -89,6 +89,24 @@ int or_assign_blocks(const int32_t* chrom, const double* genpos_morgans, long M,
 void or_block_jackknife(const double* x, const int32_t* block_sizes, long m, int nb,
                         double* est, double* var);
 
+/* cpu_backend.cpp:124-151 (survivor_blocks): keep[b] = 0 when block b has both a missing
+ * pair (vpair not > 0, f2_estimator.hpp:49-51) and a present one, else 1. Returns the
+ * number kept. */
+int or_survivor_blocks(const double* vpair, int P, int nb, int32_t* keep);
+
+/* f-statistics from an F2BlockTensor over its surviving blocks, with the block jackknife
+ * of each (cpu_backend.cpp:2064-2216 assemble_f4 / assemble_f4_quartets /
+ * assemble_f3_triples, then or_block_jackknife). kind 0: quartets idx[4k..4k+3] ->
+ * 0.5(f2(p2,p3) + f2(p1,p4) - f2(p1,p3) - f2(p2,p4)); kind 1: triples (c, a, b) ->
+ * 0.5(f2(c,a) + f2(c,b) - f2(a,b)); kind 2: left idx[0..n_left) and right
+ * idx[n_left..n_left+n_right) with L0 = left[0], R0 = right[0]: statistic
+ * k = j + nr*i (i < nl = n_left-1, j < nr = n_right-1) -> 0.5(f2(Li,R0) + f2(L0,Rj) -
+ * f2(L0,R0) - f2(Li,Rj)). n_stat: quartets / triples count (kinds 0, 1) or n_left
+ * (kind 2, n_right = n_idx - n_left). Returns the number of surviving blocks;
+ * x_blocks (optional, n_out x survivors) receives the assembled per-block values. */
+int or_fstats(const double* f2, const double* vpair, const int32_t* block_sizes, int P, int nb, int kind,
+              const int32_t* idx, long n_idx, long n_stat, double* est, double* var, double* x_blocks);
+
 #ifdef __cplusplus
 }
 #endif

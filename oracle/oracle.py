@@ -230,3 +230,40 @@ def f2_from_panel(records, sel_rows, pop_offsets, block_id, n_block, ploidy=None
     if threads is not None and threads > 1:
         return compute_f2_blocks_sharded(q, v, nd, P, block_id, n_block, threads, lib)
     return compute_f2_blocks(q, v, nd, P, block_id, n_block, lib)
+
+
+def survivor_blocks(vpair, P, nb):
+    """cpu_backend.cpp:124-151: keep flags per block."""
+    vp = np.ascontiguousarray(vpair, np.float64)
+    keep = np.zeros(max(nb, 1), np.int32)
+    port().fn("survivor_blocks", C.c_int, [_P, C.c_int, C.c_int, _P])(_ptr(vp), P, nb, _ptr(keep))
+    return keep[:nb].astype(bool)
+
+
+FSTAT_KINDS = {"f4": 0, "f3": 1, "f4_lr": 2}
+
+
+def fstats(f2, vpair, block_sizes, P, nb, kind, idx, n_stat, lib: str = "port", with_blocks: bool = False):
+    """f4 quartets / f3 triples / f4 left-right statistics with their block jackknife over
+    the surviving blocks (see or_fstats). Returns (est, var, n_survivors[, x_blocks])."""
+    k = FSTAT_KINDS[kind] if isinstance(kind, str) else int(kind)
+    f2 = np.ascontiguousarray(f2, np.float64)
+    vp = np.ascontiguousarray(vpair, np.float64)
+    bs = np.ascontiguousarray(block_sizes, np.int32)
+    ix = np.ascontiguousarray(idx, np.int32)
+    if k == 2:
+        m = max(n_stat - 1, 0) * max(ix.size - n_stat - 1, 0)
+    else:
+        m = n_stat
+    est, var = np.zeros(max(m, 1)), np.zeros(max(m, 1))
+    if lib == "ref":
+        ns = ref().fn("fstats", C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_long, C.c_long, _P, _P])(
+            _ptr(f2), _ptr(vp), _ptr(bs), P, nb, k, _ptr(ix), ix.size, n_stat, _ptr(est), _ptr(var))
+        if ns < 0:
+            raise ValueError("reference f-statistics failed")
+        return est[:m], var[:m], ns
+    xb = np.zeros(max(m, 1) * max(nb, 1))
+    ns = port().fn("fstats", C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_long, C.c_long, _P, _P, _P])(
+        _ptr(f2), _ptr(vp), _ptr(bs), P, nb, k, _ptr(ix), ix.size, n_stat, _ptr(est), _ptr(var), _ptr(xb))
+    out = (est[:m], var[:m], ns)
+    return out + (xb[:m * ns].reshape(ns, m),) if with_blocks else out

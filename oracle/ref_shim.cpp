@@ -143,4 +143,36 @@ int ref_block_jackknife(const double* x, const int* block_sizes, long m, int nb,
     }
 }
 
+// The reference's f-statistic assembly and jackknife through its public surface
+// (cpu_backend.cpp:2064-2216, :2273-2306), arguments as or_fstats. Returns the number of
+// surviving blocks, or -1.
+int ref_fstats(const double* f2, const double* vpair, const int* block_sizes, int P, int nb, int kind,
+               const int* idx, long n_idx, long n_stat, double* est, double* var) {
+    try {
+        steppe::F2BlockTensor t;
+        t.P = P;
+        t.n_block = nb;
+        const std::size_t n = static_cast<std::size_t>(P) * static_cast<std::size_t>(P) * static_cast<std::size_t>(nb);
+        t.f2.assign(f2, f2 + n);
+        t.vpair.assign(vpair, vpair + n);
+        t.block_sizes.assign(block_sizes, block_sizes + nb);
+        auto& be = backend();
+        steppe::F4Blocks f;
+        if (kind == 0) f = be->assemble_f4_quartets(t, std::span<const int>(idx, static_cast<std::size_t>(4 * n_stat)), steppe::Precision::fp64());
+        else if (kind == 1) f = be->assemble_f3_triples(t, std::span<const int>(idx, static_cast<std::size_t>(3 * n_stat)), steppe::Precision::fp64());
+        else f = be->assemble_f4(t, std::span<const int>(idx, static_cast<std::size_t>(n_stat)),
+                                 std::span<const int>(idx + n_stat, static_cast<std::size_t>(n_idx - n_stat)),
+                                 steppe::Precision::fp64());
+        const steppe::JackknifeDiag d = be->jackknife_diag(f, f.block_sizes, steppe::Precision::fp64());
+        const std::size_t m = static_cast<std::size_t>(f.nl) * static_cast<std::size_t>(f.nr);
+        for (std::size_t k = 0; k < m; ++k) {
+            est[k] = k < f.x_total.size() ? f.x_total[k] : 0.0;
+            var[k] = k < d.var.size() ? d.var[k] : 0.0;
+        }
+        return f.n_block;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
 }  // extern "C"

@@ -36,6 +36,9 @@ PREC_FP32_SIMT = 0
 PREC_SPLIT_BF16 = 1
 PREC_SPLIT_F16 = 2
 PREC_SPLIT_F16_FINE = 3
+FSTAT_F4 = 0
+FSTAT_F3 = 1
+FSTAT_F4_LEFT_RIGHT = 2
 
 PLOIDY_AUTO = 0
 PLOIDY_PSEUDO = 1
@@ -103,6 +106,8 @@ SIGNATURES = {
     "stp_f2_extract_blocks": (C.c_int, [_P, C.POINTER(F2Request), C.POINTER(F2Output)]),
     "stp_f2_extract_batch": (C.c_int, [_P, C.POINTER(F2Request), C.c_int32, C.POINTER(F2Output)]),
     "stp_last_batch_times": (C.c_int, [_P, _P, C.c_int32]),
+    "stp_fstats": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int64, C.c_int64,
+                             _P, _P, _P]),
     "stp_f2_jackknife": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, _P, _P]),
     "stp_plan_create": (_P, [_P, C.POINTER(F2Request), C.POINTER(C.c_int)]),
     "stp_plan_run": (C.c_int, [_P, _P, _P, _P, _P]),

@@ -237,6 +237,44 @@ class Context:
         L.check(L.lib().stp_f2_extract_batch(self._h, reqs, len(requests), outs))
         return results
 
+    # -- f-statistics from an F2BlockTensor -----------------------------------------------------
+    def fstats(self, f2, vpair, block_sizes, P: int, n_block: int, kind: int, idx, n_stat: int):
+        """stp_fstats: (est, var, n_survivors). f2 / vpair flat [P*P*n_block], numpy (host) or
+        torch CUDA (device)."""
+        on_dev = _is_torch_cuda(f2)
+        if not on_dev:
+            f2 = np.ascontiguousarray(f2, np.float64)
+            vpair = np.ascontiguousarray(vpair, np.float64)
+        bs, ix = _i32(block_sizes), _i32(idx)
+        if kind == L.FSTAT_F4_LEFT_RIGHT:
+            m = max(n_stat - 1, 0) * max(ix.size - n_stat - 1, 0)
+        else:
+            m = n_stat
+        est, var = np.zeros(max(m, 1)), np.zeros(max(m, 1))
+        ns = C.c_int32(0)
+        L.check(L.lib().stp_fstats(self._h, _data_ptr(f2), _data_ptr(vpair), L.ptr(bs), P, n_block, 1 if on_dev else 0,
+                                   kind, L.ptr(ix), ix.size, n_stat, L.ptr(est), L.ptr(var), C.byref(ns)))
+        return est[:m], var[:m], int(ns.value)
+
+    def f4(self, t: F2Tensor, quartets):
+        """f4(p1, p2; p3, p4) per quartet row with its jackknife variance (est, var, n_survivors)."""
+        q = _i32(quartets).reshape(-1, 4)
+        return self.fstats(t.f2, t.vpair, t.block_sizes, t.P, t.n_block, L.FSTAT_F4, q.reshape(-1), q.shape[0])
+
+    def f3(self, t: F2Tensor, triples):
+        """f3(c; a, b) per triple row (c, a, b)."""
+        q = _i32(triples).reshape(-1, 3)
+        return self.fstats(t.f2, t.vpair, t.block_sizes, t.P, t.n_block, L.FSTAT_F3, q.reshape(-1), q.shape[0])
+
+    def f4_matrix(self, t: F2Tensor, left, right):
+        """qpAdm's f4 matrix: statistic j + nr*i for left[1+i], right[1+j] against left[0],
+        right[0]; returned as est, var of shape [nl, nr]."""
+        lf, rt = _i32(left), _i32(right)
+        est, var, ns = self.fstats(t.f2, t.vpair, t.block_sizes, t.P, t.n_block, L.FSTAT_F4_LEFT_RIGHT,
+                                   np.concatenate([lf, rt]), lf.size)
+        nl, nr = max(lf.size - 1, 0), max(rt.size - 1, 0)
+        return est.reshape(nl, nr), var.reshape(nl, nr), ns
+
     def last_batch_times(self, n: int) -> np.ndarray:
         """Per-request completion times (ms from the start of the group's device work) of the
         last extract_batch call; NaN for requests that ran on their own."""

@@ -1270,6 +1270,80 @@ stp_status stp_f2_extract_batch(stp_ctx* ctx, const stp_f2_request* reqs, int32_
     });
 }
 
+stp_status stp_fstats(stp_ctx* ctx, const double* f2, const double* vpair, const int32_t* block_sizes,
+                      int32_t P, int32_t n_block, int32_t on_device, int32_t kind, const int32_t* idx,
+                      int64_t n_idx, int64_t n_stat, double* est, double* var, int32_t* n_survivors) {
+    return guarded([&] {
+        need(ctx != nullptr, "null context");
+        need(kind >= STP_FSTAT_F4 && kind <= STP_FSTAT_F4_LEFT_RIGHT, "unknown f-statistic kind");
+        need(P >= 0 && n_block >= 0 && n_idx >= 0 && n_stat >= 0, "negative extent");
+        use_device(*ctx);
+        int64_t m = 0, nr = 0;
+        if (kind == STP_FSTAT_F4) {
+            need(n_idx == 4 * n_stat, "quartets: n_idx must be 4 * n_stat");
+            m = n_stat;
+        } else if (kind == STP_FSTAT_F3) {
+            need(n_idx == 3 * n_stat, "triples: n_idx must be 3 * n_stat");
+            m = n_stat;
+        } else {
+            need(n_stat <= n_idx, "left indices exceed n_idx");
+            const int64_t nl = n_stat - 1;
+            nr = n_idx - n_stat - 1;
+            m = (nl > 0 && nr > 0) ? nl * nr : 0;
+        }
+        if (n_survivors) *n_survivors = 0;
+        if (m > 0) {
+            need(est != nullptr && var != nullptr, "null output");
+            std::fill(est, est + m, 0.0);
+            std::fill(var, var + m, 0.0);
+        }
+        if (m <= 0 || n_block <= 0 || P <= 0) return;
+        need(f2 && vpair && block_sizes && idx, "null argument");
+        for (int64_t q = 0; q < n_idx; ++q) need(idx[q] >= 0 && idx[q] < P, "population index outside [0, P)");
+        cudaStream_t s = ctx->stream;
+        const size_t elems = static_cast<size_t>(P) * P * n_block;
+        const double* d_f2 = f2;
+        const double* d_vp = vpair;
+        if (!on_device) {
+            ctx->ws_f2.reserve(elems * 8);
+            ctx->ws_vpair.reserve(elems * 8);
+            STPF2_CUDA(cudaMemcpyAsync(ctx->ws_f2.ptr, f2, elems * 8, cudaMemcpyHostToDevice, s));
+            STPF2_CUDA(cudaMemcpyAsync(ctx->ws_vpair.ptr, vpair, elems * 8, cudaMemcpyHostToDevice, s));
+            d_f2 = ctx->ws_f2.as<double>();
+            d_vp = ctx->ws_vpair.as<double>();
+        }
+        DevBuf d_keep;
+        d_keep.reserve(static_cast<size_t>(n_block) * 4);
+        launch_survivors(*ctx, d_vp, P, n_block, d_keep.as<int32_t>(), s);
+        std::vector<int32_t> keep(static_cast<size_t>(n_block));
+        STPF2_CUDA(cudaMemcpyAsync(keep.data(), d_keep.ptr, keep.size() * 4, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaStreamSynchronize(s));
+        std::vector<int32_t> surv, bl;
+        for (int32_t b = 0; b < n_block; ++b)
+            if (keep[b]) {
+                surv.push_back(b);
+                bl.push_back(block_sizes[b]);
+            }
+        const int ns = static_cast<int>(surv.size());
+        if (n_survivors) *n_survivors = ns;
+        if (ns == 0) return;
+        std::vector<int32_t> ix(idx, idx + n_idx);
+        DevBuf d_surv, d_bl, d_idx, d_x, d_est, d_var;
+        upload(d_surv, surv, s);
+        upload(d_bl, bl, s);
+        upload(d_idx, ix, s);
+        d_x.reserve(static_cast<size_t>(m) * ns * 8);
+        d_est.reserve(static_cast<size_t>(m) * 8);
+        d_var.reserve(static_cast<size_t>(m) * 8);
+        launch_fstat_assemble(*ctx, d_f2, P, d_surv.as<int32_t>(), ns, kind, d_idx.as<int32_t>(), n_stat, m, nr,
+                              d_x.as<double>(), s);
+        launch_jackknife(*ctx, d_x.as<double>(), d_bl.as<int32_t>(), m, ns, d_est.as<double>(), d_var.as<double>(), s);
+        STPF2_CUDA(cudaMemcpyAsync(est, d_est.ptr, static_cast<size_t>(m) * 8, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaMemcpyAsync(var, d_var.ptr, static_cast<size_t>(m) * 8, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 stp_status stp_last_batch_times(stp_ctx* ctx, double* ms, int32_t n) {
     return guarded([&] {
         need(ctx != nullptr, "null context");

@@ -324,6 +324,9 @@ void launch_f2_umma_blocks(Ctx& c, UmmaPlan* p, int b0, int b1, double* f2, doub
 void umma_check(UmmaPlan* p);
 int umma_tile();
 
+void launch_survivors(Ctx& c, const double* vpair, int P, int nb, int32_t* keep, cudaStream_t s);
+void launch_fstat_assemble(Ctx& c, const double* f2, int P, const int32_t* surv, int ns, int kind,
+                           const int32_t* idx, int64_t n_stat, int64_t m, int64_t nr, double* x, cudaStream_t s);
 void launch_jackknife(Ctx& c, const double* x, const int32_t* block_sizes, int64_t m, int nb,
                       double* est, double* var, cudaStream_t s);
 
