@@ -688,23 +688,26 @@ void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t
 namespace {
 // Operand images of one request from packed per-population counts (pop-major, row u at
 // counts + u * cnt_ld, SNP s at column s): its population i reads row upop[i], its padded
-// column c SNP col_snp[c]. One CTA per (64 populations, quad of 4 column tiles); lane =
-// (population, 8-column chunk), as in the decode's emit phase, with the same terms.
+// column c SNP col_snp[c]. Work unit = (8-row group, 32-column tile), one per warp from a
+// flat range (row groups of one tile on neighbouring warps, so the tile's column maps are
+// shared through L1), so every warp is busy whatever the population count; lane =
+// (row, 8-column chunk), and each 16-byte store of a plane fills 8 whole 64-byte rows of
+// the tile image. The terms are the decode's (terms8_from_counts).
 template <OpFmt F>
-__global__ void __launch_bounds__(kDecThreads2)
+__global__ void __launch_bounds__(256)
 emit_counts_kernel(const uint32_t* __restrict__ counts, int64_t cnt_ld, const int32_t* __restrict__ upop, int P,
                    int64_t n_tiles, const int32_t* __restrict__ col_snp, const double* __restrict__ center_snp,
                    const double* __restrict__ rec_n, const double* __restrict__ rec_nm1, OperandPlanes op) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     const int r = lane & 7, chunk = lane >> 3;
-    const int i = blockIdx.y * kDecPops + warp * 8 + r;
-    if (i >= P) return;
-    const uint32_t* row = counts + static_cast<int64_t>(__ldg(upop + i)) * cnt_ld;
-    const int64_t q = blockIdx.x;
-#pragma unroll 1
-    for (int sub = 0; sub < 4; ++sub) {
-        const int64_t t = 4 * q + sub;
-        if (t >= n_tiles) break;
+    const int64_t n_rg = (P + 7) / 8;
+    const int64_t n_units = n_rg * n_tiles;
+    const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+    for (int64_t u = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); u < n_units; u += warps) {
+        const int64_t t = u / n_rg;
+        const int i = static_cast<int>(u - t * n_rg) * 8 + r;
+        if (i >= P) continue;
+        const uint32_t* row = counts + static_cast<int64_t>(__ldg(upop + i)) * cnt_ld;
         const int64_t col0 = t * kTileCols + 8 * chunk;
         uint32_t v[8];
         double cen[8];
@@ -768,11 +771,13 @@ void launch_emit_counts(Ctx& c, const uint32_t* counts, int64_t cnt_ld, const in
                         const int32_t* col_snp, const double* center_snp, const double* rec_n, const double* rec_nm1,
                         const OperandPlanes& op, cudaStream_t s) {
     if (P <= 0 || n_tiles <= 0) return;
-    const dim3 grid(static_cast<unsigned>((n_tiles + 3) / 4), static_cast<unsigned>((P + kDecPops - 1) / kDecPops));
+    const int64_t units = (P + 7) / 8 * n_tiles;
+    const int64_t cap = static_cast<int64_t>(c.sm_count) * 16;  // 16 CTAs of 8 warps per SM, grid-stride beyond
+    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((units + 7) / 8, cap)));
     switch (op.fmt) {
-        case OpFmt::F32: emit_counts_kernel<OpFmt::F32><<<grid, kDecThreads2, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
-        case OpFmt::BF16: emit_counts_kernel<OpFmt::BF16><<<grid, kDecThreads2, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
-        case OpFmt::F16: emit_counts_kernel<OpFmt::F16><<<grid, kDecThreads2, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
+        case OpFmt::F32: emit_counts_kernel<OpFmt::F32><<<grid, 256, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
+        case OpFmt::BF16: emit_counts_kernel<OpFmt::BF16><<<grid, 256, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
+        case OpFmt::F16: emit_counts_kernel<OpFmt::F16><<<grid, 256, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
     }
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
