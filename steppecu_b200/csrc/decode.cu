@@ -649,6 +649,45 @@ __global__ void feed_qvn_kernel(const double* __restrict__ Q, const double* __re
 
 }  // namespace
 
+namespace {
+// The same rule with one warp per 4-byte record word (16 samples): the lanes read the word
+// from 32 records at a time (coalesced across the warps of neighbouring words) and OR
+// their het masks (code 1: low bit set, high bit clear); lanes 0-15 then write the
+// ploidy of the word's selected samples (pos: file row -> selected index, -1 if not).
+__global__ void detect_ploidy_words_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t window,
+                                           int64_t n_ind, const int32_t* __restrict__ pos, uint32_t* __restrict__ sel) {
+    const int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (16 * w >= n_ind) return;  // warp-uniform
+    uint32_t het = 0;
+    for (int64_t s = lane; s < window; s += 32) {
+        const uint32_t x = __ldg(reinterpret_cast<const uint32_t*>(records + s * pitch) + w);
+        het |= (x & 0x55555555u) & ~((x >> 1) & 0x55555555u);
+    }
+    het = __reduce_or_sync(0xffffffffu, het);
+    const int64_t row = 16 * w + lane;
+    if (lane < 16 && row < n_ind) {
+        const int32_t g = __ldg(pos + row);
+        if (g >= 0) {
+            const bool h = (het >> (8 * (lane >> 2) + 6 - 2 * (lane & 3))) & 1u;
+            sel[g] = (sel[g] & ~3u) | (h ? 2u : 1u);
+        }
+    }
+}
+}  // namespace
+
+void launch_detect_ploidy_words(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_snp, int64_t n_ind,
+                                const int32_t* pos, uint32_t* sel, cudaStream_t s) {
+    if (n_ind <= 0 || n_snp <= 0) return;
+    if (pitch % 4 != 0 || reinterpret_cast<uintptr_t>(records) % 4 != 0)
+        fail(STP_INVALID_ARGUMENT, "word-wise ploidy detection needs 4-byte aligned records and pitch");
+    const int64_t window = n_snp < kPloidyWindow ? n_snp : kPloidyWindow;
+    const int64_t warps = (n_ind + 15) / 16;
+    detect_ploidy_words_kernel<<<static_cast<unsigned>((warps + 7) / 8), 256, 0, s>>>(records, pitch, window, n_ind, pos, sel);
+    STPF2_CUDA(cudaGetLastError());
+    c.launches++;
+}
+
 void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_snp,
                              uint32_t* sel, int64_t n_sel, cudaStream_t s) {
     if (n_sel <= 0) return;

@@ -142,7 +142,7 @@ void noalloc_decode_counts(Ctx& c, const uint8_t* d_records, uint64_t pitch, int
         n_snp, n_tiles, d_tiles, d_col_snp, d_po64, d_po32, P);
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
-    if (detect) launch_detect_ploidy_pa(c, d_records, pitch, n_snp, d_desc, n_sel, s);
+    if (detect) launch_detect_ploidy_words(c, d_records, pitch, n_snp, n_ind, d_pos, d_desc, s);
     launch_transpose_pa(c, d_records, pitch, n_ind, d_tiles, n_tiles, d_pos, n_sel_pad, d_canon, d_center, s);
     CanonDecodeArgs a;
     a.canon = d_canon;

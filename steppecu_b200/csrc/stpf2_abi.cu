@@ -342,7 +342,8 @@ void launch_decode(Plan& p, const uint8_t* d_records, int32_t* cnt_ac2, int32_t*
                                      static_cast<size_t>(p.n_snp), cudaMemcpyDeviceToDevice, s));
         rec = p.repitched.as<uint8_t>();
     }
-    if (p.detect && detect) launch_detect_ploidy_pa(c, rec, p.pitch, p.n_snp, p.sel.as<uint32_t>(), p.n_sel, s);
+    if (p.detect && detect)
+        launch_detect_ploidy_words(c, rec, p.pitch, p.n_snp, p.n_ind, p.pos.as<int32_t>(), p.sel.as<uint32_t>(), s);
     if (t1 <= t0) return;
     launch_transpose_pa(c, rec, p.pitch, p.n_ind, p.tiles.as<TileInfo>() + t0, t1 - t0, p.pos.as<int32_t>(),
                         p.n_sel_pad, p.canon_ptr, p.center_ptr + t0 * kTileK, s);
@@ -732,7 +733,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
     launch_timestamp(c, d_t0, s);
     launch_layout_tables(c, reinterpret_cast<BlockInfo*>(U + o_one), reinterpret_cast<int64_t*>(U + o_zero), 1,
                          n_utiles * kTileK, d_cols_u, d_tiles_u, s);
-    if (any_auto) launch_detect_ploidy_pa(c, d_rec, pitch, M, d_desc_u, n_u, s);
+    if (any_auto) launch_detect_ploidy_words(c, d_rec, pitch, M, n_ind, d_pos_u, d_desc_u, s);
     launch_transpose_pa(c, d_rec, pitch, n_ind, d_tiles_u, n_utiles, d_pos_u, n_u_pad, d_canon_u, d_center_u, s);
 
     // Host tables of every request, in parallel, while the device runs the shared passes.

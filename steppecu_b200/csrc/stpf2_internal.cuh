@@ -264,6 +264,10 @@ struct CanonDecodeArgs {
     int64_t cnt_ld = 0;
 };
 
+// Ploidy detection over 4-byte record words (records and pitch 4-byte aligned); pos maps
+// file rows to selected indices (-1: not selected), each row selected once.
+void launch_detect_ploidy_words(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_snp, int64_t n_ind,
+                                const int32_t* pos, uint32_t* sel, cudaStream_t s);
 void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_snp,
                              uint32_t* sel, int64_t n_sel, cudaStream_t s);
 void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_ind, const TileInfo* tiles,
