@@ -215,6 +215,68 @@ def run_e2e(args, ctx, rec, panel, sel, po, bpr, n_out, barrier, dist, dev, P, M
     return e2e
 
 
+def run_config(workload: str, dev: str, modes, steps: int = 3, per_block: bool = False,
+               precision_threads: int = 0) -> dict:
+    """One of the other panel configs at full size on the device (records resident in HBM):
+    each arithmetic as one persistent launch over all blocks, optionally also one launch per
+    block, and optionally its precision against the CPU reference on a bounded block sample."""
+    import torch
+
+    import steppecu_b200 as sb
+    from steppecu_b200 import synth
+
+    panel = synth.generate(workload, seed=20261203 + 100 + int(workload[1]), device=dev)
+    sel, po = panel.selection()
+    P, M, B = panel.n_pop, panel.n_snp, panel.n_block
+    bpr = panel.bytes_per_record
+    pitch = (bpr + 15) // 16 * 16
+    rec = torch.zeros((M, pitch), dtype=torch.uint8, device=dev)
+    rec[:, :bpr] = panel.records
+    panel.records = None
+    f2 = torch.empty(P * P * B, dtype=torch.float64, device=dev)
+    vp = torch.empty_like(f2)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = sb.Context(int(dev.split(":")[1]) if ":" in dev else 0)
+    counts = torch.bincount(torch.as_tensor(panel.block_id), minlength=B)
+    out = {"populations": P, "samples": panel.n_ind, "snps": M, "blocks": B,
+           "block_snps": {"min": int(counts.min()), "median": int(counts.median()), "max": int(counts.max())}}
+
+    def timed(plan, n):
+        plan.run(rec, f2, vp, stream.cuda_stream)
+        torch.cuda.synchronize()
+        plan.set_timing(True)
+        l0 = ctx.launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            plan.run(rec, f2, vp, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dec, con = plan.last_times()
+        plan.set_timing(False)
+        return e0.elapsed_time(e1) / n, dec, con, (ctx.launches - l0) / n
+
+    for mode in modes:
+        plan = ctx.plan(rec, panel.n_ind, sel, po, panel.block_id, B, precision=mode)
+        ms, dec, con, nl = timed(plan, steps)
+        r = {"value": units(P, M) / (ms / 1e3), "ms_per_step": ms, "decode_ms": dec, "contract_ms": con,
+             "launches_per_step": nl}
+        if per_block and mode != "fp32":
+            plan.set_per_block_launch(True)
+            ms_b, _, con_b, nl_b = timed(plan, steps)
+            plan.set_per_block_launch(False)
+            r["per_block_launches"] = {"ms_per_step": ms_b, "contract_ms": con_b, "launches_per_step": nl_b,
+                                       "persistent_speedup": ms_b / ms}
+        plan.close()
+        out[mode] = r
+    if precision_threads:
+        u, t, kind, desc, sample = cpu_sample(workload, precision_threads, gen_device=dev, keep=True)
+        out["cpu_baseline"] = {"value": u / t, "unit": UNIT, "cores": precision_threads, "kind": kind, "sample": desc}
+        out["precision"] = precision_report(ctx, sample, modes)
+    ctx.close()
+    return out
+
+
 def run_batched(dev: str, steps: int = 3, n_req: int = 64, serial_baselines: bool = True) -> dict:
     """Many requests over one shared panel (8,000 samples x 1.15M SNPs, 64 requests of
     4-300 populations, each with its own 5 cM block map): one grouped stp_f2_extract_batch
@@ -325,6 +387,8 @@ def main():
     ap.add_argument("--quick", action="store_true", help="headline timing only: no other arithmetics, e2e or CPU leg")
     ap.add_argument("--no-batched", dest="batched", action="store_false",
                     help="skip the many-requests (grouped batch) measurement")
+    ap.add_argument("--no-other-configs", dest="other_configs", action="store_false",
+                    help="skip the 100-population and uneven-block config measurements")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -489,6 +553,16 @@ def main():
         modes = [args.precision] + [m for m in ("split_f16_fine", "split_bf16", "fp32") if m != args.precision]
         precision = {"against": f"{kind} CPU f2 on the cpu_baseline sample", **precision_report(ctx, sample, modes)}
 
+    other_configs = None
+    if world == 1 and not args.quick and args.other_configs:
+        # The full-panel plain GPU form (100 pops x 20) and the uneven-blocks config (1,000
+        # lognormal pops, lognormal blocks): full size, records in HBM.
+        threads = args.cpu_threads or (os.cpu_count() or 1)
+        other_configs = {
+            "c2": run_config("c2", dev, ["fp32", "split_f16"], precision_threads=threads),
+            "c4": run_config("c4", dev, ["split_f16", "split_bf16"], per_block=True),
+        }
+
     batched = None
     if world == 1 and not args.quick and args.batched:
         plan.close()
@@ -514,6 +588,7 @@ def main():
             "other_arithmetics": others,
             "per_block_launches": per_block,
             "batched_requests": batched,
+            "other_configs": other_configs,
         }
         print(json.dumps(line), flush=True)
     if batched is None:
