@@ -159,6 +159,14 @@ def precision_report(ctx, sample, modes) -> dict:
                      "max_rel_f2_ge_0.01": float((d[sig] / a[sig]).max()),
                      "frac_f2_ge_0.01": float(sig.mean()),
                      "vpair_bit_exact": bool(np.array_equal(t.vpair, vp_ref))}
+        if mode == modes[0]:
+            # Per jackknife block of the sample (slab b = the block's P x P values).
+            slab = p.n_pop * p.n_pop
+            db, ab, sb = d.reshape(nb, slab), a.reshape(nb, slab), sig.reshape(nb, slab)
+            out[mode]["per_block"] = {
+                "max_abs": [float(x) for x in db.max(axis=1)],
+                "max_rel_f2_ge_0.01": [float((db[b][sb[b]] / ab[b][sb[b]]).max(initial=0.0)) for b in range(nb)],
+            }
     return out
 
 
