@@ -77,6 +77,7 @@ struct UmmaArgs {
     int rcp_max;
     int* err;
     int* next_item;    // work-item counter, zero at launch
+    int b_base;        // block id whose slab starts the output buffers (0: the whole tensor)
     uint32_t idesc_pp, idesc_am, idesc_i8;
     // Grouped launch (a batch of requests): per-request images and outputs, indexed by
     // BlockInfo::grp; null for one request (images, n_ck, P, f2, vpair above). Optional
@@ -399,7 +400,7 @@ __device__ __forceinline__ ItemOut item_out(const UmmaArgs& a, int it, int r, in
     o.i = w.ti * kTile + r;
     o.i0 = w.ti * kTile + (r & ~31);
     o.j0 = w.tj * kTile + h * kCols;
-    o.slab = static_cast<int64_t>(o.P) * o.P * bi.b;
+    o.slab = static_cast<int64_t>(o.P) * o.P * (bi.b - a.b_base);
     return o;
 }
 
@@ -699,7 +700,7 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
 void umma_plan_destroy(UmmaPlan* p) { delete p; }
 
 void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, double* f2, double* vpair,
-                       cudaStream_t s);
+                       cudaStream_t s, int b_base = 0);
 
 void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s, bool per_block) {
     if (!p || p->n_items <= 0) return;
@@ -713,16 +714,19 @@ void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t
     launch_umma_items(c, p, p->items.as<WorkItem>(), p->n_items, f2, vpair, s);
 }
 
-void launch_f2_umma_blocks(Ctx& c, UmmaPlan* p, int b0, int b1, double* f2, double* vpair, cudaStream_t s) {
+void launch_f2_umma_blocks(Ctx& c, UmmaPlan* p, int b0, int b1, double* f2, double* vpair, cudaStream_t s,
+                           bool rebase) {
     if (!p || b1 <= b0) return;
     const int n = p->block_item_off[static_cast<size_t>(b1)] - p->block_item_off[static_cast<size_t>(b0)];
     if (n > 0)
-        launch_umma_items(c, p, p->block_items.as<WorkItem>() + p->block_item_off[static_cast<size_t>(b0)], n, f2, vpair, s);
+        launch_umma_items(c, p, p->block_items.as<WorkItem>() + p->block_item_off[static_cast<size_t>(b0)], n, f2, vpair, s,
+                          rebase ? b0 : 0);
 }
 
 void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, double* f2, double* vpair,
-                       cudaStream_t s) {
+                       cudaStream_t s, int b_base) {
     UmmaArgs a{};
+    a.b_base = b_base;
     a.images = p->images;
     a.n_ck = p->n_ck;
     a.items = items;

@@ -426,9 +426,11 @@ void upload_rows(const stp_geno_view& g, uint8_t* d, uint64_t dp, int64_t s0, in
 // upload of segment k+1, the decode and contraction of segment k and the download of
 // segment k-1's f2 / vpair slabs overlap on three streams. A segment's records are a
 // contiguous run of SNP rows, its operand columns a tile range, its output a contiguous
-// run of block slabs.
-void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, uint8_t* d_rec, uint64_t dp,
-                   double* d_f2, double* d_vp) {
+// run of block slabs. The device holds only two segments' slabs (a ring: segment k's
+// contraction waits for the download of segment k-2 from the same buffer), so the output
+// tensor itself may exceed device memory (the out-of-core tier: only the host holds all
+// P x P x B slabs).
+void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, uint8_t* d_rec, uint64_t dp) {
     const BlockLayout& L = p.L;
     const int B = L.n_block;
     const int64_t M = L.n_snp;
@@ -446,7 +448,11 @@ void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, u
     }
     bounds.push_back(B);
     const size_t nseg = bounds.size() - 1;
-    std::vector<cudaEvent_t> ev(2 * nseg, nullptr);
+    size_t ring = 1;  // slabs per ring buffer: the largest segment
+    for (size_t k = 0; k < nseg; ++k) ring = std::max<size_t>(ring, static_cast<size_t>(bounds[k + 1] - bounds[k]));
+    c.ws_f2.reserve(2 * ring * slab * sizeof(double));
+    c.ws_vpair.reserve(2 * ring * slab * sizeof(double));
+    std::vector<cudaEvent_t> ev(3 * nseg, nullptr);  // per segment: uploaded, contracted, downloaded
     struct Free {
         std::vector<cudaEvent_t>& ev;
         ~Free() {
@@ -462,16 +468,20 @@ void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, u
         for (int b = b0; b < b1; ++b) nsnp += L.blocks[b].k;
         const int64_t t0 = L.blocks[b0].col / kTileK;
         const int64_t t1 = (b1 < B ? L.blocks[b1].col : L.ld) / kTileK;
+        double* f2k = c.ws_f2.as<double>() + (k % 2) * ring * slab;
+        double* vpk = c.ws_vpair.as<double>() + (k % 2) * ring * slab;
         upload_rows(r.geno, d_rec, dp, snp0, nsnp, c.h2d);
-        STPF2_CUDA(cudaEventRecord(ev[2 * k], c.h2d));
-        STPF2_CUDA(cudaStreamWaitEvent(c.stream, ev[2 * k], 0));
+        STPF2_CUDA(cudaEventRecord(ev[3 * k], c.h2d));
+        STPF2_CUDA(cudaStreamWaitEvent(c.stream, ev[3 * k], 0));
         launch_decode(p, d_rec, nullptr, nullptr, c.stream, t0, t1, k == 0);
-        launch_f2_umma_blocks(c, p.umma, b0, b1, d_f2, d_vp, c.stream);
-        STPF2_CUDA(cudaEventRecord(ev[2 * k + 1], c.stream));
-        STPF2_CUDA(cudaStreamWaitEvent(c.d2h, ev[2 * k + 1], 0));
+        if (k >= 2) STPF2_CUDA(cudaStreamWaitEvent(c.stream, ev[3 * (k - 2) + 2], 0));  // ring buffer free
+        launch_f2_umma_blocks(c, p.umma, b0, b1, f2k, vpk, c.stream, true);
+        STPF2_CUDA(cudaEventRecord(ev[3 * k + 1], c.stream));
+        STPF2_CUDA(cudaStreamWaitEvent(c.d2h, ev[3 * k + 1], 0));
         const size_t bytes = slab * static_cast<size_t>(b1 - b0) * sizeof(double);
-        STPF2_CUDA(cudaMemcpyAsync(o.f2 + slab * b0, d_f2 + slab * b0, bytes, cudaMemcpyDeviceToHost, c.d2h));
-        STPF2_CUDA(cudaMemcpyAsync(o.vpair + slab * b0, d_vp + slab * b0, bytes, cudaMemcpyDeviceToHost, c.d2h));
+        STPF2_CUDA(cudaMemcpyAsync(o.f2 + slab * b0, f2k, bytes, cudaMemcpyDeviceToHost, c.d2h));
+        STPF2_CUDA(cudaMemcpyAsync(o.vpair + slab * b0, vpk, bytes, cudaMemcpyDeviceToHost, c.d2h));
+        STPF2_CUDA(cudaEventRecord(ev[3 * k + 2], c.d2h));
         snp0 += nsnp;
     }
     STPF2_CUDA(cudaStreamSynchronize(c.d2h));
@@ -505,18 +515,18 @@ void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
     std::unique_ptr<Plan> p = build_plan(c, r, pitch, c.ws_misc.ptr, true);
     if (o.block_sizes) copy_block_sizes(p->L, o.block_sizes);
     const size_t out_elems = static_cast<size_t>(std::max(r.n_pop, 0)) * std::max(r.n_pop, 0) * std::max(r.n_block, 0);
-    double* d_f2 = o.f2;
-    double* d_vp = o.vpair;
-    if (!o.on_device && out_elems) {
-        c.ws_f2.reserve(out_elems * sizeof(double));
-        c.ws_vpair.reserve(out_elems * sizeof(double));
-        d_f2 = c.ws_f2.as<double>();
-        d_vp = c.ws_vpair.as<double>();
-    }
     if (pipelined && p->umma && !p->repitch && out_elems) {
         STPF2_CUDA(cudaStreamSynchronize(s));  // the plan's tables are uploaded on s
-        run_pipelined(c, r, o, *p, c.ws_records.as<uint8_t>(), dp, d_f2, d_vp);
+        run_pipelined(c, r, o, *p, c.ws_records.as<uint8_t>(), dp);
     } else {
+        double* d_f2 = o.f2;
+        double* d_vp = o.vpair;
+        if (!o.on_device && out_elems) {
+            c.ws_f2.reserve(out_elems * sizeof(double));
+            c.ws_vpair.reserve(out_elems * sizeof(double));
+            d_f2 = c.ws_f2.as<double>();
+            d_vp = c.ws_vpair.as<double>();
+        }
         if (pipelined) upload_rows(r.geno, c.ws_records.as<uint8_t>(), dp, 0, r.geno.n_snp, s);
         run_plan(*p, d_rec, d_f2, d_vp, s);
         if (!o.on_device && out_elems) {

@@ -323,7 +323,10 @@ void umma_plan_destroy(UmmaPlan* p);
 // blocks (the comparison form of the grouped schedule).
 void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s, bool per_block = false);
 // The tile pairs of blocks [b0, b1) only, in one launch.
-void launch_f2_umma_blocks(Ctx& c, UmmaPlan* p, int b0, int b1, double* f2, double* vpair, cudaStream_t s);
+// Blocks [b0, b1) only; rebase: f2 / vpair point at block b0's slab (a buffer of b1 - b0
+// slabs) instead of the whole tensor.
+void launch_f2_umma_blocks(Ctx& c, UmmaPlan* p, int b0, int b1, double* f2, double* vpair, cudaStream_t s,
+                           bool rebase = false);
 // After a stream sync: raises STP_DEVICE_TIMEOUT if the kernel's bounded waits expired.
 void umma_check(UmmaPlan* p);
 int umma_tile();

@@ -318,3 +318,30 @@ def test_extract_f2_files_roundtrip(tmp_path, c1):
     assert_f2_close(h.tensor, want, MODES[-1])
     h2 = extract_f2(tmp_path / "panel", pops=pops, maxmiss=1.0, precision=MODES[-1])
     assert np.array_equal(h2.to_numpy(), h.to_numpy())
+
+
+def test_host_streaming_bounds_device_output_memory():
+    """Host records and host outputs stream in segments of whole blocks through a two-segment
+    ring of device slabs: the result equals the device-output extraction bit for bit, and the
+    device memory the call takes stays well below the F2BlockTensor it returns."""
+    import torch
+
+    from steppecu_b200 import Context
+
+    p = synth.generate("c3", seed=5, n_snp=20_000, n_pop=600)
+    sel, po = p.selection()
+    rec = p.records_numpy()
+    P, B = p.n_pop, p.n_block
+    full = 2 * P * P * B * 8
+    with Context(0) as c:
+        free0 = torch.cuda.mem_get_info(0)[0]
+        t = c.extract_blocks(rec, p.n_ind, sel, po, p.block_id, B, precision="split_f16")
+        taken = free0 - torch.cuda.mem_get_info(0)[0]
+    assert taken < 0.5 * full, (taken, full)
+    f2d = torch.zeros(P * P * B, dtype=torch.float64, device="cuda")
+    vpd = torch.zeros_like(f2d)
+    with Context(0) as c:
+        c.extract_blocks(torch.from_numpy(rec).cuda(), p.n_ind, sel, po, p.block_id, B, precision="split_f16",
+                         out=(f2d, vpd))
+    assert np.array_equal(t.f2, f2d.cpu().numpy())
+    assert np.array_equal(t.vpair, vpd.cpu().numpy())
