@@ -1,14 +1,17 @@
 // steppecu_b200/csrc/decode.cu
 //
-// Genotype decode for the f2 path (sm_100a). The hot kernel, decode_pa_kernel, reads
-// SNP-major PACKEDANCESTRYMAP records straight from HBM (coalesced 128-bit loads into a
-// shared-memory tile of 32 records), folds every selected sample of every population into
-// exact integer counts (ac2 = 2*ac, n) following decode_af.hpp:58-65, and writes the
-// contraction operands for those counts directly into the block-padded planes the
-// contraction kernels read. Also here: per-sample ploidy detection (detect_ploidy_kernel.cu
-// :32-57), the canonical-tile decode behind ComputeBackend::decode_af (cpu_backend.cpp
-// :267-319) and the Q/V/N feeder behind compute_f2_blocks(MatView...) (f2_block_kernel.cu
-// :37-61 computes the same per-element terms).
+// Genotype decode for the f2 path (sm_100a), in two passes over an intermediate canonical
+// copy of the selected samples' genotypes. transpose_pa_kernel reads the SNP-major
+// PACKEDANCESTRYMAP records from HBM in staged slices and writes each selected sample's
+// codes for 128 columns as one 32-byte sector (plus a per-column centre);
+// decode_canon_kernel folds every selected sample of every population into exact integer
+// counts (ac2 = 2*ac, n) following decode_af.hpp:58-65 and writes the contraction operands
+// for those counts straight into the block-padded tile images the contraction kernels read.
+// Also here: per-sample ploidy detection (detect_ploidy_kernel.cu:32-57), the
+// canonical-tile decode behind ComputeBackend::decode_af (cpu_backend.cpp:267-319), the
+// operand emit from packed counts used by grouped batches, and the Q/V/N feeder behind
+// compute_f2_blocks(MatView...) (f2_block_kernel.cu:37-61 computes the same per-element
+// terms).
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 

@@ -10,7 +10,8 @@
 //   warp 1      TMEM owner + single-thread tcgen05.mma issuer. Per 16-SNP K step, seven
 //               kind::f16 MMAs accumulate num/2 = sum(Ah_i M_j + M_i Ah_j - Pt_i Pt_j) over
 //               the hi/lo splits (the -Pt Pt products use the descriptor's A-negate bit)
-//               into one FP32 TMEM buffer per 32-SNP chunk; one kind::i8 MMA per stage
+//               into one FP32 TMEM buffer per chunk (64 SNPs = two stages; 32 SNPs in the
+//               fine mode); one kind::i8 MMA per stage
 //               accumulates the exact both-present count M M^T into an int32 TMEM buffer.
 //   warps 2-17  epilogue, four warps per TMEM lane quarter, 32 tile columns each: drains
 //               the FP32 chunks two at a time into FP64 registers (one round-to-nearest FP32
