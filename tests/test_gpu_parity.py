@@ -113,6 +113,26 @@ def test_decode_counts_device_records(ctx, uneven):
     assert np.array_equal(ac2, wa.reshape(-1, P).T) and np.array_equal(n, wn.reshape(-1, P).T)
 
 
+@pytest.mark.parametrize("panel_pops,n_snp", [(1232, 4001), (1250, 4000)])
+def test_wide_panel_scattered_selection(ctx, panel_pops, n_snp):
+    """40 scattered populations, in descending order, from panels of 12,320 and 12,500
+    samples. 12,320 samples give 3,080-byte records, a multiple of 4 bytes but not of 16,
+    which the transpose reads at their own pitch with 4-byte copies; 12,500 samples give
+    3,125-byte records, which are re-pitched to 16 bytes first. Counts bit-exact, f2 within
+    tolerance."""
+    p = synth.generate("c3", seed=panel_pops + n_snp, n_snp=n_snp, n_pop=panel_pops)
+    sel, po = p.selection(list(range(panel_pops - 1, -1, -31))[:40])
+    rec = p.records_numpy()
+    P = len(po) - 1
+    pl = oracle.detect_ploidy_pa(rec, sel)
+    ac2, n = ctx.decode_counts(rec, p.n_ind, sel, po)
+    wa, wn = oracle.decode_counts_pa(rec, sel, po, pl)
+    assert np.array_equal(ac2, wa.reshape(-1, P).T) and np.array_equal(n, wn.reshape(-1, P).T)
+    want, _ = oracle_f2(p, sel, po, ploidy=pl)
+    got = ctx.extract_blocks(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision=TC_DEFAULT)
+    assert_f2_close(got, want, TC_DEFAULT)
+
+
 @pytest.mark.parametrize("size,n_pop,n_snp", [(250, 5, 3000), (16383, 1, 300)])
 def test_decode_counts_large_populations(ctx, size, n_pop, n_snp):
     """Populations far above the decode's in-register sample window, up to the largest
