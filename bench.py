@@ -42,6 +42,28 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 CONTRACTION_TRAFFIC = {("c3", "split_f16"): 13.58e9 + 12.24e9}
 
 
+def issued_tensor_work(P: int, block_id, n_block: int, con_ms: float, peak: float) -> dict:
+    """Tensor work one split-arithmetic contraction launch issues, over its measured time.
+
+    Every 32-SNP stage of a 128 x 128 tile pair (ti <= tj) issues 14 kind::f16 MMAs of
+    128 x 128 x 16 (seven hi/lo products per 16 SNPs) and one kind::i8 MMA of 128 x 128 x 32
+    (the exact vpair count). The algorithmic 6 * P^2 * M counts the full square of useful
+    products once; the issued figure counts the split products, the triangle of tile pairs
+    and the padding of P to tiles and of blocks to stages: it is what the tensor pipe runs.
+    """
+    import numpy as np
+
+    k = np.bincount(np.asarray(block_id, np.int64), minlength=n_block)
+    stages = int(((k + 31) // 32).sum())
+    rt = (P + 127) // 128
+    pairs = rt * (rt + 1) // 2
+    f16 = pairs * stages * 14 * 2.0 * 128 * 128 * 16
+    i8 = pairs * stages * 2.0 * 128 * 128 * 32
+    sec = con_ms / 1000.0
+    return {"f16_flops": f16, "i8_ops": i8, "f16_tflops": f16 / sec / 1e12, "f16_frac": f16 / sec / 1e12 / peak,
+            "i8_tops": i8 / sec / 1e12}
+
+
 def load_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -545,13 +567,15 @@ def main():
     flops = 6.0 * P * P * M
     achieved = flops / (con_ms / 1000.0) / 1e12
     peak = float(peaks.get("bf16_tflops", PEAKS_FALLBACK["bf16_tflops"]))
-    # DRAM bytes (read + write) of one contraction launch on this workload, from the ncu
-    # capture summarised in profiles/traffic_full_workload_1000pops_1.15M_snps.md.
+    # DRAM bytes (read + write) of one contraction launch on this workload, from one ncu
+    # capture of it (summarised under profiles/).
     traffic = CONTRACTION_TRAFFIC.get((args.workload, args.precision)) if args.snps is None else None
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                 "kernel_ms": con_ms, "decode_ms": dec_ms,
                 "decode_hbm_gbs": (M * bpr + 11 * P * M) / (dec_ms / 1000.0) / 1e9}
+    if args.precision != "fp32":
+        roofline["issued"] = issued_tensor_work(P, panel.block_id, B, con_ms, peak)
 
     cpu = None
     precision = None
