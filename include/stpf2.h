@@ -168,7 +168,11 @@ stp_status stp_f2_from_qvn(stp_ctx* ctx, const double* Q, const double* V, const
                            int32_t precision, double* f2, double* vpair, int32_t* block_sizes);
 
 /* The extract-f2 hot path: packed genotypes -> ploidy -> decode -> per-block contraction
- * -> FP64 F2BlockTensor (src/app/extract_f2_core.cpp:93-407, Resident tier). */
+ * -> FP64 F2BlockTensor (src/app/extract_f2_core.cpp:93-407, Resident tier). With host
+ * records and host outputs on the tensor cores, the call streams segments of whole blocks
+ * and downloads only the upper 128-row bands of each (exactly symmetric) slab; it fills
+ * the lower tiles of the host outputs itself, on up to hardware_concurrency host threads,
+ * before it returns. */
 stp_status stp_f2_extract_blocks(stp_ctx* ctx, const stp_f2_request* req, stp_f2_output* out);
 
 /* Many independent requests (each its own populations and block map). The reference runs

@@ -1,7 +1,7 @@
 """Build recipe for the native parts of steppecu_b200.
 
-- ``libstpf2.so``: every CUDA source in ``csrc/`` compiled for sm_100a (B200) only, with
-  the CUDA runtime linked statically, so the library needs nothing from torch.
+- ``libstpf2.so``: every CUDA source in ``csrc/`` compiled for sm_100a (B200) only (and the
+  host-only ``.cpp`` sources there), with the CUDA runtime linked statically, so the library needs nothing from torch.
 - ``oracle/``: the CPU checkers (``make -C oracle``); the reference's own CpuBackend is
   built there too when the reference sources are present.
 
@@ -47,7 +47,7 @@ def build_lib(verbose: bool = False, extra: list[str] | None = None) -> Path:
     nvcc = _nvcc()
     BUILD.mkdir(exist_ok=True)
     headers = sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "stpf2.h"]
-    srcs = sorted(CSRC.glob("*.cu"))
+    srcs = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))  # .cpp: host-only sources
     flags = NVFLAGS + (extra or [])
 
     def compile_one(src: Path) -> Path:

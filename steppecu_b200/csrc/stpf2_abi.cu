@@ -421,6 +421,45 @@ void upload_rows(const stp_geno_view& g, uint8_t* d, uint64_t dp, int64_t s0, in
     }
 }
 
+// Runs f(i) for i in [0, n) on up to hardware_concurrency threads; rethrows the first error.
+template <class F>
+void parallel_for(int n, F&& f) {
+    const int nt = std::max(1, std::min<int>(n, static_cast<int>(std::thread::hardware_concurrency())));
+    std::atomic<int> next{0};
+    std::vector<std::exception_ptr> errs(static_cast<size_t>(nt));
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            try {
+                for (int i = next++; i < n; i = next++) f(i);
+            } catch (...) {
+                errs[t] = std::current_exception();
+            }
+        });
+    for (auto& x : th) x.join();
+    for (auto& e : errs)
+        if (e) std::rethrow_exception(e);
+}
+
+// Copies the upper row bands of slabs [0, nb) of a device slab run into the host run: per
+// row tile, one 3-D copy of rows [r0, r0 + T) x columns [r0, P) x every slab.
+void download_upper_bands(double* host, const double* dev, int64_t P, int64_t T, int64_t nb, cudaStream_t st) {
+    for (int64_t r0 = 0; r0 < P; r0 += T) {
+        const int64_t nr = std::min(T, P - r0);
+        cudaMemcpy3DParms m{};
+        m.srcPtr = make_cudaPitchedPtr(const_cast<double*>(dev), static_cast<size_t>(P) * sizeof(double),
+                                       static_cast<size_t>(P) * sizeof(double), static_cast<size_t>(P));
+        m.dstPtr = make_cudaPitchedPtr(host, static_cast<size_t>(P) * sizeof(double),
+                                       static_cast<size_t>(P) * sizeof(double), static_cast<size_t>(P));
+        m.srcPos = make_cudaPos(static_cast<size_t>(r0) * sizeof(double), static_cast<size_t>(r0), 0);
+        m.dstPos = m.srcPos;
+        m.extent = make_cudaExtent(static_cast<size_t>(nr) * sizeof(double), static_cast<size_t>(P - r0),
+                                   static_cast<size_t>(nb));
+        m.kind = cudaMemcpyDeviceToHost;
+        STPF2_CUDA(cudaMemcpy3DAsync(&m, st));
+    }
+}
+
 // Host buffers in and out, tensor-core arithmetic: the pass runs in segments of whole
 // blocks (about a twelfth of the SNPs each, the first covering the ploidy window) so the
 // upload of segment k+1, the decode and contraction of segment k and the download of
@@ -431,6 +470,7 @@ void upload_rows(const stp_geno_view& g, uint8_t* d, uint64_t dp, int64_t s0, in
 // tensor itself may exceed device memory (the out-of-core tier: only the host holds all
 // P x P x B slabs).
 void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, uint8_t* d_rec, uint64_t dp) {
+    constexpr int64_t kBand = 128;  // rows per downloaded band (one contraction tile)
     const BlockLayout& L = p.L;
     const int B = L.n_block;
     const int64_t M = L.n_snp;
@@ -478,11 +518,21 @@ void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, u
         launch_f2_umma_blocks(c, p.umma, b0, b1, f2k, vpk, c.stream, true);
         STPF2_CUDA(cudaEventRecord(ev[3 * k + 1], c.stream));
         STPF2_CUDA(cudaStreamWaitEvent(c.d2h, ev[3 * k + 1], 0));
-        const size_t bytes = slab * static_cast<size_t>(b1 - b0) * sizeof(double);
-        STPF2_CUDA(cudaMemcpyAsync(o.f2 + slab * b0, f2k, bytes, cudaMemcpyDeviceToHost, c.d2h));
-        STPF2_CUDA(cudaMemcpyAsync(o.vpair + slab * b0, vpk, bytes, cudaMemcpyDeviceToHost, c.d2h));
+        download_upper_bands(o.f2 + slab * b0, f2k, p.P, kBand, b1 - b0, c.d2h);
+        download_upper_bands(o.vpair + slab * b0, vpk, p.P, kBand, b1 - b0, c.d2h);
         STPF2_CUDA(cudaEventRecord(ev[3 * k + 2], c.d2h));
         snp0 += nsnp;
+    }
+    // Every slab is exactly symmetric (the contraction stores one value at (i, j) and
+    // (j, i)), so only its upper row bands crossed PCIe; the host fills the lower tiles of
+    // each segment once its download has landed, while later segments are still in flight.
+    for (size_t k = 0; k < nseg; ++k) {
+        STPF2_CUDA(cudaEventSynchronize(ev[3 * k + 2]));
+        const int b0 = bounds[k], nb = bounds[k + 1] - bounds[k];
+        parallel_for(2 * nb, [&](int u) {
+            double* base = (u % 2 == 0) ? o.f2 : o.vpair;
+            mirror_lower_tiles(base + slab * static_cast<size_t>(b0 + u / 2), p.P, kBand);
+        });
     }
     STPF2_CUDA(cudaStreamSynchronize(c.d2h));
     STPF2_CUDA(cudaStreamSynchronize(c.stream));
@@ -614,25 +664,6 @@ void prepare_member(const stp_f2_request& r, const stp_f2_output& o, int64_t n_i
     m.out_bytes = o.on_device ? 0 : 2 * align256(elems * sizeof(double));
 }
 
-// Runs f(i) for i in [0, n) on up to hardware_concurrency threads; rethrows the first error.
-template <class F>
-void parallel_for(int n, F&& f) {
-    const int nt = std::max(1, std::min<int>(n, static_cast<int>(std::thread::hardware_concurrency())));
-    std::atomic<int> next{0};
-    std::vector<std::exception_ptr> errs(static_cast<size_t>(nt));
-    std::vector<std::thread> th;
-    for (int t = 0; t < nt; ++t)
-        th.emplace_back([&, t] {
-            try {
-                for (int i = next++; i < n; i = next++) f(i);
-            } catch (...) {
-                errs[t] = std::current_exception();
-            }
-        });
-    for (auto& x : th) x.join();
-    for (auto& e : errs)
-        if (e) std::rethrow_exception(e);
-}
 
 // A batch of requests over one panel, all on the tensor cores with one arithmetic:
 //   1. the union of their samples goes through one ploidy pass and one transpose into

@@ -337,6 +337,10 @@ void launch_fstat_assemble(Ctx& c, const double* f2, int P, const int32_t* surv,
 void launch_jackknife(Ctx& c, const double* x, const int32_t* block_sizes, int64_t m, int nb,
                       double* est, double* var, cudaStream_t s);
 
+// Fills the lower tiles of a symmetric P x P column-major slab whose upper row bands of T
+// rows (band t: rows [t*T, t*T + T) x columns [t*T, P)) are in place (host_mirror.cpp).
+void mirror_lower_tiles(double* S, int64_t P, int64_t T);
+
 // Allocation-free count decode (noalloc.cu): every intermediate lives in one static
 // device array of kNoAllocScratchBytes.
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;

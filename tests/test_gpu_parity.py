@@ -340,6 +340,42 @@ def test_extract_f2_files_roundtrip(tmp_path, c1):
     assert np.array_equal(h2.to_numpy(), h.to_numpy())
 
 
+@pytest.mark.parametrize("n_pop,misalign", [(600, False), (603, False), (600, True)])
+def test_host_band_download_equals_device_output(n_pop, misalign):
+    """Host outputs receive only the upper 128-row bands of each slab over PCIe and the
+    library fills the lower tiles on the host: with 4 x 4 register transposes when P % 4 == 0
+    and the output is 32-byte aligned, else with scalar copies (P = 603, and an output that
+    starts 8 bytes past an aligned address). Each equals the device-output extraction bit
+    for bit."""
+    import torch
+
+    from steppecu_b200 import Context
+
+    p = synth.generate("c3", seed=n_pop, n_snp=6_000, n_pop=n_pop)
+    sel, po = p.selection()
+    rec = p.records_numpy()
+    P, B = p.n_pop, p.n_block
+    n = P * P * B
+    if misalign:  # both outputs start 8 bytes past a 32-byte boundary
+        def at8(m):
+            buf = np.zeros(m + 4)
+            off = ((8 - buf.ctypes.data) % 32) // 8
+            return buf[off:off + m]
+
+        f2h, vph = at8(n), at8(n)
+        assert f2h.ctypes.data % 32 == 8 and vph.ctypes.data % 32 == 8
+    else:
+        f2h, vph = np.zeros(n), np.zeros(n)
+    f2d = torch.zeros(n, dtype=torch.float64, device="cuda")
+    vpd = torch.zeros_like(f2d)
+    with Context(0) as c:
+        c.extract_blocks(rec, p.n_ind, sel, po, p.block_id, B, precision="split_f16", out=(f2h, vph))
+        c.extract_blocks(torch.from_numpy(rec).cuda(), p.n_ind, sel, po, p.block_id, B, precision="split_f16",
+                         out=(f2d, vpd))
+    assert np.array_equal(f2h, f2d.cpu().numpy())
+    assert np.array_equal(vph, vpd.cpu().numpy())
+
+
 def test_host_streaming_bounds_device_output_memory():
     """Host records and host outputs stream in segments of whole blocks through a two-segment
     ring of device slabs: the result equals the device-output extraction bit for bit, and the
