@@ -539,6 +539,9 @@ void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, u
 }
 
 void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
+    // The padded SNP axis is 32-bit: refuse M > INT_MAX before reading or allocating
+    // anything (the reference throws std::runtime_error for it).
+    if (r.geno.n_snp > INT_MAX) fail(STP_RUNTIME_ERROR, "n_snp exceeds INT_MAX (M > INT_MAX is not supported)");
     need(o.f2 != nullptr || r.n_pop == 0 || r.n_block == 0, "output f2 is NULL");
     need(o.vpair != nullptr || r.n_pop == 0 || r.n_block == 0, "output vpair is NULL");
     cudaStream_t s = c.stream;

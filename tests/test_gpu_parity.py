@@ -340,6 +340,38 @@ def test_extract_f2_files_roundtrip(tmp_path, c1):
     assert np.array_equal(h2.to_numpy(), h.to_numpy())
 
 
+def test_int_max_and_device_oom_statuses(ctx):
+    """The reference's M > INT_MAX guard (std::runtime_error) and its device-OOM status
+    (CudaError(cudaErrorMemoryAllocation) -> Status::DeviceOom), through the raw C ABI with
+    tiny buffers that neither call reads: n_snp = 2^31 fails with STP_RUNTIME_ERROR before
+    anything is allocated; 2^30 SNPs of 256-byte host records fail with STP_DEVICE_OOM when
+    the 256 GiB upload buffer cannot be allocated. The context stays usable."""
+    import ctypes as C
+
+    from steppecu_b200 import _lib as L
+
+    rec = np.zeros(256, np.uint8)
+    sel = np.arange(4, dtype=np.int64)
+    po = np.array([0, 2, 4], np.int64)
+    bid = np.zeros(4, np.int32)
+    f2, vp, bs = np.zeros(8), np.zeros(8), np.zeros(2, np.int32)
+
+    def call(n_snp):
+        g = L.GenoView(rec.ctypes.data, 256, 256, n_snp, 1024, 0)
+        r = L.F2Request(g, sel.ctypes.data, po.ctypes.data, 2, None, L.PLOIDY_AUTO, bid.ctypes.data, 2,
+                        L.PREC_SPLIT_F16)
+        o = L.F2Output(f2.ctypes.data, vp.ctypes.data, bs.ctypes.data, 0, None)
+        return L.lib().stp_f2_extract_blocks(ctx._h, C.byref(r), C.byref(o))
+
+    assert call(2**31) == L.STP_RUNTIME_ERROR
+    assert b"INT_MAX" in L.lib().stp_last_error()
+    assert call(2**30) == L.STP_DEVICE_OOM
+    p = synth.generate("c1", seed=3, n_snp=2000, n_pop=4)
+    s2, po2 = p.selection()
+    t = ctx.extract_blocks(p.records_numpy(), p.n_ind, s2, po2, p.block_id, p.n_block, precision=TC_DEFAULT)
+    assert t.f2.size == 16 * p.n_block
+
+
 @pytest.mark.parametrize("n_pop,misalign", [(600, False), (603, False), (600, True)])
 def test_host_band_download_equals_device_output(n_pop, misalign):
     """Host outputs receive only the upper 128-row bands of each slab over PCIe and the
