@@ -460,6 +460,18 @@ void download_upper_bands(double* host, const double* dev, int64_t P, int64_t T,
     }
 }
 
+// On an error, copies between the device and the caller's buffers may still be in flight:
+// drains the context's streams before the error reaches the caller (who may free them).
+struct DrainOnError {
+    Ctx& c;
+    ~DrainOnError() {
+        if (std::uncaught_exceptions() == 0) return;
+        cudaStreamSynchronize(c.h2d);
+        cudaStreamSynchronize(c.stream);
+        cudaStreamSynchronize(c.d2h);
+    }
+};
+
 // Host buffers in and out, tensor-core arithmetic: the pass runs in segments of whole
 // blocks (about a twelfth of the SNPs each, the first covering the ploidy window) so the
 // upload of segment k+1, the decode and contraction of segment k and the download of
@@ -542,6 +554,7 @@ void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
     // The padded SNP axis is 32-bit: refuse M > INT_MAX before reading or allocating
     // anything (the reference throws std::runtime_error for it).
     if (r.geno.n_snp > INT_MAX) fail(STP_RUNTIME_ERROR, "n_snp exceeds INT_MAX (M > INT_MAX is not supported)");
+    DrainOnError drain{c};
     need(o.f2 != nullptr || r.n_pop == 0 || r.n_block == 0, "output f2 is NULL");
     need(o.vpair != nullptr || r.n_pop == 0 || r.n_block == 0, "output vpair is NULL");
     cudaStream_t s = c.stream;
