@@ -64,6 +64,53 @@ def issued_tensor_work(P: int, block_id, n_block: int, con_ms: float, peak: floa
             "i8_tops": i8 / sec / 1e12}
 
 
+def run_fstats(ctx, f2, vp, block_id, P: int, B: int, n_stat: int = 100_000, reps: int = 3) -> dict:
+    """f4 statistics with their block jackknife through stp_fstats on the device-resident f2
+    tensor of the workload: the survivor pass over every slab's vpair, each quartet's
+    per-block values from four f2 slabs, and the jackknife, for n_stat random quartets of
+    distinct populations; the median of reps timed calls (host wall clock around the
+    synchronous call, including the copy of est / var back). The CPU leg runs the reference
+    CpuBackend's f-statistics (the port when the reference is absent) on one thread, on the
+    sub-tensor of the first 40 populations (the per-statistic work does not depend on P)."""
+    import numpy as np
+    import torch
+
+    import oracle
+    from steppecu_b200 import _lib as L
+
+    rng = np.random.default_rng(20261203)
+
+    def quartets(n_pop, n):
+        q = rng.integers(0, n_pop, size=(3 * n, 4))
+        distinct = np.array([len(set(r)) == 4 for r in q.tolist()])
+        return np.ascontiguousarray(q[distinct][:n], np.int32)
+
+    bs = np.bincount(np.asarray(block_id, np.int64), minlength=B).astype(np.int32)
+    q = quartets(P, n_stat)
+    ctx.fstats(f2, vp, bs, P, B, L.FSTAT_F4, q.reshape(-1), q.shape[0])
+    ts = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.fstats(f2, vp, bs, P, B, L.FSTAT_F4, q.reshape(-1), q.shape[0])
+        ts.append(time.perf_counter() - t0)
+    t = statistics.median(ts)
+
+    sub, n_cpu = min(40, P), 20_000
+    f2s = f2.view(B, P, P)[:, :sub, :sub].contiguous().cpu().numpy().reshape(-1)
+    vps = vp.view(B, P, P)[:, :sub, :sub].contiguous().cpu().numpy().reshape(-1)
+    qc = quartets(sub, n_cpu)
+    lib = "ref" if oracle.ref_available() else "port"
+    t0 = time.perf_counter()
+    oracle.fstats(f2s, vps, bs, sub, B, "f4", qc.reshape(-1), qc.shape[0], lib=lib)
+    tc = time.perf_counter() - t0
+    unit = "f4 statistics/s (with block jackknife)"
+    return {"statistics": int(q.shape[0]), "blocks": B, "ms": 1000.0 * t, "value": q.shape[0] / t, "unit": unit,
+            "cpu_baseline": {"value": qc.shape[0] / tc, "unit": unit, "cores": 1,
+                             "kind": "reference" if lib == "ref" else "port",
+                             "sample": f"{qc.shape[0]} quartets over the first {sub} populations, {B} blocks, one thread"}}
+
+
 def load_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -562,6 +609,10 @@ def main():
         per_block = {"ms_per_step": ms_b, "contract_ms": con_b, "launches_per_step": l_b / max(1, min(args.steps, 3)),
                      "value": units(P, M) * world / (ms_b / 1000.0)}
 
+    fst = None
+    if not args.quick and rank == 0 and world == 1 and P >= 4:
+        fst = run_fstats(ctx, f2, vp, panel.block_id, P, B)
+
     e2e = None
     if not args.quick:
         e2e = run_e2e(args, ctx, rec, panel, sel, po, bpr, n_out, barrier, dist, dev, P, M, B, world)
@@ -624,7 +675,7 @@ def main():
             "precision": precision,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "other_arithmetics": others,
-            "per_block_launches": per_block,
+            "per_block_launches": per_block, "fstats": fst,
             "batched_requests": batched,
             "other_configs": other_configs,
         }

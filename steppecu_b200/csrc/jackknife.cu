@@ -67,10 +67,23 @@ __global__ void survivor_kernel(const double* __restrict__ vpair, int64_t slab, 
     const int64_t b = blockIdx.x;
     const double* v = vpair + slab * b;
     int missing = 0, present = 0;
-    for (int64_t e = threadIdx.x; e < slab; e += blockDim.x) {
-        const bool p = v[e] > 0.0;
-        present |= p;
-        missing |= !p;
+    // Four independent loads per thread in flight: the pass streams every slab once.
+    for (int64_t e = threadIdx.x; e < slab; e += 4 * static_cast<int64_t>(blockDim.x)) {
+        double x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t k = e + static_cast<int64_t>(u) * blockDim.x;
+            x[u] = k < slab ? __ldg(v + k) : 0.0;  // not loaded, and not counted, past the slab
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t k = e + static_cast<int64_t>(u) * blockDim.x;
+            if (k < slab) {
+                const bool p = x[u] > 0.0;
+                present |= p;
+                missing |= !p;
+            }
+        }
     }
     missing = __syncthreads_or(missing);
     present = __syncthreads_or(present);

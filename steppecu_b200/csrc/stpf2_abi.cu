@@ -1370,11 +1370,26 @@ stp_status stp_fstats(stp_ctx* ctx, const double* f2, const double* vpair, const
             d_f2 = ctx->ws_f2.as<double>();
             d_vp = ctx->ws_vpair.as<double>();
         }
-        DevBuf d_keep;
-        d_keep.reserve(static_cast<size_t>(n_block) * 4);
-        launch_survivors(*ctx, d_vp, P, n_block, d_keep.as<int32_t>(), s);
+        // Scratch in one grow-only context workspace (per-call allocations would each free
+        // with a device-wide synchronisation): keep flags, survivors, their sizes, the
+        // indices, the per-block values (sized for every block surviving) and est / var.
+        Packing pk;
+        const size_t o_keep = pk.add(static_cast<size_t>(n_block) * 4), o_surv = pk.add(static_cast<size_t>(n_block) * 4),
+                     o_bl = pk.add(static_cast<size_t>(n_block) * 4), o_idx = pk.add(static_cast<size_t>(n_idx) * 4),
+                     o_x = pk.add(static_cast<size_t>(m) * n_block * 8), o_est = pk.add(static_cast<size_t>(m) * 8),
+                     o_var = pk.add(static_cast<size_t>(m) * 8);
+        ctx->ws_fstat.reserve(pk.end);
+        uint8_t* W = ctx->ws_fstat.as<uint8_t>();
+        auto* d_keep = reinterpret_cast<int32_t*>(W + o_keep);
+        auto* d_surv = reinterpret_cast<int32_t*>(W + o_surv);
+        auto* d_bl = reinterpret_cast<int32_t*>(W + o_bl);
+        auto* d_idx = reinterpret_cast<int32_t*>(W + o_idx);
+        auto* d_x = reinterpret_cast<double*>(W + o_x);
+        auto* d_est = reinterpret_cast<double*>(W + o_est);
+        auto* d_var = reinterpret_cast<double*>(W + o_var);
+        launch_survivors(*ctx, d_vp, P, n_block, d_keep, s);
         std::vector<int32_t> keep(static_cast<size_t>(n_block));
-        STPF2_CUDA(cudaMemcpyAsync(keep.data(), d_keep.ptr, keep.size() * 4, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaMemcpyAsync(keep.data(), d_keep, keep.size() * 4, cudaMemcpyDeviceToHost, s));
         STPF2_CUDA(cudaStreamSynchronize(s));
         std::vector<int32_t> surv, bl;
         for (int32_t b = 0; b < n_block; ++b)
@@ -1385,19 +1400,13 @@ stp_status stp_fstats(stp_ctx* ctx, const double* f2, const double* vpair, const
         const int ns = static_cast<int>(surv.size());
         if (n_survivors) *n_survivors = ns;
         if (ns == 0) return;
-        std::vector<int32_t> ix(idx, idx + n_idx);
-        DevBuf d_surv, d_bl, d_idx, d_x, d_est, d_var;
-        upload(d_surv, surv, s);
-        upload(d_bl, bl, s);
-        upload(d_idx, ix, s);
-        d_x.reserve(static_cast<size_t>(m) * ns * 8);
-        d_est.reserve(static_cast<size_t>(m) * 8);
-        d_var.reserve(static_cast<size_t>(m) * 8);
-        launch_fstat_assemble(*ctx, d_f2, P, d_surv.as<int32_t>(), ns, kind, d_idx.as<int32_t>(), n_stat, m, nr,
-                              d_x.as<double>(), s);
-        launch_jackknife(*ctx, d_x.as<double>(), d_bl.as<int32_t>(), m, ns, d_est.as<double>(), d_var.as<double>(), s);
-        STPF2_CUDA(cudaMemcpyAsync(est, d_est.ptr, static_cast<size_t>(m) * 8, cudaMemcpyDeviceToHost, s));
-        STPF2_CUDA(cudaMemcpyAsync(var, d_var.ptr, static_cast<size_t>(m) * 8, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaMemcpyAsync(d_surv, surv.data(), surv.size() * 4, cudaMemcpyHostToDevice, s));
+        STPF2_CUDA(cudaMemcpyAsync(d_bl, bl.data(), bl.size() * 4, cudaMemcpyHostToDevice, s));
+        STPF2_CUDA(cudaMemcpyAsync(d_idx, idx, static_cast<size_t>(n_idx) * 4, cudaMemcpyHostToDevice, s));
+        launch_fstat_assemble(*ctx, d_f2, P, d_surv, ns, kind, d_idx, n_stat, m, nr, d_x, s);
+        launch_jackknife(*ctx, d_x, d_bl, m, ns, d_est, d_var, s);
+        STPF2_CUDA(cudaMemcpyAsync(est, d_est, static_cast<size_t>(m) * 8, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaMemcpyAsync(var, d_var, static_cast<size_t>(m) * 8, cudaMemcpyDeviceToHost, s));
         STPF2_CUDA(cudaStreamSynchronize(s));
     });
 }

@@ -108,6 +108,7 @@ struct Ctx {
     // populations' counts and every request's tables; the contraction's work lists; and
     // the pinned staging of the tables.
     DevBuf ws_batch, ws_union, ws_tables, ws_items;
+    DevBuf ws_fstat;  // stp_fstats scratch
     PinnedBuf pin_union, pin_tables, pin_items;
     // Completion time of each request of the last stp_f2_extract_batch call, in ms from the
     // start of its group's device work (NaN for requests that ran on their own).
