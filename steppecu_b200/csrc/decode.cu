@@ -347,7 +347,9 @@ transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t
 // Pass 2: one CTA per (64 populations, quad of 4 column tiles), in two phases.
 //
 // Fold: a warp holds 8 populations x 4 tiles, lane = (population, tile), so the four lanes
-// of a population read one 32-byte sector of the quad per sample. Each thread folds its
+// of a population read one 32-byte sector of the quad per sample. With a fold order the
+// warps take the CTA's 64 populations largest first, so that the populations of one warp
+// have similar sample counts (the counts land in the same shared slots either way). Each thread folds its
 // population's samples into exact integer counts for its tile's 32 columns at once with
 // SWAR bytes: PRMT maps four 2-bit codes, taken as selector nibbles straight from the
 // masked code bits, to four count bytes through the sample's ploidy table (byte b of count
@@ -444,7 +446,7 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
                     const double* __restrict__ rec_nm1, const int32_t* __restrict__ col_snp, int64_t col_base,
                     OperandPlanes op, int32_t* __restrict__ cnt_ac2, int32_t* __restrict__ cnt_n,
                     const int32_t* __restrict__ umap, const double* __restrict__ center_snp,
-                    uint32_t* __restrict__ cnt_packed, int64_t cnt_ld) {
+                    uint32_t* __restrict__ cnt_packed, int64_t cnt_ld, const int32_t* __restrict__ fold_order) {
     extern __shared__ uint32_t s_cnt[];
     __shared__ double s_center[4 * kCenterPitch];
     const int64_t q = blockIdx.x;
@@ -463,7 +465,9 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     {
-        const int sub = lane & 3, pl_ = warp * 8 + (lane >> 2);
+        const int sub = lane & 3;
+        const int slot = warp * 8 + (lane >> 2);
+        const int pl_ = fold_order ? __ldg(fold_order + blockIdx.y * kDecPops + slot) : slot;
         const int i = blockIdx.y * kDecPops + pl_;
         if (i < P && 4 * q + sub < n_tiles) {
             const int g0 = __ldg(pop_off + i), g1 = __ldg(pop_off + i + 1);
@@ -837,7 +841,7 @@ void launch_decode_canon(Ctx& c, const CanonDecodeArgs& a, cudaStream_t s) {
     if (a.P <= 0 || a.n_tiles <= 0) return;
     const dim3 grid(static_cast<unsigned>((a.n_tiles + 3) / 4), static_cast<unsigned>((a.P + kDecPops - 1) / kDecPops));
 #define STPF2_DECODE_ARGS a.canon, a.n_tiles, a.n_sel, a.sel, a.pop_off, a.P, a.center, a.rec_n, a.rec_nm1, a.col_snp, \
-                          a.col_base, a.op, a.cnt_ac2, a.cnt_n, a.umap, a.center_snp, a.cnt_packed, a.cnt_ld
+                          a.col_base, a.op, a.cnt_ac2, a.cnt_n, a.umap, a.center_snp, a.cnt_packed, a.cnt_ld, a.fold_order
 #define STPF2_DECODE_LAUNCH(F)                                                                      \
     (a.umap ? decode_canon_kernel<F, true><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS) \
             : decode_canon_kernel<F, false><<<grid, kDecThreads2, kDecSmemBytes, s>>>(STPF2_DECODE_ARGS))

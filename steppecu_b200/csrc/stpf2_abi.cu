@@ -161,6 +161,7 @@ struct Plan {
     bool detect = false;
     BlockLayout L;
     DevBuf sel, pop_off, pos, tiles, col_snp, rec_n, rec_nm1, canon, center, blocks, items, own_planes, repitched;
+    DevBuf fold_order;  // per 64-population group, local indices largest first (null: all equal)
     uint64_t* canon_ptr = nullptr;  // canon's storage, or a context workspace (one-shot calls)
     double* center_ptr = nullptr;
     int64_t n_ind = 0, n_tiles = 0, n_sel_pad = 0;
@@ -244,6 +245,27 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
     for (int i = 0; i < r.n_pop; ++i) max_pop = std::max<int64_t>(max_pop, r.pop_offsets[i + 1] - r.pop_offsets[i]);
     need(max_pop <= 16383, "a population has more than 16383 samples");
     upload(p->pop_off, po, s);
+    // The decode's fold order: within each group of 64 populations, largest first. Only
+    // when sizes differ (equal sizes keep the natural order and no table).
+    {
+        bool uneven = false;
+        for (int i = 1; i < r.n_pop && !uneven; ++i)
+            uneven = (po[i + 1] - po[i]) != (po[1] - po[0]);
+        if (uneven) {
+            const int groups = (r.n_pop + 63) / 64;
+            std::vector<int32_t> order(static_cast<size_t>(groups) * 64);
+            for (int gidx = 0; gidx < groups; ++gidx) {
+                int32_t* o = order.data() + 64 * gidx;
+                for (int k = 0; k < 64; ++k) o[k] = k;
+                auto size_of = [&](int k) {
+                    const int i = 64 * gidx + k;
+                    return i < r.n_pop ? po[i + 1] - po[i] : -1;
+                };
+                std::stable_sort(o, o + 64, [&](int32_t x, int32_t y) { return size_of(x) > size_of(y); });
+            }
+            upload(p->fold_order, order, s);
+        }
+    }
 
     // File row -> selected index (each row may be selected once).
     p->n_ind = r.geno.n_ind;
@@ -363,6 +385,7 @@ void launch_decode(Plan& p, const uint8_t* d_records, int32_t* cnt_ac2, int32_t*
     if (cnt_ac2) a.op.planes = nullptr;
     a.cnt_ac2 = cnt_ac2;
     a.cnt_n = cnt_n;
+    a.fold_order = p.fold_order.as<int32_t>();
     launch_decode_canon(c, a, s);
 }
 

@@ -263,6 +263,10 @@ struct CanonDecodeArgs {
     // cnt_packed[i * cnt_ld + s].
     uint32_t* cnt_packed = nullptr;
     int64_t cnt_ld = 0;
+    // Optional fold order: within each group of 64 populations, the order in which the fold
+    // warps take them (local indices, largest population first), so that a warp's eight
+    // populations have similar sample counts; null keeps the natural order.
+    const int32_t* fold_order = nullptr;
 };
 
 // Ploidy detection over 4-byte record words (records and pitch 4-byte aligned); pos maps
