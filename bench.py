@@ -672,6 +672,10 @@ def main():
                        "cuda_graph": True,
                        "parallelism": f"block-sharded x{world}" if world > 1 else "1 GPU"},
             "gpu_launches": int(launches), "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            # The same throughput counted over ordered population pairs with the diagonal
+            # (M * P^2 per pass), the other convention for this metric.
+            "value_ordered_pairs": {"value": value * 2.0 * P / (P - 1) if P > 1 else None,
+                                    "unit": "SNP·ordered-pop-pairs/s (P^2 per SNP)"},
             "precision": precision,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "other_arithmetics": others,
