@@ -226,8 +226,11 @@ def precision_report(ctx, sample, modes) -> dict:
         # arithmetic; max_rel_f2_ge_0.01 is the relative error over non-degenerate values.
         out[mode] = {"max_abs": float(d.max()), "max_rel": float((d[big] / a[big]).max()),
                      "max_rel_f2_ge_0.01": float((d[sig] / a[sig]).max()),
+                     # the reference's combined check: |c - r| / (1e-9 + |r|)
+                     "max_comb": float((d / (1e-9 + a)).max()),
                      "frac_f2_ge_0.01": float(sig.mean()),
-                     "vpair_bit_exact": bool(np.array_equal(t.vpair, vp_ref))}
+                     "vpair_bit_exact": bool(np.array_equal(t.vpair, vp_ref)),
+                     "vpair_mismatches": int(np.count_nonzero(t.vpair != vp_ref))}
         if mode == modes[0]:
             # Per jackknife block of the sample (slab b = the block's P x P values).
             slab = p.n_pop * p.n_pop
