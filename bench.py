@@ -172,6 +172,12 @@ def units(P: int, M: int) -> float:
     return float(M) * P * (P - 1) / 2.0
 
 
+def band_d2h_bytes(P: int, B: int, band: int = 128) -> int:
+    """Bytes the host-output extraction downloads per call: f2 and vpair, the upper row bands
+    of every P x P slab (band t: rows [t*band, t*band + band) x columns [t*band, P))."""
+    return 2 * 8 * B * sum(min(band, P - r0) * (P - r0) for r0 in range(0, P, band))
+
+
 def make_panel(workload: str, rank: int, device: str, n_snp: int | None = None):
     from steppecu_b200 import synth
 
@@ -292,7 +298,7 @@ def run_e2e(args, ctx, rec, panel, sel, po, bpr, n_out, barrier, dist, dev, P, M
     # Host output through the tensor-core path: only the upper 128-row bands of every
     # (exactly symmetric) slab cross PCIe and the library fills the lower tiles on the host.
     banded = args.precision != "fp32" and B >= 2 and P > 0
-    d2h = 2 * 8 * B * sum(min(128, P - r0) * (P - r0) for r0 in range(0, P, 128)) if banded else 2 * n_out * 8
+    d2h = band_d2h_bytes(P, B) if banded else 2 * n_out * 8
     e2e = {"value": units(P, M) * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(rec_h.numel()),
            "d2h_bytes_per_step": int(d2h), "output_bytes_per_step": int(2 * n_out * 8),
            "ms_per_step": 1000.0 * e2e_s, "steps": e2e_steps}
