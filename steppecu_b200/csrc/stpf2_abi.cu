@@ -720,6 +720,7 @@ void prepare_member(const stp_f2_request& r, const stp_f2_output& o, int64_t n_i
 // stored. done_ms[m] receives request idx[m]'s completion time from the start of the group.
 void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* outs, const std::vector<int>& idx,
                            std::vector<double>& done_ms) {
+    DrainOnError drain{c};
     cudaStream_t s = c.stream;
     const stp_geno_view& g = reqs[idx[0]].geno;
     const int64_t M = g.n_snp, n_ind = g.n_ind;
