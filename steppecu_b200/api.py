@@ -141,13 +141,30 @@ class Context:
         """stp_decode_counts_noalloc: device records (torch CUDA uint8 [n_snp, pitch], pitch a
         multiple of 16) -> the caller's device int32 buffers d_ac2 / d_n (n_pop * n_snp each,
         column-major like decode_counts). Allocates nothing on the device."""
+        import torch
+
         if not (_is_torch_cuda(d_records) and _is_torch_cuda(d_ac2) and _is_torch_cuda(d_n)):
             raise TypeError("decode_counts_noalloc takes torch CUDA tensors")
-        v = self.geno_view(d_records, n_ind)
         sel, po = _i64(sel_rows), _i64(pop_offsets)
+        P = po.size - 1
+        if d_records.dtype != torch.uint8 or not d_records.is_contiguous() or d_records.dim() != 2:
+            raise ValueError("d_records must be a contiguous uint8 CUDA tensor [n_snp, pitch]")
+        need = max(P, 0) * d_records.shape[0]
+        for name, t in (("d_ac2", d_ac2), ("d_n", d_n)):
+            if t.dtype != torch.int32 or not t.is_contiguous():
+                raise ValueError(f"{name} must be a contiguous int32 CUDA tensor")
+            if t.numel() < need:
+                raise ValueError(f"{name} holds {t.numel()} elements; n_pop * n_snp = {need} are written")
+            if t.device.index != self.device or d_records.device.index != self.device:
+                raise ValueError(f"{name} and d_records must be on this context's device cuda:{self.device}")
+        v = self.geno_view(d_records, n_ind)
         sp = None if sample_ploidy is None else _i32(sample_ploidy)
         mode = PLOIDY[str(ploidy)] if not isinstance(ploidy, int) else ploidy
-        st = None if stream is None else C.c_void_p(stream.cuda_stream)
+        # Work is ordered after what torch queued on the current stream (the records upload,
+        # the output tensors' fills) unless the caller names a stream.
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        st = C.c_void_p(stream.cuda_stream)
         L.check(L.lib().stp_decode_counts_noalloc(self._h, C.byref(v), L.ptr(sel), L.ptr(po), po.size - 1,
                                                   L.ptr(sp), mode, C.c_void_p(d_ac2.data_ptr()),
                                                   C.c_void_p(d_n.data_ptr()), st))

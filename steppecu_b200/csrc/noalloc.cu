@@ -14,6 +14,7 @@
 // on a device, so calls whose work overlaps in time (other host threads, other streams)
 // race on it and must be serialised by the caller.
 #include <algorithm>
+#include <exception>
 #include <mutex>
 #include <string>
 
@@ -58,6 +59,15 @@ __global__ void noalloc_layout_kernel(int64_t n_snp, int64_t n_tiles, TileInfo* 
     }
     if (k <= P) po32[k] = static_cast<int32_t>(po64[k]);
 }
+
+// An error thrown after work was queued must not return while that work still writes the
+// caller's outputs and the shared scratch: wait for the stream first.
+struct SyncOnError {
+    cudaStream_t s;
+    ~SyncOnError() {
+        if (std::uncaught_exceptions() > 0) cudaStreamSynchronize(s);
+    }
+};
 
 void* scratch_base(int device) {
     if (device < 0 || device >= kMaxDevices) fail(STP_INVALID_ARGUMENT, "device ordinal out of range");
@@ -125,6 +135,7 @@ void noalloc_decode_counts(Ctx& c, const uint8_t* d_records, uint64_t pitch, int
     auto* d_canon = reinterpret_cast<uint64_t*>(take(static_cast<size_t>(n_quads) * n_sel_pad * 32));
     auto* d_err = reinterpret_cast<int*>(take(256));
 
+    SyncOnError sync_on_error{s};
     STPF2_CUDA(cudaMemcpyAsync(d_sel_rows, sel_rows, static_cast<size_t>(n_sel) * 8, cudaMemcpyHostToDevice, s));
     STPF2_CUDA(cudaMemcpyAsync(d_po64, pop_offsets, static_cast<size_t>(P + 1) * 8, cudaMemcpyHostToDevice, s));
     if (d_pl)

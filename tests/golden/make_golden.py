@@ -10,11 +10,13 @@ Source: docs/examples/f2_9pop/{f2.bin, pops.txt, meta.json} in the reference (a 
 - f2_9pop_pops.txt     the population labels in P-axis order.
 
 Run from the repository root: python tests/golden/make_golden.py [reference_root]
+(default: $STEPPE_REFERENCE_ROOT).
 """
 from __future__ import annotations
 
 import hashlib
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -24,7 +26,10 @@ HEAD_BLOCKS = 12
 HERE = Path(__file__).resolve().parent
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str = "") -> None:
+    ref_root = ref_root or os.environ.get("STEPPE_REFERENCE_ROOT", "")
+    if not ref_root:
+        raise SystemExit("give the reference checkout as an argument or in STEPPE_REFERENCE_ROOT")
     ex = Path(ref_root) / "docs" / "examples" / "f2_9pop"
     data = (ex / "f2.bin").read_bytes()
     pops = (ex / "pops.txt").read_bytes()
