@@ -38,6 +38,11 @@ sys.path.insert(0, str(ROOT / "oracle"))
 METRIC = "f2 SNP·pop-pairs/s: split-BF16 TC vs plain FP32 on 1 B200, rel err ≤1e-6 vs FP64"
 UNIT = "SNP·pop-pairs/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# The arithmetic each precision mode computes in (the bench line's dtype), and the operand
+# bytes the decode writes per (population, SNP) in it.
+DTYPES = {"split_bf16": "bf16x3", "split_f16": "f16x3", "split_f16_fine": "f16x3", "fixed_i8": "i8x4 (int32 exact)",
+          "fp32": "f32"}
+OPERAND_BYTES = {"split_bf16": 11, "split_f16": 11, "split_f16_fine": 11, "fixed_i8": 10, "fp32": 9}
 # dram__bytes_read.sum + dram__bytes_write.sum of one f2_umma_kernel launch (ncu, one pass).
 CONTRACTION_TRAFFIC = {("c3", "split_f16"): 13.58e9 + 12.24e9}
 
@@ -62,6 +67,73 @@ def issued_tensor_work(P: int, block_id, n_block: int, con_ms: float, peak: floa
     sec = con_ms / 1000.0
     return {"f16_flops": f16, "i8_ops": i8, "f16_tflops": f16 / sec / 1e12, "f16_frac": f16 / sec / 1e12 / peak,
             "i8_tops": i8 / sec / 1e12}
+
+
+def issued_fixed_work(P: int, block_id, n_block: int, con_ms: float, peak_bf16: float) -> dict:
+    """Tensor work the fixed-point contraction issues, over its measured time (both kernels).
+
+    Per 32-SNP stage of a 128 x 128 tile pair (ti <= tj): 18 kind::i8 MMAs of 128 x 128 x 32
+    in the f2 kernel (ten digit products of X, four E(i) M(j), four M(i) E(j)) and one in the
+    vpair kernel. The dense int8 tensor peak is twice the bf16 one on this part; the fraction
+    is reported against twice the measured bf16 figure.
+    """
+    import numpy as np
+
+    k = np.bincount(np.asarray(block_id, np.int64), minlength=n_block)
+    stages = int(((k + 31) // 32).sum())
+    rt = (P + 127) // 128
+    pairs = rt * (rt + 1) // 2
+    i8 = pairs * stages * 19 * 2.0 * 128 * 128 * 32
+    sec = con_ms / 1000.0
+    return {"i8_ops": i8, "i8_tops": i8 / sec / 1e12, "i8_frac": i8 / sec / 1e12 / (2.0 * peak_bf16),
+            "peak_i8_tops": 2.0 * peak_bf16, "mmas_per_stage": 19}
+
+
+def precision_all_blocks(f2_dev, vp_dev, rec_host, panel, sel, po, step: int = 10, threads: int | None = None,
+                         rtol: float = 1e-6, atol: float = 1e-9) -> dict:
+    """f2 error against the CPU oracle in every jackknife block of the full panel, on the pairs
+    of every step-th population (step 10 at 1,000 populations: 100 of them, one in each 10,
+    so their pairs fall in every 128 x 128 tile pair of the contraction; step 1: all pairs).
+    f2 of a pair depends only on its two populations, so the oracle runs on that
+    sub-selection: decode, then the per-block f2 on `threads` host threads."""
+    import numpy as np
+    import torch
+
+    import oracle
+
+    P, B = panel.n_pop, panel.n_block
+    idx = np.arange(0, P, step)
+    sub_sel = np.concatenate([sel[po[i]:po[i + 1]] for i in idx]).astype(np.int64)
+    sub_po = np.concatenate([[0], np.cumsum([po[i + 1] - po[i] for i in idx])]).astype(np.int64)
+    threads = threads or os.cpu_count() or 1
+    t0 = time.perf_counter()
+    pl = oracle.detect_ploidy_pa(rec_host, sub_sel)
+    f2_ref, vp_ref, _ = oracle.f2_from_panel(rec_host, sub_sel, sub_po, panel.block_id, B, pl, threads=threads)
+    cpu_s = time.perf_counter() - t0
+    n = idx.size
+    it = torch.as_tensor(idx, device=f2_dev.device)
+    got = f2_dev.view(B, P, P).index_select(1, it).index_select(2, it).cpu().numpy().reshape(B, n, n)
+    gvp = vp_dev.view(B, P, P).index_select(1, it).index_select(2, it).cpu().numpy().reshape(B, n, n)
+    want = f2_ref.reshape(B, n, n)
+    d = np.abs(got - want)
+    a = np.abs(want)
+    big = a >= 1e-12
+    rel = np.where(big, d / np.where(big, a, 1.0), 0.0)
+    per_abs = d.reshape(B, -1).max(axis=1)
+    per_rel = rel.reshape(B, -1).max(axis=1)
+    bad = d > atol + rtol * a
+    return {
+        "pairs": "every %d-th population: %d populations, %d pairs per block" % (step, n, n * (n - 1) // 2),
+        "blocks": B, "oracle": "port (the C restatement: long-double pairwise sums, as the reference CpuBackend)",
+        "oracle_seconds": cpu_s, "oracle_threads": threads,
+        "max_abs": float(d.max()), "max_rel_f2_ge_1e-12": float(rel.max()),
+        "max_comb_1e-9": float((d / (1e-9 + a)).max()),
+        "max_rel_floor_1e-3": float((d / np.maximum(a, 1e-3)).max()),
+        "tolerance": {"rtol": rtol, "atol": atol, "violations": int(bad.sum())},
+        "vpair_bit_exact": bool(np.array_equal(gvp, vp_ref.reshape(B, n, n))),
+        "per_block_max_abs": [float(x) for x in per_abs],
+        "per_block_max_rel": [float(x) for x in per_rel],
+    }
 
 
 def run_fstats(ctx, f2, vp, block_id, P: int, B: int, n_stat: int = 100_000, reps: int = 3) -> dict:
@@ -368,7 +440,8 @@ def run_config(workload: str, dev: str, modes, steps: int = 3, per_block: bool =
     return out
 
 
-def run_batched(dev: str, steps: int = 3, n_req: int = 64, serial_baselines: bool = True, warmup: int = 3) -> dict:
+def run_batched(dev: str, steps: int = 3, n_req: int = 64, serial_baselines: bool = True, warmup: int = 3,
+                precision: str = "split_f16") -> dict:
     """Many requests over one shared panel (8,000 samples x 1.15M SNPs, 64 requests of
     4-300 populations, each with its own 5 cM block map): one grouped stp_f2_extract_batch
     call against the same requests extracted one after another (plain FP32 SIMT and
@@ -415,8 +488,8 @@ def run_batched(dev: str, steps: int = 3, n_req: int = 64, serial_baselines: boo
         ser_f32 = serial(ctx, "fp32")
         ctx.close()
         ctx = sb.Context(ordinal)
-        serial(ctx, "split_f16")  # warm-up
-        ser_f16 = serial(ctx, "split_f16")
+        serial(ctx, precision)  # warm-up
+        ser_f16 = serial(ctx, precision)
         ref = [(f2.clone(), vp.clone()) for f2, vp in outs]
         ctx.close()
 
@@ -425,7 +498,7 @@ def run_batched(dev: str, steps: int = 3, n_req: int = 64, serial_baselines: boo
     def grouped():
         torch.cuda.synchronize()
         t = time.perf_counter()
-        ctx.extract_batch(rec, panel.n_ind, reqs, precision="split_f16", out=outs)
+        ctx.extract_batch(rec, panel.n_ind, reqs, precision=precision, out=outs)
         return time.perf_counter() - t
 
     for _ in range(max(1, warmup)):  # warm-up (the first call allocates the batch workspace)
@@ -449,8 +522,8 @@ def run_batched(dev: str, steps: int = 3, n_req: int = 64, serial_baselines: boo
                     "device_span_ms": float(np.nanmax(done)),
                     "device_value": total_units / (float(np.nanmax(done)) / 1e3),
                     "completion_ms_p50": pct(done, 50), "completion_ms_p99": pct(done, 99), "gpu_launches": launches,
-                    "equals_serial_split_f16": same},
-        "serial_split_f16": None if ser_f16 is None else {
+                    "precision": precision, "equals_serial": same},
+        "serial_same_precision": None if ser_f16 is None else {
             "value": total_units / (ser_f16[-1] / 1e3), "ms_total": ser_f16[-1],
             "completion_ms_p50": pct(ser_f16, 50), "completion_ms_p99": pct(ser_f16, 99)},
         "serial_fp32": None if ser_f32 is None else {
@@ -469,7 +542,7 @@ def main():
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c5: only the many-requests measurement (grouped batch vs serial)")
     ap.add_argument("--precision", default="split_f16")
-    ap.add_argument("--also", default="split_bf16,split_f16_fine",
+    ap.add_argument("--also", default="split_f16,fixed_i8,split_bf16,split_f16_fine",
                     help="other tensor-core arithmetics timed beside the headline (comma-separated, or none)")
     ap.add_argument("--compare-simt", action="store_true", default=True)
     ap.add_argument("--no-compare-simt", dest="compare_simt", action="store_false")
@@ -481,6 +554,10 @@ def main():
                     help="skip the many-requests (grouped batch) measurement")
     ap.add_argument("--no-other-configs", dest="other_configs", action="store_false",
                     help="skip the 100-population and uneven-block config measurements")
+    ap.add_argument("--precision-step", type=int, default=10,
+                    help="per-block f2 error of the headline pass against the CPU oracle on the pairs of every "
+                         "n-th population, all blocks (1: all pairs, several minutes of host time at 1,000 "
+                         "populations; 0: skip)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -512,14 +589,15 @@ def main():
 
     dev = f"cuda:{local}"
     if args.workload == "c5":
-        b = run_batched(dev, steps=args.steps, serial_baselines=not args.quick, warmup=args.warmup)
+        b = run_batched(dev, steps=args.steps, serial_baselines=not args.quick, warmup=args.warmup,
+                        precision=args.precision)
         if rank == 0:
             print(json.dumps({
                 "metric": METRIC, "value": b["grouped"]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": b["grouped"]["ms_per_call"], "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f16x3", "data": "synthetic",
+                "vs_baseline": None, "dtype": DTYPES.get(args.precision, "f32"), "data": "synthetic",
                 "config": {"workload": "c5", "requests": b["requests"], "samples": 8000, "snps": 1150000,
-                           "precision": "split_f16", "parallelism": "1 GPU"},
+                           "precision": args.precision, "parallelism": "1 GPU"},
                 "gpu_launches": b["grouped"]["gpu_launches"], "batched_requests": b}), flush=True)
         if dist is not None:
             dist.destroy_process_group()
@@ -587,6 +665,15 @@ def main():
         # Per-kernel split (decode vs contraction) from event-bracketed plain runs.
         _, dec_ms, con_ms, _ = timed(plan, args.steps, args.warmup)
     clocks = clk.summary()
+    # The headline pass's f2 against the CPU oracle in every block (before other plans reuse
+    # the output buffers).
+    prec_all = None
+    if rank == 0 and world == 1 and not args.quick and args.precision_step > 0:
+        rec_host = rec[:, :bpr].cpu().numpy()
+        prec_all = precision_all_blocks(f2, vp, rec_host, panel, sel, po, step=args.precision_step,
+                                        threads=args.cpu_threads)
+        prec_all["precision"] = args.precision
+        del rec_host
     if dist is not None:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -638,8 +725,10 @@ def main():
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                 "kernel_ms": con_ms, "decode_ms": dec_ms,
-                "decode_hbm_gbs": (M * bpr + 11 * P * M) / (dec_ms / 1000.0) / 1e9}
-    if args.precision != "fp32":
+                "decode_hbm_gbs": (M * bpr + OPERAND_BYTES.get(args.precision, 11) * P * M) / (dec_ms / 1000.0) / 1e9}
+    if args.precision == "fixed_i8":
+        roofline["issued"] = issued_fixed_work(P, panel.block_id, B, con_ms, peak)
+    elif args.precision != "fp32":
         roofline["issued"] = issued_tensor_work(P, panel.block_id, B, con_ms, peak)
 
     cpu = None
@@ -648,7 +737,8 @@ def main():
         threads = args.cpu_threads or (os.cpu_count() or 1)
         u, t, kind, desc, sample = cpu_sample(args.workload, threads, gen_device=dev, keep=True)
         cpu = {"value": u / t, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc}
-        modes = [args.precision] + [m for m in ("split_f16_fine", "split_bf16", "fp32") if m != args.precision]
+        modes = [args.precision] + [m for m in ("fixed_i8", "split_f16", "split_f16_fine", "split_bf16", "fp32")
+                                    if m != args.precision]
         precision = {"against": f"{kind} CPU f2 on the cpu_baseline sample", **precision_report(ctx, sample, modes)}
 
     other_configs = None
@@ -657,8 +747,8 @@ def main():
         # lognormal pops, lognormal blocks): full size, records in HBM.
         threads = args.cpu_threads or (os.cpu_count() or 1)
         other_configs = {
-            "c2": run_config("c2", dev, ["fp32", "split_f16"], precision_threads=threads),
-            "c4": run_config("c4", dev, ["split_f16", "split_bf16"], per_block=True),
+            "c2": run_config("c2", dev, ["fp32", "fixed_i8", "split_f16"], precision_threads=threads),
+            "c4": run_config("c4", dev, ["fixed_i8", "split_f16", "split_bf16"], per_block=True),
         }
 
     batched = None
@@ -668,13 +758,13 @@ def main():
         del rec, f2, vp, plan, ctx
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
-        batched = run_batched(dev, warmup=args.warmup)
+        batched = run_batched(dev, warmup=args.warmup, precision=args.precision)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": {"split_bf16": "bf16x3", "split_f16": "f16x3", "split_f16_fine": "f16x3"}.get(args.precision, "f32"),
+            "vs_baseline": None, "dtype": DTYPES.get(args.precision, "f32"),
             "data": "synthetic",
             "config": {"workload": args.workload, "populations": P, "samples": panel.n_ind, "snps": M,
                        "blocks": B, "precision": args.precision, "l2": "inputs larger than L2 (no flush)",
@@ -686,6 +776,7 @@ def main():
             "value_ordered_pairs": {"value": value * 2.0 * P / (P - 1) if P > 1 else None,
                                     "unit": "SNP·ordered-pop-pairs/s (P^2 per SNP)"},
             "precision": precision,
+            "precision_all_blocks": prec_all,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "other_arithmetics": others,
             "per_block_launches": per_block, "fstats": fst,

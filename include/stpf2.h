@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define STPF2_ABI_VERSION 1
+#define STPF2_ABI_VERSION 2
 
 /* Status codes. 0..5 keep the numbering of steppe::Status (include/steppe/error.hpp:14-26);
  * the rest stand for the reference's exception types (std::invalid_argument /
@@ -43,8 +43,11 @@ typedef enum stp_precision {
     STP_PREC_SPLIT_BF16 = 1, /* tcgen05 split-BF16 (hi+lo, 3 products), FP32 TMEM, FP64 drain */
     STP_PREC_SPLIT_F16 = 2,  /* tcgen05 split-FP16 (scaled hi+lo, 3 products), same pipeline;
                                 FP32 sums over 64-SNP chunks (max rel f2 error ~8e-7) */
-    STP_PREC_SPLIT_F16_FINE = 3 /* split-FP16 with FP32 sums over 32-SNP chunks (~4.5e-7,
+    STP_PREC_SPLIT_F16_FINE = 3, /* split-FP16 with FP32 sums over 32-SNP chunks (~4.5e-7,
                                    ~15% slower contraction) */
+    STP_PREC_FIXED_I8 = 4 /* tcgen05 kind::i8 on 32-bit fixed-point operands held as four
+                             int8 digits, exact int32 accumulation, FP64 combine: f2 within
+                             ~1e-9 absolute of FP64 per SNP, far less on block means */
 } stp_precision;
 
 /* steppe::ExtractPloidy (include/steppe/extract.hpp) */
@@ -53,6 +56,30 @@ typedef enum stp_ploidy_mode {
     STP_PLOIDY_PSEUDO = 1, /* every sample pseudo-haploid */
     STP_PLOIDY_DIPLOID = 2 /* every sample diploid */
 } stp_ploidy_mode;
+
+/* steppe::StrandMode (include/steppe/config.hpp:128). The keep mask never flips alleles,
+ * so FLIP keeps ambiguous SNPs as KEEP does (src/io/filter/snp_filter.hpp:6). */
+typedef enum stp_strand_mode {
+    STP_STRAND_DROP = 0,
+    STP_STRAND_KEEP = 1,
+    STP_STRAND_FLIP = 2
+} stp_strand_mode;
+
+/* The per-SNP filters of extract-f2 (FilterConfig, include/steppe/config.hpp:131-164, as
+ * extract_f2_core.cpp:188-260 applies them; the include / exclude SNP lists are the
+ * caller's to apply). A SNP is kept when its alleles are two distinct bases, it is not
+ * strand-ambiguous (under STP_STRAND_DROP), its pooled minor allele frequency is >= maf_min,
+ * it is polymorphic (when drop_monomorphic), a transversion (when transversions_only), on
+ * chromosomes 1..22 (when autosomes_only), and at most maxmiss of the populations have no
+ * call at it (maxmiss = 1: no bound). */
+typedef struct stp_snp_filter {
+    double maf_min;
+    double maxmiss;
+    int32_t autosomes_only;
+    int32_t drop_monomorphic;
+    int32_t transversions_only;
+    int32_t strand_mode; /* stp_strand_mode */
+} stp_snp_filter;
 
 typedef struct stp_ctx stp_ctx;
 typedef struct stp_plan stp_plan;
@@ -78,9 +105,17 @@ typedef struct stp_f2_request {
     int32_t n_pop;
     const int32_t* sample_ploidy; /* [n_sel] 1/2, or NULL to use ploidy_mode */
     int32_t ploidy_mode;          /* stp_ploidy_mode, used when sample_ploidy is NULL */
-    const int32_t* block_id;      /* [n_snp] non-decreasing in [0, n_block) (core::assign_blocks) */
+    const int32_t* block_id;      /* [n_snp] (or [n_kept]) non-decreasing in [0, n_block) (core::assign_blocks) */
     int32_t n_block;
     int32_t precision;            /* stp_precision */
+    /* Optional SNP compaction (the kept set of extract_f2_core.cpp:188-291): kept_rows[k] is
+     * the record row of the request's k-th SNP, strictly increasing, k < n_kept. The decode
+     * reads those records in place (no compacted copy is made); block_id then has n_kept
+     * entries. Ploidy is still detected on the first min(1000, n_snp) records, as the
+     * reference detects it before filtering. NULL: every record, in order. In
+     * stp_f2_extract_batch a request with kept rows runs on its own. */
+    const int64_t* kept_rows;
+    int64_t n_kept;
 } stp_f2_request;
 
 /* Caller-owned result buffers in F2BlockTensor layout. */
@@ -149,6 +184,33 @@ stp_status stp_decode_counts_noalloc(stp_ctx* ctx, const stp_geno_view* geno, co
                                      const int32_t* sample_ploidy, int32_t ploidy_mode,
                                      int32_t* d_ac2, int32_t* d_n, void* stream);
 
+/* extract-f2's per-SNP keep mask, on the device (the regime-B mask of
+ * src/device/cuda/decode_compact_kernel.cu:39-68): exact counts of the selected samples
+ * (as stp_decode_counts), then per SNP the pooled summary of
+ * src/io/filter/snp_summary_reduce.hpp:38-59 over the populations in order (q = ac / n, the
+ * product q * n rounded before it is added, ploidy 2) and the rules of stp_snp_filter.
+ * ref / alt / chrom: host [n_snp] (.snp alleles and chromosome codes). Out: keep [n_snp]
+ * host (1 = keep), *n_kept, and optionally summary [4 * n_snp] host: pooled ref allele
+ * frequency, pooled minor allele frequency, missing fraction, pooled called-allele count
+ * (io::filter::PerSnpSummary). The kept rows are what stp_f2_request.kept_rows takes. */
+stp_status stp_snp_keep_mask(stp_ctx* ctx, const stp_geno_view* geno, const int64_t* sel_rows,
+                             const int64_t* pop_offsets, int32_t n_pop, const int32_t* sample_ploidy,
+                             int32_t ploidy_mode, const char* ref, const char* alt, const int32_t* chrom,
+                             const stp_snp_filter* filter, uint8_t* keep, int64_t* n_kept, double* summary);
+
+/* ComputeBackend::decode_af_compact_filter (src/device/backend.hpp:914-925) on the
+ * canonical individual-major tile (as stp_decode_af): the keep mask of stp_snp_keep_mask
+ * over the tile's SNPs (total_indiv: the selection's individual count for the missing
+ * fraction), then q / v / n of the kept SNPs only, [P x n_kept] column-major FP64, device
+ * pointers when out_on_device. With q = v = n = NULL only keep [n_snp] (host) and *n_kept are
+ * written: a caller that sizes its outputs from *n_kept calls twice. */
+stp_status stp_decode_af_compact_filter(stp_ctx* ctx, const uint8_t* packed, uint64_t bytes_per_record,
+                                        int64_t n_snp, int64_t n_ind, const int64_t* pop_offsets, int32_t n_pop,
+                                        const int32_t* sample_ploidy, int32_t ploidy, int32_t packed_on_device,
+                                        const char* ref, const char* alt, const int32_t* chrom,
+                                        const stp_snp_filter* filter, double total_indiv, uint8_t* keep,
+                                        int64_t* n_kept, double* q, double* v, double* n, int32_t out_on_device);
+
 /* ComputeBackend::decode_af(DecodeTileView) (src/device/backend.hpp:736) on the canonical
  * individual-major tile: record g (bytes_per_record >= ceil(n_snp/4)) holds selected
  * sample g's SNP codes MSB-first; pop_offsets[P+1] index records. sample_ploidy NULL with
@@ -214,6 +276,15 @@ stp_status stp_fstats(stp_ctx* ctx, const double* f2, const double* vpair, const
  * item of each request); NaN for requests that ran on their own. No counterpart in the
  * reference. */
 stp_status stp_last_batch_times(stp_ctx* ctx, double* ms, int32_t n);
+
+/* The bound on every device-side wait of the fixed-point contraction (STP_PREC_FIXED_I8),
+ * and a test hook. No counterpart in the reference, whose kernels do not wait on one
+ * another. timeout_ns (0 = the default of 4 s) bounds each wait; when one runs out the kernel
+ * stops, frees its tensor memory and the call returns STP_DEVICE_TIMEOUT with the context
+ * still usable. withhold_stage >= 0 makes the f2 kernel's feed stop before that pipeline
+ * stage (its MMA issuer's wait then runs out: how the timeout path is tested); -1 turns it
+ * off. Per context. */
+stp_status stp_set_wait_bounds(stp_ctx* ctx, uint64_t timeout_ns, int64_t withhold_stage);
 
 /* Block jackknife over per-block values (cpu_backend.cpp:2674-2720, :2273-2306), FP64 on
  * the device: x[k + m*b] with m = P*P -> est[m], var[m]. Host pointers. */

@@ -384,3 +384,61 @@ int or_fstats(const double* f2, const double* vpair, const int32_t* block_sizes,
     free(x);
     return ns;
 }
+
+/* ---- extract-f2 keep mask ---------------------------------------------------------------- */
+
+/* filter_decision.hpp:43-58: A/C/G/T in either case, anything else is no allele (0). */
+static char or_norm_allele(char a) {
+    const char u = (a >= 'a' && a <= 'z') ? (char)(a - 0x20) : a;
+    return (u == 'A' || u == 'C' || u == 'G' || u == 'T') ? u : 0;
+}
+
+static char or_complement(char a) {
+    switch (a) {
+        case 'A': return 'T';
+        case 'T': return 'A';
+        case 'C': return 'G';
+        case 'G': return 'C';
+    }
+    return 0;
+}
+
+void or_keep_mask(const double* Q, const double* N, int P, long M, const char* ref, const char* alt,
+                  const int32_t* chrom, double maf_min, double maxmiss, int autosomes_only, int drop_monomorphic,
+                  int transversions_only, int strand_mode, double total_indiv, uint8_t* keep, double* summary4) {
+    for (long s = 0; s < M; ++s) {
+        /* snp_summary_reduce.hpp:38-59: products rounded before the add (no contraction). */
+        double pooled = 0.0, alleles = 0.0, nonmiss = 0.0;
+        int missing_pops = 0;
+        for (int p = 0; p < P; ++p) {
+            const long o = (long)P * s + p;
+            const double prod = Q[o] * N[o];
+            pooled = pooled + prod;
+            alleles += N[o];
+            nonmiss += N[o] / 2.0;
+            if (N[o] <= 0.0) ++missing_pops;
+        }
+        const double ref_af = alleles > 0.0 ? pooled / alleles : 0.0;
+        const double minor = (ref_af < 1.0 - ref_af) ? ref_af : (1.0 - ref_af);
+        const double missing = total_indiv > 0.0 ? 1.0 - nonmiss / total_indiv : 1.0;
+        if (summary4) {
+            summary4[s] = ref_af;
+            summary4[M + s] = minor;
+            summary4[2 * M + s] = missing;
+            summary4[3 * M + s] = alleles;
+        }
+        /* keep_decision_pooled (snp_summary_reduce.hpp:64-79), pooled missing bound 1. */
+        const char a = or_norm_allele(ref[s]), b = or_norm_allele(alt[s]);
+        int k = 1;
+        if (a == 0 || b == 0 || a == b) k = 0;                                  /* multiallelic */
+        else if (strand_mode == 0 && a == or_complement(b)) k = 0;             /* strand-ambiguous */
+        else if (!(minor >= maf_min)) k = 0;
+        else if (!(missing <= 1.0)) k = 0;
+        else if (drop_monomorphic && minor == 0.0) k = 0;
+        else if (transversions_only && ((a == 'A' || a == 'G') == (b == 'A' || b == 'G'))) k = 0;
+        else if (autosomes_only && !(chrom[s] >= 1 && chrom[s] <= 22)) k = 0;
+        /* the population-coverage bound (extract_f2_core.cpp:245-259) */
+        if (k && maxmiss < 1.0 && (double)missing_pops / (double)P > maxmiss) k = 0;
+        keep[s] = (uint8_t)k;
+    }
+}

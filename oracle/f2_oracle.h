@@ -107,6 +107,16 @@ int or_survivor_blocks(const double* vpair, int P, int nb, int32_t* keep);
 int or_fstats(const double* f2, const double* vpair, const int32_t* block_sizes, int P, int nb, int kind,
               const int32_t* idx, long n_idx, long n_stat, double* est, double* var, double* x_blocks);
 
+/* extract-f2's per-SNP keep mask (src/io/filter/snp_summary_reduce.hpp:38-79,
+ * src/io/filter/filter_decision.hpp:22-90, extract_f2_core.cpp:245-259): per SNP s the
+ * pooled summary over populations p = 0..P-1 of Q / N [P x M] (i + P*s), ploidy 2, then the
+ * keep rule (multiallelic, strand under Drop, MAF, monomorphic, transversions, autosomes
+ * 1..22) and the population-coverage bound maxmiss. strand_mode 0 Drop, 1 Keep, 2 Flip.
+ * summary4 (optional) [4 * M]: ref AF, minor AF, missing fraction, allele count. */
+void or_keep_mask(const double* Q, const double* N, int P, long M, const char* ref, const char* alt,
+                  const int32_t* chrom, double maf_min, double maxmiss, int autosomes_only, int drop_monomorphic,
+                  int transversions_only, int strand_mode, double total_indiv, uint8_t* keep, double* summary4);
+
 #ifdef __cplusplus
 }
 #endif

@@ -267,3 +267,30 @@ def fstats(f2, vpair, block_sizes, P, nb, kind, idx, n_stat, lib: str = "port", 
         _ptr(f2), _ptr(vp), _ptr(bs), P, nb, k, _ptr(ix), ix.size, n_stat, _ptr(est), _ptr(var), _ptr(xb))
     out = (est[:m], var[:m], ns)
     return out + (xb[:m * ns].reshape(ns, m),) if with_blocks else out
+
+
+def keep_mask(Q, N, P, ref_alleles, alt_alleles, chrom, maf_min=0.0, maxmiss=1.0, autosomes_only=False, drop_monomorphic=False,
+              transversions_only=False, strand_mode=0, total_indiv=None, lib: str = "port"):
+    """extract-f2's per-SNP keep mask from Q / N [P x M] (flat, i + P*s) and the .snp alleles /
+    chromosomes. Returns (keep uint8 [M], summary float64 [4, M]: ref AF, minor AF, missing
+    fraction, allele count). total_indiv defaults to the called-allele capacity / 2 of the
+    selection (pass the selection's individual count)."""
+    Qa = np.ascontiguousarray(Q, np.float64)
+    Na = np.ascontiguousarray(N, np.float64)
+    M = Qa.size // P if P > 0 else 0
+    r = np.ascontiguousarray(np.asarray(ref_alleles, dtype="S1").view(np.uint8))
+    a = np.ascontiguousarray(np.asarray(alt_alleles, dtype="S1").view(np.uint8))
+    c = np.ascontiguousarray(chrom, np.int32)
+    keep = np.zeros(max(M, 1), np.uint8)
+    summ = np.zeros(4 * max(M, 1))
+    args = [_P, _P, C.c_int, C.c_long, _P, _P, _P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+            C.c_double, _P, _P]
+    vals = (_ptr(Qa), _ptr(Na), P, M, _ptr(r), _ptr(a), _ptr(c), float(maf_min), float(maxmiss), int(autosomes_only),
+            int(drop_monomorphic), int(transversions_only), int(strand_mode), float(total_indiv), _ptr(keep),
+            _ptr(summ))
+    if lib == "ref":
+        rc = ref().fn("keep_mask", C.c_int, args)(*vals)
+        assert rc == 0
+    else:
+        port().fn("keep_mask", None, args)(*vals)
+    return keep[:M], summ[:4 * M].reshape(4, M)

@@ -18,6 +18,7 @@
 #include "core/domain/block_partition_rule.hpp"
 #include "device/backend.hpp"
 #include "device/backend_factory.hpp"
+#include "io/filter/snp_summary_reduce.hpp"
 
 namespace {
 
@@ -173,6 +174,45 @@ int ref_fstats(const double* f2, const double* vpair, const int* block_sizes, in
     } catch (const std::exception&) {
         return -1;
     }
+}
+
+// extract-f2's per-SNP keep mask as the reference decides it: the shared pooled summary and
+// keep rule (io::filter::derive_pooled_summary_one / keep_decision_pooled,
+// src/io/filter/snp_summary_reduce.hpp:38-79, ploidy 2, the pooled missing-fraction bound at
+// 1 as cuda_backend_decode.cu:512-513 sets it) and the population-coverage bound of
+// extract_f2_core.cpp:245-259 / decode_compact_kernel.cu:53-64, over Q / N [P x M].
+// strand_mode: 0 Drop, 1 Keep, 2 Flip. summary4 (optional) [4 * M]: ref AF, minor AF,
+// missing fraction, allele count.
+int ref_keep_mask(const double* Q, const double* N, int P, long M, const char* ref, const char* alt, const int* chrom,
+                  double maf_min, double maxmiss, int autosomes_only, int drop_monomorphic, int transversions_only,
+                  int strand_mode, double total_indiv, unsigned char* keep, double* summary4) {
+    steppe::FilterConfig cfg;
+    cfg.maf_min = maf_min;
+    cfg.geno_max_missing = 1.0;
+    cfg.autosomes_only = autosomes_only != 0;
+    cfg.drop_monomorphic = drop_monomorphic != 0;
+    cfg.transversions_only = transversions_only != 0;
+    cfg.strand_mode = strand_mode == 0 ? steppe::StrandMode::Drop
+                      : strand_mode == 1 ? steppe::StrandMode::Keep : steppe::StrandMode::Flip;
+    for (long s = 0; s < M; ++s) {
+        const steppe::io::filter::PooledSnpSummary ps =
+            steppe::io::filter::derive_pooled_summary_one(Q, N, P, s, 2.0, total_indiv);
+        bool k = steppe::io::filter::keep_decision_pooled(ps, ref[s], alt[s], chrom[s], cfg, true);
+        if (k && maxmiss < 1.0) {
+            int miss = 0;
+            for (int p = 0; p < P; ++p)
+                if (N[static_cast<long>(P) * s + p] <= 0.0) ++miss;
+            if (static_cast<double>(miss) / static_cast<double>(P) > maxmiss) k = false;
+        }
+        keep[s] = k ? 1 : 0;
+        if (summary4) {
+            summary4[s] = ps.pooled_ref_af;
+            summary4[M + s] = ps.pooled_minor_af;
+            summary4[2 * M + s] = ps.missing_frac;
+            summary4[3 * M + s] = ps.pooled_allele_count;
+        }
+    }
+    return 0;
 }
 
 }  // extern "C"

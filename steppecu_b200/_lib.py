@@ -36,6 +36,7 @@ PREC_FP32_SIMT = 0
 PREC_SPLIT_BF16 = 1
 PREC_SPLIT_F16 = 2
 PREC_SPLIT_F16_FINE = 3
+PREC_FIXED_I8 = 4
 FSTAT_F4 = 0
 FSTAT_F3 = 1
 FSTAT_F4_LEFT_RIGHT = 2
@@ -75,6 +76,8 @@ class F2Request(C.Structure):
         ("block_id", C.c_void_p),
         ("n_block", C.c_int32),
         ("precision", C.c_int32),
+        ("kept_rows", C.c_void_p),
+        ("n_kept", C.c_int64),
     ]
 
 
@@ -88,6 +91,19 @@ class F2Output(C.Structure):
     ]
 
 
+class SnpFilter(C.Structure):
+    _fields_ = [
+        ("maf_min", C.c_double),
+        ("maxmiss", C.c_double),
+        ("autosomes_only", C.c_int32),
+        ("drop_monomorphic", C.c_int32),
+        ("transversions_only", C.c_int32),
+        ("strand_mode", C.c_int32),
+    ]
+
+
+STRAND_DROP, STRAND_KEEP, STRAND_FLIP = 0, 1, 2
+
 # Every symbol include/stpf2.h declares, with its ctypes signature (restype, argtypes).
 _P = C.c_void_p
 SIGNATURES = {
@@ -96,10 +112,16 @@ SIGNATURES = {
     "stp_create": (_P, [C.c_int, C.POINTER(C.c_int)]),
     "stp_destroy": (None, [_P]),
     "stp_launch_count": (C.c_uint64, [_P]),
+    "stp_set_wait_bounds": (C.c_int, [_P, C.c_uint64, C.c_int64]),
     "stp_detect_ploidy": (C.c_int, [_P, C.POINTER(GenoView), _P, C.c_int64, _P]),
     "stp_detect_ploidy_tile": (C.c_int, [_P, _P, C.c_uint64, C.c_int64, C.c_int64, C.c_int32, _P]),
     "stp_decode_counts": (C.c_int, [_P, C.POINTER(GenoView), _P, _P, C.c_int32, _P, C.c_int32, _P, _P]),
     "stp_decode_counts_noalloc": (C.c_int, [_P, C.POINTER(GenoView), _P, _P, C.c_int32, _P, C.c_int32, _P, _P, _P]),
+    "stp_snp_keep_mask": (C.c_int, [_P, C.POINTER(GenoView), _P, _P, C.c_int32, _P, C.c_int32, _P, _P, _P,
+                                    C.POINTER(SnpFilter), _P, C.POINTER(C.c_int64), _P]),
+    "stp_decode_af_compact_filter": (C.c_int, [_P, _P, C.c_uint64, C.c_int64, C.c_int64, _P, C.c_int32, _P, C.c_int32,
+                                               C.c_int32, _P, _P, _P, C.POINTER(SnpFilter), C.c_double, _P,
+                                               C.POINTER(C.c_int64), _P, _P, _P, C.c_int32]),
     "stp_decode_af": (C.c_int, [_P, _P, C.c_uint64, C.c_int64, C.c_int64, _P, C.c_int32, _P, C.c_int32,
                                 C.c_int32, C.c_int32, _P, _P, _P]),
     "stp_f2_from_qvn": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int64, _P, C.c_int32, C.c_int32, _P, _P, _P]),

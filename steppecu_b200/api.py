@@ -24,13 +24,27 @@ PRECISIONS = {
     "bf16x3": L.PREC_SPLIT_BF16, "split_bf16": L.PREC_SPLIT_BF16, "bf16": L.PREC_SPLIT_BF16,
     "f16x3": L.PREC_SPLIT_F16, "split_f16": L.PREC_SPLIT_F16, "fp16": L.PREC_SPLIT_F16,
     "split_f16_fine": L.PREC_SPLIT_F16_FINE, "f16x3_fine": L.PREC_SPLIT_F16_FINE,
+    "fixed_i8": L.PREC_FIXED_I8, "i8x4": L.PREC_FIXED_I8,
 }
 PRECISION_TAGS = {L.PREC_FP32_SIMT: "fp32_simt", L.PREC_SPLIT_BF16: "split_bf16", L.PREC_SPLIT_F16: "split_f16",
-                  L.PREC_SPLIT_F16_FINE: "split_f16_fine"}
+                  L.PREC_SPLIT_F16_FINE: "split_f16_fine", L.PREC_FIXED_I8: "fixed_i8"}
 DEFAULT_PRECISION = "split_f16"
 
 PLOIDY = {"auto": L.PLOIDY_AUTO, "1": L.PLOIDY_PSEUDO, "pseudo": L.PLOIDY_PSEUDO,
           "pseudo_haploid": L.PLOIDY_PSEUDO, "2": L.PLOIDY_DIPLOID, "diploid": L.PLOIDY_DIPLOID}
+
+
+STRAND = {"drop": L.STRAND_DROP, "keep": L.STRAND_KEEP, "flip": L.STRAND_FLIP}
+
+
+def snp_filter(maf_min: float = 0.0, maxmiss: float = 1.0, autosomes_only: bool = False,
+               drop_monomorphic: bool = False, transversions_only: bool = False,
+               strand_mode: str = "drop") -> L.SnpFilter:
+    """The stp_snp_filter of extract-f2's per-SNP filters (FilterConfig)."""
+    if strand_mode not in STRAND:
+        raise ValueError("strand_mode must be one of 'drop', 'keep', 'flip'")
+    return L.SnpFilter(float(maf_min), float(maxmiss), int(bool(autosomes_only)), int(bool(drop_monomorphic)),
+                       int(bool(transversions_only)), STRAND[strand_mode])
 
 
 def parse_precision(precision) -> int:
@@ -42,6 +56,14 @@ def parse_precision(precision) -> int:
         return PRECISIONS[str(precision)]
     except KeyError:
         raise ValueError(f"precision must be one of {sorted(PRECISIONS)} (got {precision!r})") from None
+
+
+def _alleles(x) -> np.ndarray:
+    """Per-SNP allele characters as uint8 codes (from a uint8 code array or characters)."""
+    a = np.asarray(x)
+    if a.dtype in (np.uint8, np.int8):
+        return np.ascontiguousarray(a.view(np.uint8))
+    return np.ascontiguousarray(np.asarray(a, dtype="S1").view(np.uint8))
 
 
 def _i64(a) -> np.ndarray:
@@ -90,6 +112,11 @@ class Context:
     @property
     def launches(self) -> int:
         return int(L.lib().stp_launch_count(self._h))
+
+    def set_wait_bounds(self, timeout_ns: int = 0, withhold_stage: int = -1) -> None:
+        """stp_set_wait_bounds: the device-side wait bound of the fixed-point contraction
+        (0 = default) and its test hook (withhold_stage >= 0 starves the MMA issuer)."""
+        L.check(L.lib().stp_set_wait_bounds(self._h, int(timeout_ns), int(withhold_stage)))
 
     # -- genotype views ---------------------------------------------------------------
     @staticmethod
@@ -200,23 +227,79 @@ class Context:
         return F2Tensor(f2, vp, bs, P, n_block)
 
     def _request(self, records, n_ind, sel_rows, pop_offsets, block_id, n_block, precision,
-                 sample_ploidy=None, ploidy="auto"):
+                 sample_ploidy=None, ploidy="auto", kept_rows=None):
         v = self.geno_view(records, n_ind)
         sel, po, bid = _i64(sel_rows), _i64(pop_offsets), _i32(block_id)
         sp = None if sample_ploidy is None else _i32(sample_ploidy)
+        kr = None if kept_rows is None else _i64(kept_rows)
         mode = PLOIDY[str(ploidy)] if not isinstance(ploidy, int) else ploidy
         r = L.F2Request(v, L.ptr(sel), L.ptr(po), po.size - 1, L.ptr(sp), mode, L.ptr(bid), n_block,
-                        parse_precision(precision))
-        r._keep = (v, sel, po, bid, sp)
+                        parse_precision(precision), L.ptr(kr), 0 if kr is None else kr.size)
+        r._keep = (v, sel, po, bid, sp, kr)
         return r
+
+    def snp_keep_mask(self, records, n_ind: int, sel_rows, pop_offsets, ref, alt, chrom, *, maf_min: float = 0.0,
+                      maxmiss: float = 1.0, autosomes_only: bool = False, drop_monomorphic: bool = False,
+                      transversions_only: bool = False, strand_mode: str = "drop", sample_ploidy=None,
+                      ploidy="auto", summary: bool = False):
+        """stp_snp_keep_mask: extract-f2's per-SNP keep mask on the device (bool [n_snp]), and
+        with summary=True also the pooled summary [4, n_snp] (ref AF, minor AF, missing
+        fraction, allele count). ref / alt: per-SNP allele characters; chrom: int codes."""
+        v = self.geno_view(records, n_ind)
+        sel, po = _i64(sel_rows), _i64(pop_offsets)
+        sp = None if sample_ploidy is None else _i32(sample_ploidy)
+        mode = PLOIDY[str(ploidy)] if not isinstance(ploidy, int) else ploidy
+        M = v.n_snp
+        r = np.ascontiguousarray(_alleles(ref)[:M])
+        a = np.ascontiguousarray(_alleles(alt)[:M])
+        c = _i32(np.asarray(chrom)[:M])
+        if r.size < M or a.size < M or c.size < M:
+            raise ValueError("ref / alt / chrom need one entry per SNP")
+        f = snp_filter(maf_min, maxmiss, autosomes_only, drop_monomorphic, transversions_only, strand_mode)
+        keep = np.zeros(max(M, 1), np.uint8)
+        summ = np.zeros(4 * M) if summary else None
+        n_kept = C.c_int64(0)
+        L.check(L.lib().stp_snp_keep_mask(self._h, C.byref(v), L.ptr(sel), L.ptr(po), po.size - 1, L.ptr(sp), mode,
+                                          L.ptr(r), L.ptr(a), L.ptr(c), C.byref(f), L.ptr(keep), C.byref(n_kept),
+                                          L.ptr(summ)))
+        k = keep[:M].astype(bool)
+        return (k, summ.reshape(4, M)) if summary else k
+
+    def decode_af_compact_filter(self, packed, bytes_per_record: int, n_snp: int, pop_offsets, ref, alt, chrom,
+                                 filt: dict | None = None, sample_ploidy=None, ploidy: int = 2,
+                                 total_indiv: float | None = None):
+        """stp_decode_af_compact_filter on a canonical individual-major tile: (keep [n_snp],
+        q, v, n flat [P x n_kept])."""
+        po = _i64(pop_offsets)
+        P = po.size - 1
+        pk = np.ascontiguousarray(packed, dtype=np.uint8)
+        n_ind = pk.size // bytes_per_record if bytes_per_record else 0
+        r = _alleles(ref)
+        a = _alleles(alt)
+        c = _i32(chrom)
+        f = snp_filter(**(filt or {}))
+        sp = None if sample_ploidy is None else _i32(sample_ploidy)
+        tot = float(po[-1] if total_indiv is None else total_indiv)
+        keep = np.zeros(max(n_snp, 1), np.uint8)
+        nk = C.c_int64(0)
+        lib = L.lib()
+        args = (self._h, L.ptr(pk), bytes_per_record, n_snp, n_ind, L.ptr(po), P, L.ptr(sp), ploidy, 0, L.ptr(r),
+                L.ptr(a), L.ptr(c), C.byref(f), tot, L.ptr(keep), C.byref(nk))
+        L.check(lib.stp_decode_af_compact_filter(*args, None, None, None, 0))
+        q, v, n = (np.zeros(max(P * nk.value, 1)) for _ in range(3))
+        L.check(lib.stp_decode_af_compact_filter(*args, L.ptr(q), L.ptr(v), L.ptr(n), 0))
+        m = P * nk.value
+        return keep[:n_snp].astype(bool), q[:m], v[:m], n[:m]
 
     def extract_blocks(self, records, n_ind: int, sel_rows, pop_offsets, block_id, n_block: int,
                        precision=None, sample_ploidy=None, ploidy="auto", out=None,
-                       return_ploidy: bool = False):
+                       return_ploidy: bool = False, kept_rows=None):
         """The extract-f2 hot path on one request. records: host numpy [M, bpr] or a torch
-        CUDA tensor. out: optional (f2, vpair) buffers (numpy host or torch CUDA)."""
+        CUDA tensor. out: optional (f2, vpair) buffers (numpy host or torch CUDA). kept_rows:
+        optional strictly increasing record rows of the SNPs to extract (block_id then has
+        one entry per kept row); the decode reads them in place."""
         r = self._request(records, n_ind, sel_rows, pop_offsets, block_id, n_block, precision,
-                          sample_ploidy, ploidy)
+                          sample_ploidy, ploidy, kept_rows)
         P = r.n_pop
         n = P * P * n_block
         if out is None:
@@ -307,9 +390,9 @@ class Context:
         return est, var
 
     def plan(self, records, n_ind: int, sel_rows, pop_offsets, block_id, n_block: int, precision=None,
-             sample_ploidy=None, ploidy="auto") -> "Plan":
+             sample_ploidy=None, ploidy="auto", kept_rows=None) -> "Plan":
         return Plan(self, self._request(records, n_ind, sel_rows, pop_offsets, block_id, n_block, precision,
-                                        sample_ploidy, ploidy))
+                                        sample_ploidy, ploidy, kept_rows))
 
 
 class Plan:
@@ -450,30 +533,30 @@ def extract_f2(prefix, *, pops: list[str], out: str | None = None, device: int =
         raise ValueError(f"extract_f2: .snp has {snp.chrom.size} rows but the tile spans {h.n_snp} SNPs")
     labels, sel, po = select_pops(ind, pops)
     ctx = context(device)
-    from .filters import snp_keep_mask
-    keep = snp_keep_mask(ctx, rec, h, snp, sel, po, ploidy=ploidy, maf=maf, maxmiss=maxmiss,
-                         autosomes_only=autosomes_only, drop_monomorphic=drop_monomorphic,
-                         transversions_only=transversions_only, strand_mode=strand_mode)
+    M = h.n_snp
+    # The keep mask on the device from the exact counts (stp_snp_keep_mask); the kept rows are
+    # then read in place by the extraction (no compacted copy of the records). Ploidy is
+    # detected on the unfiltered records' first min(1000, M) SNPs, as the reference does
+    # (extract_f2_core.cpp:145-166), by both calls.
+    keep = ctx.snp_keep_mask(rec, h.n_ind, sel, po, snp.ref[:M], snp.alt[:M], snp.chrom[:M], maf_min=maf,
+                             maxmiss=maxmiss, autosomes_only=autosomes_only, drop_monomorphic=drop_monomorphic,
+                             transversions_only=transversions_only, strand_mode=strand_mode, ploidy=ploidy)
     idx = np.flatnonzero(keep)
     if idx.size == 0:
         raise ValueError(f"extract_f2: every SNP was filtered out (0 of {h.n_snp} kept) — relax the filters")
-    # Ploidy is detected on the unfiltered tile's first min(1000, M) SNPs (extract_f2_core.cpp:145-166).
-    sample_ploidy = None
-    if ploidy == "auto":
-        sample_ploidy = ctx.detect_ploidy(rec, h.n_ind, sel)
-    kept = rec if idx.size == h.n_snp else np.ascontiguousarray(rec[idx])
     bid, nb = assign_blocks(snp.chrom[idx], snp.genpos[idx], blgsize, snp.physpos[idx])
     if nb <= 0:
         raise ValueError("extract_f2: assign_blocks produced 0 blocks (check blgsize and the .snp genetic positions)")
-    t = ctx.extract_blocks(kept, h.n_ind, sel, po, bid, nb, precision=prec, sample_ploidy=sample_ploidy,
-                           ploidy=ploidy)
+    t = ctx.extract_blocks(rec, h.n_ind, sel, po, bid, nb, precision=prec, ploidy=ploidy,
+                           kept_rows=None if idx.size == M else idx)
     if out is None:
         return F2Blocks(t, labels, device)
     meta = {
         "precision_tag": PRECISION_TAGS.get(prec, ""), "blgsize_cm": blgsize * 100.0,
         "n_snp_total": h.n_snp, "n_snp_kept": int(idx.size),
         "filters": {"maf_min": maf, "maxmiss": maxmiss, "autosomes_only": autosomes_only,
-                    "drop_monomorphic": drop_monomorphic, "transversions_only": transversions_only},
+                    "drop_monomorphic": drop_monomorphic, "transversions_only": transversions_only,
+                    "strand_mode": strand_mode},
         "pop_selection": "explicit:" + ",".join(pops),
         "geno": prefix + ".geno", "snp": prefix + ".snp", "ind": prefix + ".ind",
     }

@@ -180,6 +180,112 @@ __device__ __forceinline__ void emit8(const OperandPlanes& op, int i, int64_t co
     }
 }
 
+// ---- fixed-point operands (OpFmt::FX) -------------------------------------------------------
+//
+// x = q - 1/2 and a = x^2 - h in FP64 from the exact counts, rounded once to 32-bit fixed
+// point: X = round(x * kFxScale) (|X| <= 127 * 2^24) and A = round(a * kFxAScale) (|A| <
+// 2^31). Each is stored as four balanced int8 digits (base 256, digits in [-128, 127]):
+// the bytes of (X + 0x80808080) ^ 0x80808080, least significant first. The image holds
+// X's digits, the digits of -A, and M = 64 * [n > 0]; see f2_fx.cu for the products.
+
+// Round to the nearest integer (ties to even) of |v| < 2^31, as the low word of v + 1.5 * 2^52.
+__device__ __forceinline__ uint32_t fx_round_fma(double a, double b) {
+    return static_cast<uint32_t>(__double2loint(fma(a, b, kFxRoundMagic)));
+}
+
+__device__ __forceinline__ uint32_t fx_digits(uint32_t v) { return (v + 0x80808080u) ^ 0x80808080u; }
+
+// Fixed-point operands of one population at one SNP from its q (FP64) and called count n.
+__device__ __forceinline__ void fx_terms(double q, double rnm1, uint32_t& X, uint32_t& NA) {
+    const double h = q * (1.0 - q) * rnm1;
+    const double x = q - 0.5;
+    X = fx_round_fma(x, kFxScale);
+    NA = fx_round_fma(-fma(x, x, -h), kFxAScale);
+}
+
+struct FxTerms8 {
+    uint32_t x[8], na[8];  // digit bytes (fx_digits) of X and -A
+    uint32_t mbits;        // bit c: column c called
+};
+
+__device__ __forceinline__ FxTerms8 fx_terms8_from_counts(const uint32_t (&v)[8], const double* __restrict__ rec_n,
+                                                          const double* __restrict__ rec_nm1) {
+    FxTerms8 t;
+    t.mbits = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const uint32_t n = v[c] >> 16, a2 = v[c] & 0xFFFFu;
+        uint32_t X = 0, NA = 0;
+        if (n > 0) {
+            const double a2d = __hiloint2double(0x43300000, static_cast<int>(a2)) - 4503599627370496.0;
+            fx_terms(a2d * 0.5 * __ldg(rec_n + n), __ldg(rec_nm1 + n), X, NA);
+            t.mbits |= 1u << c;
+        }
+        t.x[c] = fx_digits(X);
+        t.na[c] = fx_digits(NA);
+    }
+    return t;
+}
+
+// Byte k of each of four words, in order, as one word.
+__device__ __forceinline__ uint32_t gather_byte(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, int k) {
+    const uint32_t sel = static_cast<uint32_t>(k) | (static_cast<uint32_t>(k + 4) << 4);
+    return __byte_perm(__byte_perm(w0, w1, sel), __byte_perm(w2, w3, sel), 0x5410);
+}
+
+// Writes 8 consecutive columns (starting at a multiple of 8) of one population into its
+// fixed-point operand image (nine int8 tiles, 8 bytes each) and into the separate M tiles.
+__device__ __forceinline__ void emit8_fx(const OperandPlanes& op, int i, int64_t col, const FxTerms8& t) {
+    const int r = i % kTileRows, k = static_cast<int>(col % kTileK);
+    const int64_t tile = static_cast<int64_t>(i / kTileRows) * op.n_ck + col / kTileK;
+    uint8_t* img = static_cast<uint8_t*>(op.planes) + tile * kFxImageBytes + tile8_offset(r, k);
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        uint2 vx, vn;
+        vx.x = gather_byte(t.x[0], t.x[1], t.x[2], t.x[3], d);
+        vx.y = gather_byte(t.x[4], t.x[5], t.x[6], t.x[7], d);
+        vn.x = gather_byte(t.na[0], t.na[1], t.na[2], t.na[3], d);
+        vn.y = gather_byte(t.na[4], t.na[5], t.na[6], t.na[7], d);
+        *reinterpret_cast<uint2*>(img + d * kTile8Bytes) = vx;
+        *reinterpret_cast<uint2*>(img + (4 + d) * kTile8Bytes) = vn;
+    }
+    uint2 mv;
+    mv.x = 0;
+    mv.y = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const uint32_t b = ((t.mbits >> c) & 1u) ? uint32_t(kFxM) : 0u;
+        if (c < 4) mv.x |= b << (8 * c);
+        else mv.y |= b << (8 * (c - 4));
+    }
+    *reinterpret_cast<uint2*>(img + 8 * kTile8Bytes) = mv;
+    // The separate M tiles hold m itself (0/1): the vpair contraction counts exactly.
+    mv.x = (mv.x >> 6) & 0x01010101u;
+    mv.y = (mv.y >> 6) & 0x01010101u;
+    *reinterpret_cast<uint2*>(op.mtiles + tile * kTile8Bytes + tile8_offset(r, k)) = mv;
+}
+
+// One element (the Q/V/N feeder): q, n as FP64.
+__device__ __forceinline__ void emit_fx(const OperandPlanes& op, int i, int64_t col, double q, double nd, bool valid) {
+    uint32_t X = 0, NA = 0;
+    if (valid) {
+        const double nm1 = nd - 1.0;
+        fx_terms(q, 1.0 / ((nm1 > 1.0) ? nm1 : 1.0), X, NA);
+    }
+    const uint32_t dx = fx_digits(X), dn = fx_digits(NA);
+    const int r = i % kTileRows, k = static_cast<int>(col % kTileK);
+    const int64_t tile = static_cast<int64_t>(i / kTileRows) * op.n_ck + col / kTileK;
+    uint8_t* img = static_cast<uint8_t*>(op.planes) + tile * kFxImageBytes + tile8_offset(r, k);
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        img[d * kTile8Bytes] = static_cast<uint8_t>(dx >> (8 * d));
+        img[(4 + d) * kTile8Bytes] = static_cast<uint8_t>(dn >> (8 * d));
+    }
+    const uint8_t m = valid ? uint8_t(kFxM) : uint8_t(0);
+    img[8 * kTile8Bytes] = m;
+    op.mtiles[tile * kTile8Bytes + tile8_offset(r, k)] = valid ? 1 : 0;
+}
+
 // ---- canonical genotypes -------------------------------------------------------------------
 //
 // The decode runs in two passes over an intermediate "canonical" copy of the selected
@@ -226,7 +332,7 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
 template <bool kVec16>
 __device__ __forceinline__ void stage_slice(uint32_t* buf, const uint8_t* __restrict__ records, uint64_t pitch,
                                             const TileInfo* __restrict__ tiles, int64_t n_tiles, int64_t q,
-                                            int64_t slice) {
+                                            int64_t slice, const int32_t* __restrict__ row_map) {
     const uint64_t byte0 = static_cast<uint64_t>(slice) * kSliceBytes;
     for (int c = threadIdx.x; c < 4 * kTileCols * (kSliceBytes / 16); c += blockDim.x) {
         const int row = c / (kSliceBytes / 16), k = c % (kSliceBytes / 16);
@@ -237,7 +343,10 @@ __device__ __forceinline__ void stage_slice(uint32_t* buf, const uint8_t* __rest
         const uint8_t* src = nullptr;
         if (t < n_tiles) {
             const TileInfo ti = tiles[t];
-            if (r < ti.nvalid) src = records + (static_cast<int64_t>(ti.snp0) + r) * pitch;
+            if (r < ti.nvalid) {
+                const int64_t snp = static_cast<int64_t>(ti.snp0) + r;  // kept SNP -> its record row
+                src = records + static_cast<int64_t>(row_map ? __ldg(row_map + snp) : snp) * pitch;
+            }
         }
         if constexpr (kVec16) {
             if (src && b < pitch) cp_async16(d, src + b);
@@ -264,15 +373,17 @@ template <bool kVec16>
 __global__ void __launch_bounds__(kTransThreads)
 transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t n_ind,
                     const TileInfo* __restrict__ tiles, int64_t n_tiles, const int32_t* __restrict__ pos,
-                    int64_t n_sel, int64_t n_slices, uint64_t* __restrict__ canon, double* __restrict__ center) {
+                    int64_t n_sel, int64_t n_slices, uint64_t* __restrict__ canon, double* __restrict__ center,
+                    const int32_t* __restrict__ row_map) {
     extern __shared__ __align__(16) uint32_t srec_all[];
     const int64_t q = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    stage_slice<kVec16>(srec_all, records, pitch, tiles, n_tiles, q, 0);
+    stage_slice<kVec16>(srec_all, records, pitch, tiles, n_tiles, q, 0, row_map);
     for (int64_t slice = 0; slice < n_slices; ++slice) {
         uint32_t* srec = srec_all + (slice & 1) * kStagedWords;
         if (slice + 1 < n_slices) {
-            stage_slice<kVec16>(srec_all + ((slice + 1) & 1) * kStagedWords, records, pitch, tiles, n_tiles, q, slice + 1);
+            stage_slice<kVec16>(srec_all + ((slice + 1) & 1) * kStagedWords, records, pitch, tiles, n_tiles, q, slice + 1,
+                                row_map);
             asm volatile("cp.async.wait_group 1;" ::: "memory");
         } else {
             asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -550,7 +661,10 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
         uint32_t v[8];
 #pragma unroll
         for (int c = 0; c < 8; ++c) v[c] = cnt[c * kCntCol];
-        emit8<F>(op, i, col_base + col0, terms8_from_counts(v, cen, rec_n, rec_nm1));
+        if constexpr (F == OpFmt::FX)
+            emit8_fx(op, i, col_base + col0, fx_terms8_from_counts(v, rec_n, rec_nm1));
+        else
+            emit8<F>(op, i, col_base + col0, terms8_from_counts(v, cen, rec_n, rec_nm1));
     }
 }
 
@@ -651,7 +765,10 @@ __global__ void feed_qvn_kernel(const double* __restrict__ Q, const double* __re
     const int i = blockIdx.y * blockDim.y + threadIdx.y;
     if (s >= M || i >= P) return;
     const int64_t o = static_cast<int64_t>(i) + static_cast<int64_t>(P) * s;
-    emit<F>(op, i, snp_col[s], make_terms(Q[o], N[o], V[o] != 0.0, center[s]));
+    if constexpr (F == OpFmt::FX)
+        emit_fx(op, i, snp_col[s], Q[o], N[o], V[o] != 0.0);
+    else
+        emit<F>(op, i, snp_col[s], make_terms(Q[o], N[o], V[o] != 0.0, center[s]));
 }
 
 }  // namespace
@@ -708,7 +825,7 @@ void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int
 
 void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_ind, const TileInfo* tiles,
                          int64_t n_tiles, const int32_t* pos, int64_t n_sel, uint64_t* canon, double* center,
-                         cudaStream_t s) {
+                         cudaStream_t s, const int32_t* row_map) {
     if (n_tiles <= 0) return;
     const uint64_t align = pitch | static_cast<uint64_t>(reinterpret_cast<uintptr_t>(records));
     if (align % 4 != 0) fail(STP_INVALID_ARGUMENT, "transpose: genotype records need a 4-byte aligned pitch");
@@ -723,10 +840,10 @@ void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t
     }
     if (vec16)
         transpose_pa_kernel<true><<<static_cast<unsigned>(n_quads), kTransThreads, kTransSmemBytes, s>>>(
-            records, pitch, n_ind, tiles, n_tiles, pos, n_sel, n_slices, canon, center);
+            records, pitch, n_ind, tiles, n_tiles, pos, n_sel, n_slices, canon, center, row_map);
     else
         transpose_pa_kernel<false><<<static_cast<unsigned>(n_quads), kTransThreads, kTransSmemBytes, s>>>(
-            records, pitch, n_ind, tiles, n_tiles, pos, n_sel, n_slices, canon, center);
+            records, pitch, n_ind, tiles, n_tiles, pos, n_sel, n_slices, canon, center, row_map);
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
 }
@@ -763,7 +880,10 @@ emit_counts_kernel(const uint32_t* __restrict__ counts, int64_t cnt_ld, const in
             v[c] = s >= 0 ? __ldg(row + s) : 0u;
             cen[c] = s >= 0 ? __ldg(center_snp + s) : 0.5;
         }
-        emit8<F>(op, i, col0, terms8_from_counts(v, cen, rec_n, rec_nm1));
+        if constexpr (F == OpFmt::FX)
+            emit8_fx(op, i, col0, fx_terms8_from_counts(v, rec_n, rec_nm1));
+        else
+            emit8<F>(op, i, col0, terms8_from_counts(v, cen, rec_n, rec_nm1));
     }
 }
 }  // namespace
@@ -824,6 +944,7 @@ void launch_emit_counts(Ctx& c, const uint32_t* counts, int64_t cnt_ld, const in
         case OpFmt::F32: emit_counts_kernel<OpFmt::F32><<<grid, 256, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
         case OpFmt::BF16: emit_counts_kernel<OpFmt::BF16><<<grid, 256, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
         case OpFmt::F16: emit_counts_kernel<OpFmt::F16><<<grid, 256, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
+        case OpFmt::FX: emit_counts_kernel<OpFmt::FX><<<grid, 256, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
     }
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
@@ -850,6 +971,7 @@ void launch_decode_canon(Ctx& c, const CanonDecodeArgs& a, cudaStream_t s) {
         case OpFmt::F32: STPF2_DECODE_LAUNCH(OpFmt::F32); break;
         case OpFmt::BF16: STPF2_DECODE_LAUNCH(OpFmt::BF16); break;
         case OpFmt::F16: STPF2_DECODE_LAUNCH(OpFmt::F16); break;
+        case OpFmt::FX: STPF2_DECODE_LAUNCH(OpFmt::FX); break;
     }
 #undef STPF2_DECODE_LAUNCH
 #undef STPF2_DECODE_ARGS
@@ -892,6 +1014,7 @@ void launch_feed_qvn(Ctx& c, const double* Q, const double* V, const double* N, 
         case OpFmt::F32: feed_qvn_kernel<OpFmt::F32><<<grid, block, 0, s>>>(Q, V, N, P, M, snp_col, center, op); break;
         case OpFmt::BF16: feed_qvn_kernel<OpFmt::BF16><<<grid, block, 0, s>>>(Q, V, N, P, M, snp_col, center, op); break;
         case OpFmt::F16: feed_qvn_kernel<OpFmt::F16><<<grid, block, 0, s>>>(Q, V, N, P, M, snp_col, center, op); break;
+        case OpFmt::FX: feed_qvn_kernel<OpFmt::FX><<<grid, block, 0, s>>>(Q, V, N, P, M, snp_col, center, op); break;
     }
     STPF2_CUDA(cudaGetLastError());
     c.launches++;

@@ -1,0 +1,664 @@
+// steppecu_b200/csrc/f2_fx.cu
+//
+// The fixed-point f2 contraction (STP_PREC_FIXED_I8) for sm_100a: exact integer tensor-core
+// sums over 32-bit fixed-point operands, two persistent warp-specialised kernels over every
+// (jackknife block, 128x128 population tile pair ti <= tj) work item.
+//
+// Operands (decode.cu, emit8_fx): per population and SNP, X = round((q - 1/2) S) and
+// A = round((x^2 - h) S^2 / 2^31) with S = kFxScale, each as four balanced int8 digits
+// (X = sum_d X_d 256^d, X_d in [-128, 127]), plus M = 64 [n > 0]; a missing population has
+// X = A = M = 0. With T = (x_i - x_j)^2 - h_i - h_j = a_i + a_j - 2 x_i x_j
+// (f2_estimator.hpp:29-36) the block numerator sum_s T over SNPs where both are called is
+//     -2 / S^2 * sum_s [ X_i X_j - 2^24 (A_i M_j + M_i A_j) ]
+// and f2_fx_kernel computes the bracket in four int32 TMEM accumulators V_3..V_6 of weight
+// 256^3..256^6, exactly but for the dropped low digit products:
+//     V_w += X_a(i) X_b(j)        for a + b = w        (products of weight below 256^3 are
+//                                                       dropped: under 3.1 * 2^30 / S^2,
+//                                                       i.e. 1.7e-10, per SNP)
+//     V_w += E_w(i) M(j) + M(i) E_w(j)                  (E_3..E_6: the digits of -A)
+// i.e. 18 kind::i8 MMAs (M = N = 128, K = 32) per 32-SNP stage, all integer and exact.
+// The epilogue forms W = sum_w V_w 256^(w-3) in FP64 once per tile (every 16,384 SNPs of
+// a longer block, the int32 bound), f2 = W * kFxNumScale / vpair (0 when vpair = 0,
+// f2_estimator.hpp:42-46), and stores (i,j) and (j,i) of the block's slab.
+//
+// Error against exact arithmetic, per SNP and pair: the two roundings of x (2^-32.0 each,
+// times |x| <= 1/2, twice), of a (2^-33, twice) and the dropped digit products: under
+// 7e-10 on T; a block mean over K SNPs averages independent roundings (~1e-10 / sqrt(K)).
+//
+// vpair_fx_kernel runs first over the same items: the exact both-present counts
+// m_i . m_j (one kind::i8 MMA per 32 SNPs on the separate 0/1 M tiles, 128 SNPs per
+// stage, a ring of four TMEM accumulators) written as one compact int32 128x128 tile per
+// item, which the f2 epilogue reads for its divide and its vpair stores. (The four f2
+// accumulators fill TMEM's 512 columns, so the counts cannot share the f2 kernel.)
+//
+//   f2_fx_kernel:   warp 0 producer (one 36 KiB bulk copy per stage side, no tensor maps, no
+//                   multicast), warp 1 TMEM owner + single-thread MMA issuer, warps 2-17
+//                   epilogue (four per TMEM lane quarter, 32 tile columns each).
+//   vpair_fx_kernel: warp 0 producer (16 KiB per stage side), warp 1 issuer, warps 2-9
+//                   epilogue (two per lane quarter, 64 columns each).
+// Every wait is bounded (FxTuning::timeout_ns); on expiry the kernel raises an error flag
+// the host turns into STP_DEVICE_TIMEOUT, lets its copies and MMAs finish, frees TMEM and
+// returns.
+#include <algorithm>
+#include <climits>
+
+#include "stpf2_internal.cuh"
+#include "umma_ptx.cuh"
+
+namespace stpf2 {
+
+namespace {
+
+using namespace ptx;
+
+constexpr int kTile = 128;
+constexpr int kStageK = 32;
+constexpr int kItemRing = 4;
+constexpr int kVpTileInts = kTile * kTile;  // one compact vpair tile: (row r, column c) at c * 128 + r
+
+// ---- f2 kernel constants ----
+constexpr int kStages = 2;
+constexpr uint32_t kSide = static_cast<uint32_t>(kFxImageBytes);  // 36 KiB
+constexpr uint32_t kStageBytes = 2 * kSide;
+constexpr int kEpiWarps = 16;
+constexpr int kEpiWarp0 = 2;
+constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);  // 576
+constexpr int kCols = 4 * kTile / kEpiWarps;            // 32 tile columns per epilogue thread
+constexpr int kSegStages = 512;  // 16,384 SNPs: |V_3| < 81,920 per SNP stays below 2^31
+constexpr uint32_t kTmemCols = 512;
+constexpr int kStagePitch = 9;
+constexpr int kStageDoubles = 32 * kStagePitch;
+constexpr uint32_t kCtlBytes = 256;
+
+// ---- vpair kernel constants ----
+constexpr int kVpChunks = 4;  // 32-SNP chunks per stage
+constexpr uint32_t kVpSide = kVpChunks * static_cast<uint32_t>(kTile8Bytes);  // 16 KiB
+constexpr uint32_t kVpStageBytes = 2 * kVpSide;
+constexpr int kVpStages = 4;
+constexpr int kVpAcc = 4;  // TMEM ring of 128-column accumulators
+constexpr int kVpEpiWarps = 8;
+constexpr int kVpThreads = 32 * (2 + kVpEpiWarps);  // 320
+constexpr int kVpCols = 4 * kTile / kVpEpiWarps;   // 64
+
+struct FxArgs {
+    const uint8_t* images;  // (row tile t, chunk c) image at (t * n_ck + c) * kFxImageBytes
+    const uint8_t* mtiles;  // (row tile t, chunk c) M tile at (t * n_ck + c) * 4 KiB
+    int64_t n_ck;
+    const WorkItem* items;
+    int n_items;
+    const BlockInfo* blocks;
+    int P;
+    double* f2;
+    double* vpair;
+    int32_t* vpc;  // compact vpair tiles, item it at vpc + it * kVpTileInts
+    const double* rcp;  // rcp[k] = 1/k, k = 0..rcp_max (rcp[0] = 0)
+    int rcp_max;
+    int* err;
+    int* next_item;  // work-item counter, zero at launch
+    int b_base;      // block id whose slab starts the output buffers
+    uint32_t idesc;
+    unsigned long long timeout_ns;
+    long long withhold;  // test hook: the producer stops before its stage of this index (-1: never)
+    const GroupInfo* groups;  // grouped launch: per-request images / outputs (null for one request)
+    int* grp_done;
+    unsigned long long* grp_ns;
+    const int* grp_items;
+};
+
+struct FxCtl {
+    unsigned long long item_full[kItemRing], item_empty[kItemRing];
+    int item_idx[kItemRing];
+    unsigned long long full[kVpStages], empty[kVpStages];  // f2 kernel uses the first kStages
+    unsigned long long acc_full[kVpAcc], acc_empty[kVpAcc];  // f2 kernel uses slot 0 only
+    unsigned long long drain;
+    uint32_t tmem_base;
+    volatile int abort;
+};
+static_assert(sizeof(FxCtl) <= kCtlBytes, "barrier block overflows its slot");
+
+__device__ __forceinline__ bool waitb(unsigned long long* b, uint32_t parity, FxCtl* ctl, const FxArgs& a,
+                                      bool honour_abort = true) {
+    return wait_bounded(b, parity, &ctl->abort, a.err, a.timeout_ns, honour_abort);
+}
+
+__device__ __forceinline__ int stages_of(int k, int per) { return (k + per - 1) / per; }
+
+// Work items in list order from a global counter (costliest block first, a block's tile
+// pairs together), handed from the producer to the other roles through a small ring.
+__device__ __forceinline__ int take_item(const FxArgs& a, FxCtl* ctl, uint32_t gi, bool& ok) {
+    const int slot = static_cast<int>(gi % kItemRing);
+    ok = waitb(&ctl->item_empty[slot], ((gi / kItemRing) & 1u) ^ 1u, ctl, a);
+    if (!ok) return -1;
+    int it = atomicAdd(a.next_item, 1);
+    if (it >= a.n_items) it = -1;
+    *reinterpret_cast<volatile int*>(&ctl->item_idx[slot]) = it;
+    mbar_arrive(&ctl->item_full[slot]);
+    return it;
+}
+
+__device__ __forceinline__ int read_item(const FxArgs& a, FxCtl* ctl, uint32_t gi) {
+    const int slot = static_cast<int>(gi % kItemRing);
+    if (!waitb(&ctl->item_full[slot], (gi / kItemRing) & 1u, ctl, a)) return -2;
+    const int it = *reinterpret_cast<volatile int*>(&ctl->item_idx[slot]);
+    mbar_arrive(&ctl->item_empty[slot]);
+    return it;
+}
+
+__device__ __forceinline__ void init_ring(FxCtl* ctl, int consumers) {
+    for (int s = 0; s < kItemRing; ++s) {
+        mbar_init(&ctl->item_full[s], 1);
+        mbar_init(&ctl->item_empty[s], consumers);
+    }
+}
+
+// ============================== f2 kernel ================================================
+
+template <bool kGrouped>
+__device__ void fx_producer(const FxArgs& a, uint8_t* smem, FxCtl* ctl) {
+    uint32_t g = 0;
+    for (uint32_t gi = 0;; ++gi) {
+        bool ok = true;
+        const int it = take_item(a, ctl, gi, ok);
+        if (!ok) goto abort;
+        if (it < 0) break;
+        {
+            const WorkItem w = a.items[it];
+            const BlockInfo bi = a.blocks[w.blk];
+            const int nst = stages_of(bi.k, kStageK);
+            const bool diag = w.ti == w.tj;
+            const uint8_t* images = a.images;
+            int64_t n_ck = a.n_ck;
+            if constexpr (kGrouped) {
+                images = a.groups[bi.grp].images;
+                n_ck = a.groups[bi.grp].n_ck;
+            }
+            for (int st = 0; st < nst; ++st, ++g) {
+                if (static_cast<long long>(g) == a.withhold) return;  // test hook: stop feeding
+                const int slot = static_cast<int>(g % kStages);
+                if (!waitb(&ctl->empty[slot], ((g / kStages) & 1u) ^ 1u, ctl, a)) goto abort;
+                uint8_t* sb = smem + slot * kStageBytes;
+                mbar_expect_tx(&ctl->full[slot], diag ? kSide : kStageBytes);
+                const int64_t chunk = bi.col / kStageK + st;
+                bulk_load(sb, images + (static_cast<int64_t>(w.ti) * n_ck + chunk) * kSide, kSide, &ctl->full[slot]);
+                if (!diag)
+                    bulk_load(sb + kSide, images + (static_cast<int64_t>(w.tj) * n_ck + chunk) * kSide, kSide,
+                              &ctl->full[slot]);
+            }
+        }
+    }
+    return;
+abort:
+    // Let the copies already issued land before the CTA's shared memory goes away.
+    for (uint32_t k = (g >= kStages ? g - kStages : 0); k < g; ++k)
+        waitb(&ctl->full[k % kStages], (k / kStages) & 1u, ctl, a, false);
+}
+
+__device__ void fx_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t tmem) {
+    uint32_t g = 0, cs = 0;
+    const uint32_t V3 = tmem, V4 = tmem + 128u, V5 = tmem + 256u, V6 = tmem + 384u;
+    const uint32_t id = a.idesc;
+    for (uint32_t gi = 0;; ++gi) {
+        const int it = read_item(a, ctl, gi);
+        if (it < 0) break;
+        const WorkItem w = a.items[it];
+        const int nst = stages_of(a.blocks[w.blk].k, kStageK);
+        const bool diag = w.ti == w.tj;
+        for (int st = 0; st < nst; ++st, ++g) {
+            const int sseg = st % kSegStages;
+            if (sseg == 0) {  // the epilogue has read the accumulators of the previous segment
+                if (!waitb(&ctl->acc_empty[0], (cs & 1u) ^ 1u, ctl, a)) goto done;
+                tc_fence_after();
+            }
+            const int slot = static_cast<int>(g % kStages);
+            if (!waitb(&ctl->full[slot], (g / kStages) & 1u, ctl, a)) goto done;
+            tc_fence_after();
+            {
+                const uint32_t sa = smem_u32(smem + slot * kStageBytes);
+                const uint32_t sb = diag ? sa : sa + kSide;
+                auto dA = [&](int t) { return smem_desc(sa + static_cast<uint32_t>(t) * 4096u, 256, 6); };
+                auto dB = [&](int t) { return smem_desc(sb + static_cast<uint32_t>(t) * 4096u, 256, 6); };
+                const uint32_t f = sseg == 0 ? 0u : 1u;  // the first stage of a segment overwrites
+                // X digit products of weight >= 256^3, grouped by A operand.
+                mma_i8(V3, dA(3), dB(0), id, f);
+                mma_i8(V4, dA(3), dB(1), id, f);
+                mma_i8(V5, dA(3), dB(2), id, f);
+                mma_i8(V6, dA(3), dB(3), id, f);
+                mma_i8(V3, dA(2), dB(1), id, 1u);
+                mma_i8(V4, dA(2), dB(2), id, 1u);
+                mma_i8(V5, dA(2), dB(3), id, 1u);
+                mma_i8(V3, dA(1), dB(2), id, 1u);
+                mma_i8(V4, dA(1), dB(3), id, 1u);
+                mma_i8(V3, dA(0), dB(3), id, 1u);
+                // M(i) E_w(j) and E_w(i) M(j): tiles 4..7 are E_3..E_6, tile 8 is M.
+                mma_i8(V3, dA(8), dB(4), id, 1u);
+                mma_i8(V4, dA(8), dB(5), id, 1u);
+                mma_i8(V5, dA(8), dB(6), id, 1u);
+                mma_i8(V6, dA(8), dB(7), id, 1u);
+                mma_i8(V3, dA(4), dB(8), id, 1u);
+                mma_i8(V4, dA(5), dB(8), id, 1u);
+                mma_i8(V5, dA(6), dB(8), id, 1u);
+                mma_i8(V6, dA(7), dB(8), id, 1u);
+            }
+            mma_commit(&ctl->empty[slot]);
+            if (sseg == kSegStages - 1 || st == nst - 1) {
+                mma_commit(&ctl->acc_full[0]);
+                ++cs;
+            }
+        }
+    }
+done:
+    // Every MMA this thread issued completes before TMEM is released.
+    mma_commit(&ctl->drain);
+    waitb(&ctl->drain, 0u, ctl, a, false);
+}
+
+struct ItemOut {
+    double* f2;
+    double* vp;
+    int64_t slab;
+    int P, i, j0, i0, grp;
+    bool diag;
+};
+
+template <bool kGrouped>
+__device__ __forceinline__ ItemOut item_out(const FxArgs& a, int it, int r, int h, int cols) {
+    const WorkItem w = a.items[it];
+    const BlockInfo bi = a.blocks[w.blk];
+    ItemOut o;
+    o.grp = bi.grp;
+    o.P = a.P;
+    o.f2 = a.f2;
+    o.vp = a.vpair;
+    if constexpr (kGrouped) {
+        const GroupInfo& gr = a.groups[bi.grp];
+        o.P = gr.P;
+        o.f2 = gr.f2;
+        o.vp = gr.vpair;
+    }
+    o.diag = w.ti == w.tj;
+    o.i = w.ti * kTile + r;
+    o.i0 = w.ti * kTile + (r & ~31);
+    o.j0 = w.tj * kTile + h * cols;
+    o.slab = static_cast<int64_t>(o.P) * o.P * (bi.b - a.b_base);
+    return o;
+}
+
+template <bool kGrouped>
+__device__ __forceinline__ void stamp(const FxArgs& a, int grp, int lane) {
+    if (!kGrouped || !a.grp_done) return;
+    __syncwarp();
+    if (lane == 0) {
+        __threadfence();
+        const int d = atomicAdd(a.grp_done + grp, 1);
+        if (d == a.grp_items[grp] * kEpiWarps - 1) a.grp_ns[grp] = globaltimer();
+    }
+}
+
+template <bool kGrouped>
+__device__ void fx_epilogue(const FxArgs& a, FxCtl* ctl, uint32_t tmem, int warp, int lane, double* stage) {
+    const int e = warp - kEpiWarp0;
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int h = e >> 2;    // column part of the tile
+    const int r = q * 32 + lane;
+    const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
+    const uint32_t col_addr = static_cast<uint32_t>(h * kCols);
+    uint32_t cs = 0;
+    double acc[kCols];  // W of this thread's row and columns
+    for (uint32_t gi = 0;; ++gi) {
+        int it = 0;
+        if (lane == 0) it = read_item(a, ctl, gi);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it < 0) return;
+        const int nst = stages_of(a.blocks[a.items[it].blk].k, kStageK);
+        if (nst == 0) {  // an empty block id: zeros (cpu_backend.cpp:234)
+            const ItemOut o = item_out<kGrouped>(a, it, r, h, kCols);
+            if (o.i < o.P)
+                for (int c = 0; c < kCols; ++c) {
+                    const int j = o.j0 + c;
+                    if (j >= o.P || (o.diag && j < o.i)) continue;
+                    o.f2[o.slab + o.i + static_cast<int64_t>(o.P) * j] = 0.0;
+                    o.vp[o.slab + o.i + static_cast<int64_t>(o.P) * j] = 0.0;
+                    o.f2[o.slab + j + static_cast<int64_t>(o.P) * o.i] = 0.0;
+                    o.vp[o.slab + j + static_cast<int64_t>(o.P) * o.i] = 0.0;
+                }
+            stamp<kGrouped>(a, o.grp, lane);
+            continue;
+        }
+        // This thread's counts: column c of its part at vpt + c * 128 (+ lane). Pull the
+        // warp's 32 lines into L2 while the MMAs run.
+        const int32_t* vpt = a.vpc + static_cast<int64_t>(it) * kVpTileInts + (h * kCols) * kTile + q * 32;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(vpt + lane * kTile));
+#pragma unroll
+        for (int c = 0; c < kCols; ++c) acc[c] = 0.0;
+        const int nseg = (nst + kSegStages - 1) / kSegStages;
+        for (int sg = 0; sg < nseg; ++sg) {
+            bool ok = true;
+            if (lane == 0) ok = waitb(&ctl->acc_full[0], cs & 1u, ctl, a);
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) return;
+            tc_fence_after();
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const double ws = w == 0 ? 1.0 : (w == 1 ? 256.0 : (w == 2 ? 65536.0 : 16777216.0));
+#pragma unroll
+                for (int g8 = 0; g8 < kCols / 8; ++g8) {
+                    uint32_t v[8];
+                    tmem_ld8(tmem + lane_addr + static_cast<uint32_t>(w) * 128u + col_addr + static_cast<uint32_t>(g8) * 8u,
+                             v);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int c = 0; c < 8; ++c)
+                        acc[g8 * 8 + c] = fma(static_cast<double>(static_cast<int32_t>(v[c])), ws, acc[g8 * 8 + c]);
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&ctl->acc_empty[0]);
+            ++cs;
+        }
+        // Output: (i, j) straight from registers (32 consecutive i per store: full sectors);
+        // (j, i) through this warp's staging tile (4 rows x 8 consecutive j per store).
+        const ItemOut o = item_out<kGrouped>(a, it, r, h, kCols);
+        const int P = o.P, i = o.i, i0 = o.i0, j0 = o.j0;
+        const bool diag = o.diag;
+        const int64_t row_i = o.slab + i;
+        const int64_t row_j0 = o.slab + static_cast<int64_t>(P) * i0;
+#pragma unroll
+        for (int q8 = 0; q8 < kCols / 8; ++q8) {
+            int32_t vpi[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) vpi[c] = __ldg(vpt + (q8 * 8 + c) * kTile + lane);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int col = q8 * 8 + c;
+                const int j = j0 + col;
+                const int32_t vk = vpi[c] < a.rcp_max ? vpi[c] : a.rcp_max;
+                acc[col] = vk > 0 ? acc[col] * kFxNumScale * __ldg(a.rcp + vk) : 0.0;  // f2, in place
+                if (i < P && j < P && !(diag && j < i)) {
+                    const int64_t ij = row_i + static_cast<int64_t>(P) * j;
+                    __stcs(o.f2 + ij, acc[col]);
+                    __stcs(o.vp + ij, static_cast<double>(vpi[c]));
+                }
+            }
+            const int jj = j0 + q8 * 8 + (lane & 7);
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+                double* out = part == 0 ? o.f2 : o.vp;
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    stage[lane * kStagePitch + c] = part == 0 ? acc[q8 * 8 + c] : static_cast<double>(vpi[c]);
+                __syncwarp();
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int rr = 4 * k + (lane >> 3);
+                    if (i0 + rr < P && jj < P && !(diag && jj <= i0 + rr))
+                        __stcs(out + row_j0 + static_cast<int64_t>(P) * rr + jj, stage[rr * kStagePitch + (lane & 7)]);
+                }
+                __syncwarp();
+            }
+            // Keep the next group's count loads after this group's stores (they would
+            // otherwise all be hoisted, and held, at once).
+            asm volatile("" ::: "memory");
+        }
+        stamp<kGrouped>(a, o.grp, lane);
+    }
+}
+
+template <bool kGrouped>
+// 18 warps put five on two SM sub-partitions: at most 96 registers per thread.
+__global__ void __maxnreg__(96)
+f2_fx_kernel(const __grid_constant__ FxArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    FxCtl* ctl = reinterpret_cast<FxCtl*>(smem + kStages * kStageBytes);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        init_ring(ctl, 1 + kEpiWarps);  // the issuer and every epilogue warp
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&ctl->full[s], 1);
+            mbar_init(&ctl->empty[s], 1);
+        }
+        mbar_init(&ctl->acc_full[0], 1);
+        mbar_init(&ctl->acc_empty[0], kEpiWarps);
+        mbar_init(&ctl->drain, 1);
+        ctl->abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) tmem_alloc(&ctl->tmem_base, kTmemCols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = ctl->tmem_base;
+    if (warp < kEpiWarp0) {
+        if (warp == 0 && lane == 0) fx_producer<kGrouped>(a, smem, ctl);
+        if (warp == 1 && lane == 0) fx_issuer(a, smem, ctl, tmem);
+    } else {
+        fx_epilogue<kGrouped>(a, ctl, tmem, warp, lane,
+                              reinterpret_cast<double*>(smem + kStages * kStageBytes + kCtlBytes) +
+                                  (warp - kEpiWarp0) * kStageDoubles);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem, kTmemCols);
+}
+
+constexpr size_t kFxSmemBytes = kStages * kStageBytes + kCtlBytes + kEpiWarps * kStageDoubles * sizeof(double) + 1024;
+
+// ============================== vpair kernel ==============================================
+
+template <bool kGrouped>
+__device__ void vp_producer(const FxArgs& a, uint8_t* smem, FxCtl* ctl) {
+    uint32_t g = 0;
+    for (uint32_t gi = 0;; ++gi) {
+        bool ok = true;
+        const int it = take_item(a, ctl, gi, ok);
+        if (!ok) goto abort;
+        if (it < 0) break;
+        {
+            const WorkItem w = a.items[it];
+            const BlockInfo bi = a.blocks[w.blk];
+            const int nch = stages_of(bi.k, kStageK);
+            const bool diag = w.ti == w.tj;
+            const uint8_t* mt = a.mtiles;
+            int64_t n_ck = a.n_ck;
+            if constexpr (kGrouped) {
+                mt = a.groups[bi.grp].mtiles;
+                n_ck = a.groups[bi.grp].n_ck;
+            }
+            for (int c0 = 0; c0 < nch; c0 += kVpChunks, ++g) {
+                const uint32_t bytes = static_cast<uint32_t>(min(kVpChunks, nch - c0)) * static_cast<uint32_t>(kTile8Bytes);
+                const int slot = static_cast<int>(g % kVpStages);
+                if (!waitb(&ctl->empty[slot], ((g / kVpStages) & 1u) ^ 1u, ctl, a)) goto abort;
+                uint8_t* sb = smem + slot * kVpStageBytes;
+                mbar_expect_tx(&ctl->full[slot], diag ? bytes : 2 * bytes);
+                const int64_t chunk = bi.col / kStageK + c0;
+                bulk_load(sb, mt + (static_cast<int64_t>(w.ti) * n_ck + chunk) * kTile8Bytes, bytes, &ctl->full[slot]);
+                if (!diag)
+                    bulk_load(sb + kVpSide, mt + (static_cast<int64_t>(w.tj) * n_ck + chunk) * kTile8Bytes, bytes,
+                              &ctl->full[slot]);
+            }
+        }
+    }
+    return;
+abort:
+    for (uint32_t k = (g >= kVpStages ? g - kVpStages : 0); k < g; ++k)
+        waitb(&ctl->full[k % kVpStages], (k / kVpStages) & 1u, ctl, a, false);
+}
+
+__device__ void vp_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t tmem) {
+    uint32_t g = 0, n_acc = 0;
+    for (uint32_t gi = 0;; ++gi) {
+        const int it = read_item(a, ctl, gi);
+        if (it < 0) break;
+        const WorkItem w = a.items[it];
+        const int nch = stages_of(a.blocks[w.blk].k, kStageK);
+        if (nch == 0) continue;
+        const bool diag = w.ti == w.tj;
+        const int b = static_cast<int>(n_acc % kVpAcc);
+        if (!waitb(&ctl->acc_empty[b], ((n_acc / kVpAcc) & 1u) ^ 1u, ctl, a)) goto done;
+        tc_fence_after();
+        {
+            const uint32_t d = tmem + static_cast<uint32_t>(b) * 128u;
+            for (int c0 = 0; c0 < nch; c0 += kVpChunks, ++g) {
+                const int slot = static_cast<int>(g % kVpStages);
+                if (!waitb(&ctl->full[slot], (g / kVpStages) & 1u, ctl, a)) goto done;
+                tc_fence_after();
+                const uint32_t sa = smem_u32(smem + slot * kVpStageBytes);
+                const uint32_t sb = diag ? sa : sa + kVpSide;
+                const int n = min(kVpChunks, nch - c0);
+                for (int j = 0; j < n; ++j)
+                    mma_i8(d, smem_desc(sa + static_cast<uint32_t>(j) * 4096u, 256, 6),
+                           smem_desc(sb + static_cast<uint32_t>(j) * 4096u, 256, 6), a.idesc, (c0 + j) > 0 ? 1u : 0u);
+                mma_commit(&ctl->empty[slot]);
+            }
+        }
+        mma_commit(&ctl->acc_full[b]);
+        ++n_acc;
+    }
+done:
+    mma_commit(&ctl->drain);
+    waitb(&ctl->drain, 0u, ctl, a, false);
+}
+
+__device__ void vp_epilogue(const FxArgs& a, FxCtl* ctl, uint32_t tmem, int warp, int lane) {
+    const int q = warp & 3;
+    const int h = (warp - 2) >> 2;  // column half
+    const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
+    uint32_t n_acc = 0;
+    for (uint32_t gi = 0;; ++gi) {
+        int it = 0;
+        if (lane == 0) it = read_item(a, ctl, gi);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it < 0) return;
+        if (stages_of(a.blocks[a.items[it].blk].k, kStageK) == 0) continue;  // the f2 kernel writes zeros
+        const int b = static_cast<int>(n_acc % kVpAcc);
+        bool ok = true;
+        if (lane == 0) ok = waitb(&ctl->acc_full[b], (n_acc / kVpAcc) & 1u, ctl, a);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) return;
+        tc_fence_after();
+        int32_t* dst = a.vpc + static_cast<int64_t>(it) * kVpTileInts + (h * kVpCols) * kTile + q * 32 + lane;
+#pragma unroll
+        for (int half = 0; half < kVpCols / 32; ++half) {
+            uint32_t v[32];
+            tmem_ld32(tmem + lane_addr + static_cast<uint32_t>(b) * 128u + static_cast<uint32_t>(h * kVpCols + half * 32),
+                      v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int c = 0; c < 32; ++c) dst[(half * 32 + c) * kTile] = static_cast<int32_t>(v[c]);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&ctl->acc_empty[b]);
+        ++n_acc;
+    }
+}
+
+template <bool kGrouped>
+__global__ void __launch_bounds__(kVpThreads, 1) vpair_fx_kernel(const __grid_constant__ FxArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    FxCtl* ctl = reinterpret_cast<FxCtl*>(smem + kVpStages * kVpStageBytes);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        init_ring(ctl, 1 + kVpEpiWarps);
+        for (int s = 0; s < kVpStages; ++s) {
+            mbar_init(&ctl->full[s], 1);
+            mbar_init(&ctl->empty[s], 1);
+        }
+        for (int b = 0; b < kVpAcc; ++b) {
+            mbar_init(&ctl->acc_full[b], 1);
+            mbar_init(&ctl->acc_empty[b], kVpEpiWarps);
+        }
+        mbar_init(&ctl->drain, 1);
+        ctl->abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) tmem_alloc(&ctl->tmem_base, kTmemCols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = ctl->tmem_base;
+    if (warp < 2) {
+        if (warp == 0 && lane == 0) vp_producer<kGrouped>(a, smem, ctl);
+        if (warp == 1 && lane == 0) vp_issuer(a, smem, ctl, tmem);
+    } else {
+        vp_epilogue(a, ctl, tmem, warp, lane);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem, kTmemCols);
+}
+
+constexpr size_t kVpSmemBytes = kVpStages * kVpStageBytes + kCtlBytes + 1024;
+
+// kind::i8 instruction descriptor: D = s32, A = B = s8, K-major A and B, N >> 3 at bit
+// 17, M >> 4 at bit 24.
+uint32_t idesc_s8_s32() { return (2u << 4) | (1u << 7) | (1u << 10) | ((kTile >> 3) << 17) | ((kTile >> 4) << 24); }
+
+void set_fx_smem() {
+    const int b = static_cast<int>(kFxSmemBytes), v = static_cast<int>(kVpSmemBytes);
+    STPF2_CUDA(cudaFuncSetAttribute(f2_fx_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    STPF2_CUDA(cudaFuncSetAttribute(f2_fx_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    STPF2_CUDA(cudaFuncSetAttribute(vpair_fx_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v));
+    STPF2_CUDA(cudaFuncSetAttribute(vpair_fx_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v));
+}
+
+}  // namespace
+
+size_t fx_vpc_bytes(int n_items) { return static_cast<size_t>(std::max(n_items, 1)) * kVpTileInts * sizeof(int32_t); }
+
+void fx_prepare() { set_fx_smem(); }
+
+void launch_fx(Ctx& c, const FxLaunch& L, cudaStream_t s) {
+    if (L.n_items <= 0) return;
+    FxArgs a{};
+    a.images = L.images;
+    a.mtiles = L.mtiles;
+    a.n_ck = L.n_ck;
+    a.items = L.items;
+    a.n_items = L.n_items;
+    a.blocks = L.blocks;
+    a.P = L.P;
+    a.f2 = L.f2;
+    a.vpair = L.vpair;
+    a.vpc = L.vpc;
+    a.rcp = L.rcp;
+    a.rcp_max = L.rcp_max;
+    a.err = L.err;
+    a.b_base = L.b_base;
+    a.idesc = idesc_s8_s32();
+    a.timeout_ns = c.fx_tuning.timeout_ns;
+    a.withhold = -1;
+    a.groups = L.groups;
+    a.grp_done = L.grp_done;
+    a.grp_ns = L.grp_ns;
+    a.grp_items = L.grp_items;
+    const int grid = std::min(c.sm_count, L.n_items);
+    // Two work-item counters: one per kernel.
+    STPF2_CUDA(cudaMemsetAsync(L.counters, 0, 2 * sizeof(int), s));
+    a.next_item = L.counters;
+    if (L.groups) vpair_fx_kernel<true><<<grid, kVpThreads, kVpSmemBytes, s>>>(a);
+    else vpair_fx_kernel<false><<<grid, kVpThreads, kVpSmemBytes, s>>>(a);
+    STPF2_CUDA(cudaGetLastError());
+    c.launches++;
+    a.next_item = L.counters + 1;
+    a.withhold = c.fx_tuning.withhold_stage;  // test hook: starves the f2 kernel's issuer
+    if (L.groups) f2_fx_kernel<true><<<grid, kThreads, kFxSmemBytes, s>>>(a);
+    else f2_fx_kernel<false><<<grid, kThreads, kFxSmemBytes, s>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cudaFuncAttributes fa{};
+        cudaFuncGetAttributes(&fa, f2_fx_kernel<false>);
+        fail(STP_CUDA_ERROR, std::string("f2_fx_kernel launch: ") + cudaGetErrorString(e) + " (regs " +
+                                 std::to_string(fa.numRegs) + ", dyn smem " + std::to_string(kFxSmemBytes) + ", local " +
+                                 std::to_string(fa.localSizeBytes) + ")");
+    }
+    c.launches++;
+}
+
+}  // namespace stpf2

@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "stpf2_internal.cuh"
+#include "umma_ptx.cuh"
 
 namespace stpf2 {
 
@@ -57,7 +58,6 @@ constexpr int kCols = 4 * kTile / kEpiWarps;        // tile columns per epilogue
 // registers per thread (96 in allocation steps); 32 FP64 accumulators per thread fit.
 // Four epilogue warps per TMEM lane quarter keep enough tensor-memory loads in flight.
 constexpr uint32_t kTmemCols = 512;
-constexpr unsigned long long kTimeoutNs = 4000000000ull;
 // Per-epilogue-warp staging tile for the transposed stores (f2, then vpair): 32 rows x 8
 // columns, rows padded to 9 doubles (fewer bank conflicts).
 constexpr int kStagePitch = 9;
@@ -103,129 +103,14 @@ struct SmemCtl {
     volatile int abort;
 };
 
-// ---- PTX wrappers ---------------------------------------------------------------------
+// ---- PTX wrappers (umma_ptx.cuh) ---------------------------------------------------------
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
+using namespace ptx;
 
-__device__ __forceinline__ unsigned long long globaltimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long* b, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
-    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(b))
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, uint32_t bytes) {
-    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
-                     smem_u32(b)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(b)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait: false on timeout (which also raises the CTA's abort flag and the global
-// error flag) or when another role of this CTA has already aborted.
+// Bounded wait honouring this CTA's abort flag.
 __device__ __forceinline__ bool wait_bounded(unsigned long long* b, uint32_t parity, SmemCtl* ctl, int* err,
                                           bool honour_abort = true) {
-    if (mbar_try_wait(b, parity)) return true;
-    const unsigned long long t0 = globaltimer();
-    for (uint32_t it = 1;; ++it) {
-        if (mbar_try_wait(b, parity)) return true;
-        if ((it & 63u) == 0) {
-            if (honour_abort && ctl->abort) return false;
-            if (globaltimer() - t0 > kTimeoutNs) {
-                ctl->abort = 1;
-                atomicExch(err, 1);
-                return false;
-            }
-        }
-    }
-}
-
-// Plain bulk copy global -> shared, completing on an mbarrier (no tensor map, no
-// multicast): size and both addresses multiples of 16 bytes.
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void mma_f16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
-        "l"(a), "l"(b), "r"(idesc), "r"(acc)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_i8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
-        "l"(a), "l"(b), "r"(idesc), "r"(acc)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(unsigned long long* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-// 32 lanes x 32 consecutive 32-bit TMEM columns -> 32 registers per thread.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-// UMMA shared-memory descriptor, K-major, swizzled: start address, LBO (unused for a
-// single swizzle atom along K, encoded 1), SBO = byte distance between 8-row groups,
-// descriptor version 1 (sm_100), layout type (4 = 64B swizzle, 6 = 32B swizzle).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo_bytes, uint64_t layout) {
-    return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (1ull << 16) |
-           (static_cast<uint64_t>(sbo_bytes >> 4) << 32) | (1ull << 46) | (layout << 61);
+    return ptx::wait_bounded(b, parity, &ctl->abort, err, kTimeoutNs, honour_abort);
 }
 
 // ---- roles -------------------------------------------------------------------------------
@@ -641,8 +526,10 @@ void launch_kernel(int chunk_stages, bool grouped, int grid, const UmmaArgs& a, 
 
 struct UmmaPlan {
     const uint8_t* images = nullptr;
+    const uint8_t* mtiles = nullptr;  // FX: the 0/1 m tiles of the vpair contraction
     int64_t n_ck = 0;
     DevBuf items, blocks, err, rcp, block_items, counter;
+    DevBuf vpc;  // FX: compact vpair tiles, one per item of the largest launch
     std::vector<int> block_item_off;  // per block: its tile pairs in block_items
     int n_items = 0;
     int rcp_max = 0;
@@ -655,7 +542,7 @@ struct UmmaPlan {
 int umma_tile() { return kTile; }
 
 UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L, int chunk_stages) {
-    if (op.fmt == OpFmt::F32) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs split 16-bit planes");
+    if (op.fmt == OpFmt::F32) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs tiled operand images");
     auto p = std::make_unique<UmmaPlan>();
     if (chunk_stages != 1 && chunk_stages != 2) fail(STP_INVALID_ARGUMENT, "chunk stages must be 1 or 2");
     p->P = op.P;
@@ -694,7 +581,13 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
     if (op.n_rt <= 0 || op.n_ck <= 0) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs tiled planes");
     p->images = static_cast<const uint8_t*>(op.planes);
     p->n_ck = op.n_ck;
-    set_umma_smem();
+    if (op.fmt == OpFmt::FX) {
+        p->mtiles = op.mtiles;
+        p->vpc.reserve(fx_vpc_bytes(p->n_items));
+        fx_prepare();
+    } else {
+        set_umma_smem();
+    }
     return p.release();
 }
 
@@ -726,6 +619,26 @@ void launch_f2_umma_blocks(Ctx& c, UmmaPlan* p, int b0, int b1, double* f2, doub
 
 void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, double* f2, double* vpair,
                        cudaStream_t s, int b_base) {
+    if (p->fmt == OpFmt::FX) {
+        FxLaunch L;
+        L.images = p->images;
+        L.mtiles = p->mtiles;
+        L.n_ck = p->n_ck;
+        L.items = items;
+        L.n_items = n_items;
+        L.blocks = p->blocks.as<BlockInfo>();
+        L.P = p->P;
+        L.f2 = f2;
+        L.vpair = vpair;
+        L.vpc = p->vpc.as<int32_t>();
+        L.rcp = p->rcp.as<double>();
+        L.rcp_max = p->rcp_max;
+        L.err = p->err.as<int>();
+        L.counters = p->counter.as<int>();
+        L.b_base = b_base;
+        launch_fx(c, L, s);
+        return;
+    }
     UmmaArgs a{};
     a.b_base = b_base;
     a.images = p->images;
@@ -763,7 +676,7 @@ void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, 
 
 void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stages, const std::vector<GroupSpec>& groups,
                             cudaStream_t s, std::vector<unsigned long long>* stamps) {
-    if (fmt == OpFmt::F32) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs split 16-bit planes");
+    if (fmt == OpFmt::F32) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs tiled operand images");
     if (chunk_stages != 1 && chunk_stages != 2) fail(STP_INVALID_ARGUMENT, "chunk stages must be 1 or 2");
     const int G = static_cast<int>(groups.size());
     if (stamps) stamps->assign(static_cast<size_t>(G), 0ull);
@@ -814,6 +727,8 @@ void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stage
     const size_t o_ns = pk.add(static_cast<size_t>(G) * sizeof(unsigned long long));
     const size_t o_err = pk.add(16);
     const size_t o_counter = pk.add(16);
+    const bool fx = fmt == OpFmt::FX;
+    if (fx) c.ws_vpc.reserve(fx_vpc_bytes(static_cast<int>(items.size())));
     c.pin_items.reserve(staged);
     c.ws_items.reserve(pk.end);
     uint8_t* h = c.pin_items.as<uint8_t>();
@@ -825,6 +740,29 @@ void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stage
     uint8_t* d = c.ws_items.as<uint8_t>();
     STPF2_CUDA(cudaMemcpyAsync(d, h, staged, cudaMemcpyHostToDevice, s));
     STPF2_CUDA(cudaMemsetAsync(d + staged, 0, pk.end - staged, s));
+    if (fx) {
+        fx_prepare();
+        FxLaunch L;
+        L.images = info[ord[0]].images;
+        L.mtiles = info[ord[0]].mtiles;
+        L.n_ck = info[ord[0]].n_ck;
+        L.P = info[ord[0]].P;
+        L.f2 = info[ord[0]].f2;
+        L.vpair = info[ord[0]].vpair;
+        L.items = reinterpret_cast<const WorkItem*>(d + o_items);
+        L.n_items = static_cast<int>(items.size());
+        L.blocks = reinterpret_cast<const BlockInfo*>(d + o_blocks);
+        L.vpc = c.ws_vpc.as<int32_t>();
+        L.rcp = reinterpret_cast<const double*>(d + o_rcp);
+        L.rcp_max = max_k;
+        L.err = reinterpret_cast<int*>(d + o_err);
+        L.counters = reinterpret_cast<int*>(d + o_counter);
+        L.groups = reinterpret_cast<const GroupInfo*>(d + o_info);
+        L.grp_done = reinterpret_cast<int*>(d + o_done);
+        L.grp_ns = reinterpret_cast<unsigned long long*>(d + o_ns);
+        L.grp_items = reinterpret_cast<const int*>(d + o_nitems);
+        launch_fx(c, L, s);
+    } else {
     set_umma_smem();
 
     UmmaArgs a{};
@@ -853,6 +791,7 @@ void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stage
     launch_kernel(chunk_stages, true, grid, a, s);
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
+    }
     int err = 0;
     STPF2_CUDA(cudaMemcpyAsync(&err, d + o_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (stamps)

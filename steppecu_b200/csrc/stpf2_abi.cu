@@ -129,6 +129,7 @@ size_t operand_plane_bytes(OpFmt f, int P, int64_t ld) {
         return align256(2 * pl * 4) + align256(pl);
     }
     const size_t tiles = static_cast<size_t>((P + kTileRows - 1) / kTileRows) * static_cast<size_t>(ld / kTileK);
+    if (f == OpFmt::FX) return align256(tiles * (kFxImageBytes + kTile8Bytes));  // images, then the M tiles
     return align256(tiles * kImageBytes);
 }
 
@@ -147,6 +148,8 @@ void bind_operand_planes(OperandPlanes& op, OpFmt f, int P, int64_t ld, void* ba
         op.n_rt = (P + kTileRows - 1) / kTileRows;
         op.n_ck = ld / kTileK;
         op.m_u8 = nullptr;  // the int8 M tiles live inside the operand images
+        op.mtiles = f == OpFmt::FX ? static_cast<uint8_t*>(base) + static_cast<size_t>(op.n_rt) * op.n_ck * kFxImageBytes
+                                   : nullptr;
     }
 }
 
@@ -155,13 +158,16 @@ void bind_operand_planes(OperandPlanes& op, OpFmt f, int P, int64_t ld, void* ba
 struct Plan {
     Ctx* ctx = nullptr;
     int P = 0;
-    int64_t n_sel = 0, n_snp = 0;
+    int64_t n_sel = 0, n_snp = 0;  // n_snp: the request's SNP axis (the kept SNPs with kept_rows)
+    int64_t n_rec = 0;             // genotype records (the ploidy window and record copies span these)
     uint64_t pitch = 0;
     int precision = 0;
     bool detect = false;
     BlockLayout L;
     DevBuf sel, pop_off, pos, tiles, col_snp, rec_n, rec_nm1, canon, center, blocks, items, own_planes, repitched;
     DevBuf fold_order;  // per 64-population group, local indices largest first (null: all equal)
+    DevBuf row_map;     // kept SNP -> record row (empty: SNP s is record s)
+    std::vector<int64_t> kept;  // the same on the host (segment uploads of host records)
     uint64_t* canon_ptr = nullptr;  // canon's storage, or a context workspace (one-shot calls)
     double* center_ptr = nullptr;
     int64_t n_ind = 0, n_tiles = 0, n_sel_pad = 0;
@@ -189,7 +195,8 @@ struct Plan {
     }
 
     int launches() const {
-        const int contract = (per_block && umma) ? static_cast<int>(L.blocks.size()) : 1;
+        int contract = (per_block && umma) ? static_cast<int>(L.blocks.size()) : 1;
+        if (precision == STP_PREC_FIXED_I8) contract *= 2;  // the vpair kernel, then the f2 kernel
         return (detect ? 1 : 0) + 2 + contract;
     }
 };
@@ -200,15 +207,29 @@ namespace {
 // storage (at least operand_plane_bytes) instead of allocating it; borrow_ws takes the
 // canonical genotypes and centres from the context's grow-only workspace as well (for
 // one-shot calls, which finish before the next call on the context starts).
+// The request's SNP axis: its kept SNPs when it names them, else every record.
+int64_t snp_axis(const stp_f2_request& r) { return r.kept_rows ? r.n_kept : r.geno.n_snp; }
+
 std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch, void* planes_base,
-                                 bool borrow_ws = false) {
+                                 bool borrow_ws = false, bool counts_only = false) {
     need(r.n_pop >= 0 && r.geno.n_snp >= 0 && r.n_block >= 0, "negative extent");
     need(r.geno.bytes_per_record > 0 || r.geno.n_snp == 0, "bytes_per_record is 0");
     need(r.pop_offsets != nullptr || r.n_pop == 0, "pop_offsets is NULL");
     auto p = std::make_unique<Plan>();
     p->ctx = &c;
     p->P = r.n_pop;
-    p->n_snp = r.geno.n_snp;
+    p->n_rec = r.geno.n_snp;
+    p->n_snp = snp_axis(r);
+    if (r.kept_rows && p->n_snp > 0) {
+        need(p->n_snp < INT_MAX, "too many kept SNPs");
+        p->kept.assign(r.kept_rows, r.kept_rows + p->n_snp);
+        for (int64_t k = 0; k < p->n_snp; ++k) {
+            need(p->kept[k] >= 0 && p->kept[k] < r.geno.n_snp, "kept_rows entry outside [0, n_snp)");
+            need(k == 0 || p->kept[k] > p->kept[k - 1], "kept_rows must be strictly increasing");
+        }
+        std::vector<int32_t> rm(p->kept.begin(), p->kept.end());
+        upload(p->row_map, rm, c.stream);
+    }
     p->pitch = pitch;
     p->precision = r.precision;
     const OpFmt fmt = fmt_of(r.precision);
@@ -219,7 +240,7 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
         need(r.pop_offsets[i + 1] >= r.pop_offsets[i], "pop_offsets must be non-decreasing");
     need(n_sel == 0 || r.sel_rows != nullptr, "sel_rows is NULL");
     need(n_sel < INT_MAX, "too many selected samples");
-    need(r.block_id != nullptr || r.geno.n_snp == 0, "block_id is NULL");
+    need(r.block_id != nullptr || p->n_snp == 0, "block_id is NULL");
 
     cudaStream_t s = c.stream;
     std::vector<uint32_t> sel(static_cast<size_t>(n_sel));
@@ -287,7 +308,7 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
     upload(p->rec_n, rn, s);
     upload(p->rec_nm1, rnm1, s);
 
-    p->L = make_block_layout(r.block_id, r.geno.n_snp, r.n_block);
+    p->L = make_block_layout(r.block_id, p->n_snp, r.n_block);
     // 32-column tiles of the padded column space (blocks start on 64-column boundaries,
     // so a tile never spans two blocks).
     p->n_tiles = p->L.ld / 32;
@@ -325,9 +346,10 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
                  (r.geno.on_device && reinterpret_cast<uintptr_t>(r.geno.records) % 4 != 0);
     if (p->repitch) {
         p->pitch = (std::max<uint64_t>(r.geno.bytes_per_record, need_bytes) + 15) / 16 * 16;
-        p->repitched.reserve(std::max<size_t>(static_cast<size_t>(p->pitch) * r.geno.n_snp, 64));
+        p->repitched.reserve(std::max<size_t>(static_cast<size_t>(p->pitch) * p->n_rec, 64));
     }
     upload(p->blocks, p->L.blocks, s);
+    if (counts_only) return p;  // decode to counts only: no operand planes, no contraction
 
     const size_t ob = operand_plane_bytes(fmt, std::max(r.n_pop, 1), p->L.ld);
     if (!planes_base) {
@@ -354,21 +376,21 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
 // centres are indexed from t0, for the pipelined host-buffer path; detect runs the ploidy
 // pass first (it reads the first min(1000, M) SNPs).
 void launch_decode(Plan& p, const uint8_t* d_records, int32_t* cnt_ac2, int32_t* cnt_n, cudaStream_t s,
-                   int64_t t0 = 0, int64_t t1 = -1, bool detect = true) {
+                   int64_t t0 = 0, int64_t t1 = -1, bool detect = true, uint32_t* cnt_packed = nullptr) {
     Ctx& c = *p.ctx;
     if (p.n_snp <= 0) return;
     if (t1 < 0) t1 = p.n_tiles;
     const uint8_t* rec = d_records;
     if (p.repitch) {
         STPF2_CUDA(cudaMemcpy2DAsync(p.repitched.ptr, p.pitch, d_records, p.src_pitch, p.bpr,
-                                     static_cast<size_t>(p.n_snp), cudaMemcpyDeviceToDevice, s));
+                                     static_cast<size_t>(p.n_rec), cudaMemcpyDeviceToDevice, s));
         rec = p.repitched.as<uint8_t>();
     }
     if (p.detect && detect)
-        launch_detect_ploidy_words(c, rec, p.pitch, p.n_snp, p.n_ind, p.pos.as<int32_t>(), p.sel.as<uint32_t>(), s);
+        launch_detect_ploidy_words(c, rec, p.pitch, p.n_rec, p.n_ind, p.pos.as<int32_t>(), p.sel.as<uint32_t>(), s);
     if (t1 <= t0) return;
     launch_transpose_pa(c, rec, p.pitch, p.n_ind, p.tiles.as<TileInfo>() + t0, t1 - t0, p.pos.as<int32_t>(),
-                        p.n_sel_pad, p.canon_ptr, p.center_ptr + t0 * kTileK, s);
+                        p.n_sel_pad, p.canon_ptr, p.center_ptr + t0 * kTileK, s, p.row_map.as<int32_t>());
     CanonDecodeArgs a;
     a.canon = p.canon_ptr;
     a.n_tiles = t1 - t0;
@@ -385,6 +407,11 @@ void launch_decode(Plan& p, const uint8_t* d_records, int32_t* cnt_ac2, int32_t*
     if (cnt_ac2) a.op.planes = nullptr;
     a.cnt_ac2 = cnt_ac2;
     a.cnt_n = cnt_n;
+    if (cnt_packed) {
+        a.op.planes = nullptr;
+        a.cnt_packed = cnt_packed;
+        a.cnt_ld = p.n_snp;
+    }
     a.fold_order = p.fold_order.as<int32_t>();
     launch_decode_canon(c, a, s);
 }
@@ -536,16 +563,30 @@ void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, u
         }
     } free_events{ev};
     for (auto& e : ev) STPF2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    int64_t snp0 = 0;
+    int64_t snp0 = 0, rec_end = 0;
     for (size_t k = 0; k < nseg; ++k) {
         const int b0 = bounds[k], b1 = bounds[k + 1];
         int64_t nsnp = 0;
         for (int b = b0; b < b1; ++b) nsnp += L.blocks[b].k;
+        // The records this segment reads: its SNPs' rows (a run of kept rows spans from the
+        // first to the last), the first segment also the ploidy window; never a row twice.
+        int64_t r0 = snp0, r1 = snp0 + nsnp;
+        if (!p.kept.empty() && nsnp > 0) {
+            r0 = p.kept[static_cast<size_t>(snp0)];
+            r1 = p.kept[static_cast<size_t>(snp0 + nsnp - 1)] + 1;
+        }
+        if (k == 0) {
+            r0 = 0;
+            r1 = std::max<int64_t>(r1, std::min<int64_t>(p.n_rec, 1000));
+        }
+        r0 = std::max(r0, rec_end);
+        r1 = std::max(r1, r0);
+        rec_end = r1;
         const int64_t t0 = L.blocks[b0].col / kTileK;
         const int64_t t1 = (b1 < B ? L.blocks[b1].col : L.ld) / kTileK;
         double* f2k = c.ws_f2.as<double>() + (k % 2) * ring * slab;
         double* vpk = c.ws_vpair.as<double>() + (k % 2) * ring * slab;
-        upload_rows(r.geno, d_rec, dp, snp0, nsnp, c.h2d);
+        upload_rows(r.geno, d_rec, dp, r0, r1 - r0, c.h2d);
         STPF2_CUDA(cudaEventRecord(ev[3 * k], c.h2d));
         STPF2_CUDA(cudaStreamWaitEvent(c.stream, ev[3 * k], 0));
         launch_decode(p, d_rec, nullptr, nullptr, c.stream, t0, t1, k == 0);
@@ -598,7 +639,7 @@ void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
     }
     // Operand planes borrow the context's grow-only workspace.
     {
-        const BlockLayout probe = make_block_layout(r.block_id, r.geno.n_snp, r.n_block);
+        const BlockLayout probe = make_block_layout(r.block_id, snp_axis(r), r.n_block);
         c.ws_misc.reserve(operand_plane_bytes(fmt_of(r.precision), std::max(r.n_pop, 1), probe.ld));
     }
     std::unique_ptr<Plan> p = build_plan(c, r, pitch, c.ws_misc.ptr, true);
@@ -654,7 +695,7 @@ struct BatchMember {
     std::vector<std::vector<int64_t>> keys;  // per population
     std::vector<int32_t> plcode;             // per selected sample: 0/1/2, or 3 = detect
     std::vector<int32_t> upop;               // population -> batch population
-    size_t img_bytes = 0, out_bytes = 0;
+    size_t img_bytes = 0, out_bytes = 0, vpc_bytes = 0;
     OperandPlanes op;
 };
 
@@ -699,6 +740,10 @@ void prepare_member(const stp_f2_request& r, const stp_f2_output& o, int64_t n_i
     }
     m.L = make_block_layout(r.block_id, r.geno.n_snp, r.n_block, false);
     m.img_bytes = align256(operand_plane_bytes(fmt, r.n_pop, m.L.ld));
+    if (fmt == OpFmt::FX) {  // the compact vpair tiles of the member's work items (context workspace)
+        const int64_t T = (r.n_pop + kTileRows - 1) / kTileRows;
+        m.vpc_bytes = fx_vpc_bytes(static_cast<int>(std::min<int64_t>(INT_MAX, r.n_block * T * (T + 1) / 2)));
+    }
     const size_t elems = static_cast<size_t>(r.n_pop) * r.n_pop * r.n_block;
     m.out_bytes = o.on_device ? 0 : 2 * align256(elems * sizeof(double));
 }
@@ -927,13 +972,13 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
     STPF2_CUDA(cudaStreamSynchronize(s));
     size_t free_b = 0, total_b = 0;
     STPF2_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t held = c.ws_batch.bytes + c.ws_f2.bytes + c.ws_vpair.bytes;  // reusable for this batch's images
+    const size_t held = c.ws_batch.bytes + c.ws_f2.bytes + c.ws_vpair.bytes + c.ws_vpc.bytes;  // reusable here
     const size_t avail = free_b + held;
     const size_t budget = avail > (size_t(2) << 30) ? (avail - (size_t(2) << 30)) * 9 / 10 : 0;
     std::vector<std::vector<size_t>> waves(1);
     size_t acc = 0;
     for (size_t m = 0; m < mem.size(); ++m) {
-        const size_t b = mem[m].img_bytes + mem[m].out_bytes;
+        const size_t b = mem[m].img_bytes + mem[m].out_bytes + mem[m].vpc_bytes;
         if (!waves.back().empty() && acc + b > budget) {
             waves.emplace_back();
             acc = 0;
@@ -972,7 +1017,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
                 oo += p.out_bytes / 2;
             }
             specs[w].L = &p.L;
-            specs[w].info = GroupInfo{static_cast<const uint8_t*>(p.op.planes), f2, vp, p.op.n_ck, p.P, 0};
+            specs[w].info = GroupInfo{static_cast<const uint8_t*>(p.op.planes), f2, vp, p.op.n_ck, p.P, 0, p.op.mtiles};
             if (o.block_sizes) copy_block_sizes(p.L, o.block_sizes);
         }
         std::vector<unsigned long long> stamps;
@@ -1128,6 +1173,173 @@ stp_status stp_decode_counts(stp_ctx* ctx, const stp_geno_view* geno, const int6
         launch_decode(*p, d_rec, d_ac2.as<int32_t>(), d_n.as<int32_t>(), s);
         STPF2_CUDA(cudaMemcpyAsync(ac2, d_ac2.ptr, cnt * 4, cudaMemcpyDeviceToHost, s));
         STPF2_CUDA(cudaMemcpyAsync(n, d_n.ptr, cnt * 4, cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+namespace {
+
+void check_filter(const stp_snp_filter* f) {
+    need(f != nullptr, "filter is NULL");
+    need(f->strand_mode >= STP_STRAND_DROP && f->strand_mode <= STP_STRAND_FLIP, "unknown strand_mode");
+    need(f->maxmiss == f->maxmiss && f->maf_min == f->maf_min, "filter thresholds must not be NaN");
+}
+
+// The .snp columns the keep mask reads, on the device.
+struct SnpColumns {
+    DevBuf ref, alt, chrom;
+    SnpColumns(const char* r, const char* a, const int32_t* c, int64_t M, cudaStream_t s) {
+        need(r && a && c, "ref / alt / chrom is NULL");
+        ref.reserve(static_cast<size_t>(M));
+        alt.reserve(static_cast<size_t>(M));
+        chrom.reserve(static_cast<size_t>(M) * 4);
+        STPF2_CUDA(cudaMemcpyAsync(ref.ptr, r, static_cast<size_t>(M), cudaMemcpyHostToDevice, s));
+        STPF2_CUDA(cudaMemcpyAsync(alt.ptr, a, static_cast<size_t>(M), cudaMemcpyHostToDevice, s));
+        STPF2_CUDA(cudaMemcpyAsync(chrom.ptr, c, static_cast<size_t>(M) * 4, cudaMemcpyHostToDevice, s));
+    }
+};
+
+}  // namespace
+
+stp_status stp_snp_keep_mask(stp_ctx* ctx, const stp_geno_view* geno, const int64_t* sel_rows,
+                             const int64_t* pop_offsets, int32_t n_pop, const int32_t* sample_ploidy,
+                             int32_t ploidy_mode, const char* ref, const char* alt, const int32_t* chrom,
+                             const stp_snp_filter* filter, uint8_t* keep, int64_t* n_kept, double* summary) {
+    return guarded([&] {
+        need(ctx && geno && n_kept, "null argument");
+        use_device(*ctx);
+        check_filter(filter);
+        *n_kept = 0;
+        const int64_t M = geno->n_snp;
+        if (M <= 0) return;
+        need(keep != nullptr, "keep is NULL");
+        need(M <= INT_MAX, "n_snp exceeds INT_MAX (M > INT_MAX is not supported)");
+        cudaStream_t s = ctx->stream;
+        SnpColumns cols(ref, alt, chrom, M, s);
+        DevBuf d_keep, d_sum;
+        d_keep.reserve(static_cast<size_t>(M));
+        if (summary) d_sum.reserve(static_cast<size_t>(M) * 4 * sizeof(double));
+        if (n_pop > 0) {
+            // Exact counts of every population at every SNP, population-major (one block over
+            // all SNPs: counts do not depend on the block layout).
+            std::vector<int32_t> bid(static_cast<size_t>(M), 0);
+            stp_f2_request r{};
+            r.geno = *geno;
+            r.sel_rows = sel_rows;
+            r.pop_offsets = pop_offsets;
+            r.n_pop = n_pop;
+            r.sample_ploidy = sample_ploidy;
+            r.ploidy_mode = ploidy_mode;
+            r.block_id = bid.data();
+            r.n_block = 1;
+            r.precision = STP_PREC_FP32_SIMT;
+            const uint8_t* d_rec = geno->records;
+            uint64_t pitch = geno->pitch ? geno->pitch : geno->bytes_per_record;
+            DevBuf rec;
+            if (!geno->on_device) {
+                const uint64_t dp = device_pitch(*geno);
+                rec.reserve(static_cast<size_t>(dp) * M);
+                upload_rows(*geno, rec.as<uint8_t>(), dp, 0, M, s);
+                d_rec = rec.as<uint8_t>();
+                pitch = dp;
+            }
+            std::unique_ptr<Plan> p = build_plan(*ctx, r, pitch, nullptr, false, /*counts_only=*/true);
+            DevBuf cnt;
+            cnt.reserve(static_cast<size_t>(n_pop) * M * 4);
+            launch_decode(*p, d_rec, nullptr, nullptr, s, 0, -1, true, cnt.as<uint32_t>());
+            const double total = static_cast<double>(pop_offsets[n_pop]);
+            launch_keep_mask_counts(*ctx, cnt.as<uint32_t>(), M, n_pop, M, cols.ref.as<char>(), cols.alt.as<char>(),
+                                    cols.chrom.as<int32_t>(), *filter, total, d_keep.as<uint8_t>(),
+                                    summary ? d_sum.as<double>() : nullptr, s);
+            STPF2_CUDA(cudaMemcpyAsync(keep, d_keep.ptr, static_cast<size_t>(M), cudaMemcpyDeviceToHost, s));
+            if (summary)
+                STPF2_CUDA(cudaMemcpyAsync(summary, d_sum.ptr, static_cast<size_t>(M) * 4 * sizeof(double),
+                                           cudaMemcpyDeviceToHost, s));
+            STPF2_CUDA(cudaStreamSynchronize(s));
+        } else {
+            std::fill(keep, keep + M, uint8_t(0));
+        }
+        int64_t k = 0;
+        for (int64_t i = 0; i < M; ++i) k += keep[i] ? 1 : 0;
+        *n_kept = k;
+    });
+}
+
+stp_status stp_decode_af_compact_filter(stp_ctx* ctx, const uint8_t* packed, uint64_t bpr, int64_t n_snp, int64_t n_ind,
+                                        const int64_t* pop_offsets, int32_t n_pop, const int32_t* sample_ploidy,
+                                        int32_t ploidy, int32_t packed_on_device, const char* ref, const char* alt,
+                                        const int32_t* chrom, const stp_snp_filter* filter, double total_indiv,
+                                        uint8_t* keep, int64_t* n_kept, double* q, double* v, double* n,
+                                        int32_t out_on_device) {
+    return guarded([&] {
+        need(ctx != nullptr && n_kept != nullptr, "null argument");
+        use_device(*ctx);
+        check_filter(filter);
+        *n_kept = 0;
+        if (n_pop <= 0 || n_snp <= 0) return;
+        need(keep && pop_offsets, "null argument");
+        need(bpr * 4 >= static_cast<uint64_t>(n_snp), "bytes_per_record too small for n_snp");
+        need(pop_offsets[n_pop] <= n_ind, "pop_offsets exceed n_individuals");
+        need((q == nullptr) == (v == nullptr) && (q == nullptr) == (n == nullptr), "q, v, n: all or none");
+        cudaStream_t s = ctx->stream;
+        DevBuf d_pk, d_pl, d_po, d_q, d_v, d_n, d_keep;
+        const uint8_t* pk = packed;
+        if (!packed_on_device) {
+            d_pk.reserve(static_cast<size_t>(bpr) * std::max<int64_t>(n_ind, 1));
+            STPF2_CUDA(cudaMemcpyAsync(d_pk.ptr, packed, static_cast<size_t>(bpr) * n_ind, cudaMemcpyHostToDevice, s));
+            pk = d_pk.as<uint8_t>();
+        }
+        d_pl.reserve(sizeof(int32_t) * std::max<int64_t>(n_ind, 1));
+        if (sample_ploidy) {
+            STPF2_CUDA(cudaMemcpyAsync(d_pl.ptr, sample_ploidy, sizeof(int32_t) * n_ind, cudaMemcpyHostToDevice, s));
+        } else {
+            std::vector<int32_t> pl(static_cast<size_t>(n_ind), ploidy);
+            upload(d_pl, pl, s);
+        }
+        std::vector<int32_t> po(static_cast<size_t>(n_pop) + 1);
+        for (int i = 0; i <= n_pop; ++i) po[i] = static_cast<int32_t>(pop_offsets[i]);
+        upload(d_po, po, s);
+        const size_t cnt = static_cast<size_t>(n_pop) * n_snp;
+        d_q.reserve(cnt * 8);
+        d_v.reserve(cnt * 8);
+        d_n.reserve(cnt * 8);
+        launch_decode_canonical(*ctx, pk, bpr, n_snp, n_ind, d_po.as<int32_t>(), n_pop, d_pl.as<int32_t>(),
+                                d_q.as<double>(), d_v.as<double>(), d_n.as<double>(), s);
+        SnpColumns cols(ref, alt, chrom, n_snp, s);
+        d_keep.reserve(static_cast<size_t>(n_snp));
+        launch_keep_mask_qn(*ctx, d_q.as<double>(), d_n.as<double>(), n_pop, n_snp, cols.ref.as<char>(),
+                            cols.alt.as<char>(), cols.chrom.as<int32_t>(), *filter, total_indiv, d_keep.as<uint8_t>(),
+                            nullptr, s);
+        STPF2_CUDA(cudaMemcpyAsync(keep, d_keep.ptr, static_cast<size_t>(n_snp), cudaMemcpyDeviceToHost, s));
+        STPF2_CUDA(cudaStreamSynchronize(s));
+        std::vector<int64_t> dst(static_cast<size_t>(n_snp), -1);
+        int64_t k = 0;
+        for (int64_t i = 0; i < n_snp; ++i)
+            if (keep[i]) dst[static_cast<size_t>(i)] = k++;
+        *n_kept = k;
+        if (!q || k == 0) return;
+        DevBuf d_dst, o_q, o_v, o_n;
+        upload(d_dst, dst, s);
+        const size_t out = static_cast<size_t>(n_pop) * k;
+        double* tq = q;
+        double* tv = v;
+        double* tn = n;
+        if (!out_on_device) {
+            o_q.reserve(out * 8);
+            o_v.reserve(out * 8);
+            o_n.reserve(out * 8);
+            tq = o_q.as<double>();
+            tv = o_v.as<double>();
+            tn = o_n.as<double>();
+        }
+        launch_compact_columns(*ctx, d_q.as<double>(), n_pop, n_snp, d_dst.as<int64_t>(), tq, s);
+        launch_compact_columns(*ctx, d_v.as<double>(), n_pop, n_snp, d_dst.as<int64_t>(), tv, s);
+        launch_compact_columns(*ctx, d_n.as<double>(), n_pop, n_snp, d_dst.as<int64_t>(), tn, s);
+        if (!out_on_device) {
+            STPF2_CUDA(cudaMemcpyAsync(q, tq, out * 8, cudaMemcpyDeviceToHost, s));
+            STPF2_CUDA(cudaMemcpyAsync(v, tv, out * 8, cudaMemcpyDeviceToHost, s));
+            STPF2_CUDA(cudaMemcpyAsync(n, tn, out * 8, cudaMemcpyDeviceToHost, s));
+        }
         STPF2_CUDA(cudaStreamSynchronize(s));
     });
 }
@@ -1329,7 +1541,7 @@ stp_status stp_f2_extract_batch(stp_ctx* ctx, const stp_f2_request* reqs, int32_
             if (r.n_pop <= 0 || r.n_block <= 0) continue;
             need(outs[k].f2 != nullptr && outs[k].vpair != nullptr, "output f2 / vpair is NULL");
             fmt_of(r.precision);  // validates the mode
-            if (r.precision == STP_PREC_FP32_SIMT || r.geno.n_snp <= 0) {
+            if (r.precision == STP_PREC_FP32_SIMT || r.geno.n_snp <= 0 || r.kept_rows) {
                 extract_one(*ctx, r, outs[k]);
                 continue;
             }
@@ -1432,6 +1644,15 @@ stp_status stp_fstats(stp_ctx* ctx, const double* f2, const double* vpair, const
         STPF2_CUDA(cudaMemcpyAsync(est, d_est, static_cast<size_t>(m) * 8, cudaMemcpyDeviceToHost, s));
         STPF2_CUDA(cudaMemcpyAsync(var, d_var, static_cast<size_t>(m) * 8, cudaMemcpyDeviceToHost, s));
         STPF2_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+stp_status stp_set_wait_bounds(stp_ctx* ctx, uint64_t timeout_ns, int64_t withhold_stage) {
+    return guarded([&] {
+        need(ctx != nullptr, "null context");
+        need(withhold_stage >= -1, "withhold_stage must be -1 or a stage index");
+        ctx->fx_tuning.timeout_ns = timeout_ns ? timeout_ns : FxTuning{}.timeout_ns;
+        ctx->fx_tuning.withhold_stage = withhold_stage;
     });
 }
 

@@ -95,8 +95,17 @@ struct Packing {
 
 // ---- context --------------------------------------------------------------------------
 
+// Bounded-wait settings of the fixed-point contraction. timeout_ns bounds every device-side
+// wait; withhold_stage >= 0 makes the f2 kernel's producer stop before that stage (a test
+// hook: the issuer's wait then runs out and the call reports STP_DEVICE_TIMEOUT).
+struct FxTuning {
+    unsigned long long timeout_ns = 4000000000ull;
+    long long withhold_stage = -1;
+};
+
 struct Ctx {
     int device = 0;
+    FxTuning fx_tuning;
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     std::atomic<uint64_t> launches{0};
@@ -109,6 +118,7 @@ struct Ctx {
     // the pinned staging of the tables.
     DevBuf ws_batch, ws_union, ws_tables, ws_items;
     DevBuf ws_fstat;  // stp_fstats scratch
+    DevBuf ws_vpc;    // grouped fixed-point batches: compact vpair tiles
     PinnedBuf pin_union, pin_tables, pin_items;
     // Completion time of each request of the last stp_f2_extract_batch call, in ms from the
     // start of its group's device work (NaN for requests that ran on their own).
@@ -132,12 +142,13 @@ struct BlockInfo {  // device-visible, one per jackknife block
 
 // One request of a grouped contraction: its operand images and its output slabs.
 struct GroupInfo {
-    const uint8_t* images;  // (row tile t, chunk c) at (t * n_ck + c) * kImageBytes
+    const uint8_t* images;  // (row tile t, chunk c) at (t * n_ck + c) * kImageBytes (FX: kFxImageBytes)
     double* f2;             // [P x P x n_block]
     double* vpair;
     int64_t n_ck;
     int32_t P;
     int32_t pad_;
+    const uint8_t* mtiles;  // FX: the request's separate M tiles
 };
 
 struct BlockLayout {
@@ -166,7 +177,7 @@ std::vector<WorkItem> make_work_items(const BlockLayout& L, int P, int tile);
 // ---- operand planes --------------------------------------------------------------------
 
 // Operand formats the decode/feeder kernels emit, one per contraction arithmetic.
-enum class OpFmt : int { F32 = 0, BF16 = 1, F16 = 2 };
+enum class OpFmt : int { F32 = 0, BF16 = 1, F16 = 2, FX = 3 };
 
 inline OpFmt fmt_of(int precision) {
     switch (precision) {
@@ -174,6 +185,7 @@ inline OpFmt fmt_of(int precision) {
         case STP_PREC_SPLIT_BF16: return OpFmt::BF16;
         case STP_PREC_SPLIT_F16: return OpFmt::F16;
         case STP_PREC_SPLIT_F16_FINE: return OpFmt::F16;
+        case STP_PREC_FIXED_I8: return OpFmt::FX;
     }
     fail(STP_INVALID_ARGUMENT, "unknown precision mode " + std::to_string(precision));
 }
@@ -198,6 +210,7 @@ struct OperandPlanes {
     int64_t ld = 0;
     void* planes = nullptr;
     uint8_t* m_u8 = nullptr;  // FP32 form only: row-major int8 M
+    uint8_t* mtiles = nullptr;  // FX only: the 0/1 m tiles, (row tile, chunk) 4 KiB each
     double scale_inv = 1.0;  // numerator scale undo (F16 planes are pre-scaled)
     int n_rt = 0;            // tiled: row tiles of 128 populations
     int64_t n_ck = 0;        // tiled: column chunks of 32
@@ -218,6 +231,25 @@ __host__ __device__ inline uint32_t tile8_offset(int r, int k) {
 }
 
 constexpr int kF16PtShift = 7;  // F16: Pt scaled by 2^7, Ah by 2^14 (num by 2^14)
+
+// FX (fixed point, exact integer accumulation): one image per (row tile, chunk) of nine
+// int8 tiles [X0][X1][X2][X3][E3][E4][E5][E6][M] (128 rows x 32 bytes each, the 32-byte
+// swizzle of tile8_offset), where X0..X3 are the balanced base-256 digits of X =
+// round((q - 1/2) * kFxScale), least significant first, E3..E6 those of -A with A =
+// round((x^2 - h) * kFxAScale), and M = kFxM * [n > 0]. The images of all row tiles come
+// first; after them the 0/1 tiles of m = [n > 0] alone, (row tile, chunk) at mtiles +
+// (t * n_ck + c) * 4 KiB,
+// for the vpair contraction. kFxScale = 127 * 2^25 keeps |X| <= 127 * 2^24 (|x| <= 1/2) and
+// kFxAScale = kFxScale^2 / 2^31 keeps |A| < 2^31 (|a| <= 1/4).
+constexpr int kFxPlanes = 9;
+constexpr int64_t kFxImageBytes = kFxPlanes * kTile8Bytes;  // 36 KiB
+constexpr double kFxScale = 127.0 * 33554432.0;     // 127 * 2^25
+constexpr double kFxAScale = 16129.0 * 524288.0;    // kFxScale^2 / 2^31 = 127^2 * 2^19
+constexpr double kFxRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
+constexpr int kFxM = 64;
+// f2 numerator from W = sum_w V_w 2^(8(w-3)) (the four int32 accumulators): num = -2^25 W /
+// kFxScale^2 = -W / (16129 * 2^25).
+constexpr double kFxNumScale = -1.0 / (16129.0 * 33554432.0);
 
 size_t operand_plane_bytes(OpFmt f, int P, int64_t ld);
 void bind_operand_planes(OperandPlanes& op, OpFmt f, int P, int64_t ld, void* base);
@@ -275,9 +307,23 @@ void launch_detect_ploidy_words(Ctx& c, const uint8_t* records, uint64_t pitch, 
                                 const int32_t* pos, uint32_t* sel, cudaStream_t s);
 void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_snp,
                              uint32_t* sel, int64_t n_sel, cudaStream_t s);
+// row_map (optional): record row of every SNP index the tiles name (a kept-SNP compaction).
 void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_ind, const TileInfo* tiles,
                          int64_t n_tiles, const int32_t* pos, int64_t n_sel, uint64_t* canon, double* center,
-                         cudaStream_t s);
+                         cudaStream_t s, const int32_t* row_map = nullptr);
+// extract-f2's per-SNP keep mask (filters.cu): from packed pop-major counts (ac2 | n << 16,
+// population i, SNP s at cnt[i * ld + s]) or from FP64 q / n [P x M] (i + P * s). out4
+// (optional, device [4 * M]): pooled ref AF, pooled minor AF, missing fraction, pooled
+// allele count per SNP.
+void launch_keep_mask_counts(Ctx& c, const uint32_t* cnt, int64_t ld, int P, int64_t M, const char* ref,
+                             const char* alt, const int32_t* chrom, const stp_snp_filter& f, double total_indiv,
+                             uint8_t* keep, double* out4, cudaStream_t s);
+void launch_keep_mask_qn(Ctx& c, const double* Q, const double* N, int P, int64_t M, const char* ref, const char* alt,
+                         const int32_t* chrom, const stp_snp_filter& f, double total_indiv, uint8_t* keep,
+                         double* out4, cudaStream_t s);
+// FP64 [P x M] -> [P x n_kept]: column s goes to column dst_col[s] (-1: dropped).
+void launch_compact_columns(Ctx& c, const double* in, int P, int64_t M, const int64_t* dst_col, double* out,
+                            cudaStream_t s);
 void launch_decode_canon(Ctx& c, const CanonDecodeArgs& a, cudaStream_t s);
 void launch_decode_canonical(Ctx& c, const uint8_t* packed, uint64_t bpr, int64_t n_snp,
                              int64_t n_ind, const int32_t* pop_off, int P, const int32_t* ploidy,
@@ -318,6 +364,35 @@ void launch_emit_counts(Ctx& c, const uint32_t* counts, int64_t cnt_ld, const in
 // umap[g] (a batch's shared ploidy pass).
 void launch_copy_union_ploidy(Ctx& c, uint32_t* desc, const int32_t* umap, int64_t n_sel, const uint32_t* desc_u,
                               cudaStream_t s);
+
+// The fixed-point contraction (f2_fx.cu): vpair_fx_kernel then f2_fx_kernel over the same
+// items. vpc holds fx_vpc_bytes(n_items); counters two ints; groups non-null for a batch.
+struct FxLaunch {
+    const uint8_t* images = nullptr;
+    const uint8_t* mtiles = nullptr;
+    int64_t n_ck = 0;
+    const WorkItem* items = nullptr;
+    int n_items = 0;
+    const BlockInfo* blocks = nullptr;
+    int P = 0;
+    double* f2 = nullptr;
+    double* vpair = nullptr;
+    int32_t* vpc = nullptr;
+    const double* rcp = nullptr;
+    int rcp_max = 0;
+    int* err = nullptr;
+    int* counters = nullptr;
+    int b_base = 0;
+    const GroupInfo* groups = nullptr;
+    int* grp_done = nullptr;
+    unsigned long long* grp_ns = nullptr;
+    const int* grp_items = nullptr;
+};
+size_t fx_vpc_bytes(int n_items);
+// Shared-memory attributes of the fixed-point kernels (the current device); call before the
+// first launch, outside stream capture.
+void fx_prepare();
+void launch_fx(Ctx& c, const FxLaunch& L, cudaStream_t s);
 
 // chunk_stages: 32-SNP stages per FP32 TMEM chunk (1 or 2).
 UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L, int chunk_stages);

@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_library_loads_and_reports_abi_version():
     L = _lib.lib()
-    assert L.stp_abi_version() == 1
+    assert L.stp_abi_version() == 2
 
 
 def test_no_device_is_an_error_not_a_fallback():

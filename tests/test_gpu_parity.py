@@ -15,17 +15,23 @@ from steppecu_b200.synth import write_eigenstrat
 
 pytestmark = pytest.mark.gpu
 
-# Per-arithmetic f2 tolerance (rtol, atol) against the FP64 oracle. Every form sums the
-# numerator in FP32 over short SNP chunks and combines chunks in FP64. Split-F16 keeps ~22
-# mantissa bits per operand and FP32 SIMT 24; split-BF16 (hi+lo) keeps only ~16, so its
-# per-element error is ~2^-17 and its tolerance is wider.
+# Per-arithmetic f2 tolerance (rtol, atol) against the FP64 oracle. The floating forms sum
+# the numerator in FP32 over short SNP chunks and combine chunks in FP64. Split-F16 keeps
+# ~22 mantissa bits per operand and FP32 SIMT 24; split-BF16 (hi+lo) keeps only ~16, so its
+# per-element error is ~2^-17 and its tolerance is wider. The fixed-point form sums exactly
+# in integers over 32-bit fixed-point operands: relative 1e-6 with an absolute floor of
+# 1e-9, i.e. |gpu - oracle| <= 1e-6 * max(|oracle|, 1e-3) up to a factor of two. The floor
+# is 1e-6 of an f2 of 1e-3, an order of magnitude below the per-block f2 values and their
+# sampling spread on these panels, and it is where a relative bound stops meaning anything
+# (f2 estimates cross zero).
 TOL = {
     "fp32": (5e-6, 5e-8),
     "split_f16": (5e-6, 2e-7),
     "split_f16_fine": (5e-6, 2e-7),
     "split_bf16": (3e-4, 3e-6),
+    "fixed_i8": (1e-6, 1e-9),
 }
-MODES = ["fp32", "split_bf16", "split_f16", "split_f16_fine"]
+MODES = ["fp32", "split_bf16", "split_f16", "split_f16_fine", "fixed_i8"]
 TC_DEFAULT = "split_f16"
 
 
@@ -278,12 +284,13 @@ def test_plan_device_resident_matches_one_shot(ctx, c1):
     assert plan.launches >= 2
 
 
-def test_plan_graph_replay_equals_plan_run(ctx, c1):
+@pytest.mark.parametrize("mode", [TC_DEFAULT, "fixed_i8"])
+def test_plan_graph_replay_equals_plan_run(ctx, c1, mode):
     import torch
 
     p, sel, po, _, _ = c1
     rec = torch.as_tensor(p.records_numpy()).cuda()
-    plan = ctx.plan(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision=TC_DEFAULT)
+    plan = ctx.plan(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision=mode)
     n = p.n_pop * p.n_pop * p.n_block
     f_a, v_a = torch.zeros(n, dtype=torch.float64, device="cuda"), torch.zeros(n, dtype=torch.float64, device="cuda")
     plan.run(rec, f_a, v_a)
@@ -300,12 +307,13 @@ def test_plan_graph_replay_equals_plan_run(ctx, c1):
     plan.close()
 
 
-def test_per_block_launches_equal_persistent_launch(ctx, uneven):
+@pytest.mark.parametrize("mode", [TC_DEFAULT, "fixed_i8"])
+def test_per_block_launches_equal_persistent_launch(ctx, uneven, mode):
     import torch
 
     p, sel, po, _, _ = uneven
     rec = torch.as_tensor(p.records_numpy()).cuda()
-    plan = ctx.plan(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision=TC_DEFAULT)
+    plan = ctx.plan(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision=mode)
     n = p.n_pop * p.n_pop * p.n_block
     out = [torch.full((n,), 3.0, dtype=torch.float64, device="cuda") for _ in range(4)]
     plan.run(rec, out[0], out[1])
@@ -313,7 +321,8 @@ def test_per_block_launches_equal_persistent_launch(ctx, uneven):
     before = ctx.launches
     plan.run(rec, out[2], out[3])
     torch.cuda.synchronize()
-    assert ctx.launches - before == plan.launches == 3 + p.n_block
+    per_contraction = 2 if mode == "fixed_i8" else 1  # fixed point: the vpair kernel, then f2
+    assert ctx.launches - before == plan.launches == 3 + per_contraction * p.n_block
     assert torch.equal(out[0], out[2]) and torch.equal(out[1], out[3])
     plan.close()
 
