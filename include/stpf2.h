@@ -198,6 +198,17 @@ stp_status stp_snp_keep_mask(stp_ctx* ctx, const stp_geno_view* geno, const int6
                              int32_t ploidy_mode, const char* ref, const char* alt, const int32_t* chrom,
                              const stp_snp_filter* filter, uint8_t* keep, int64_t* n_kept, double* summary);
 
+/* The canonical individual-major tile of a DecodeTileView (record g: individual g's SNP
+ * codes, MSB-first; bytes_per_record >= ceil(n_snp/4)) rewritten as SNP-major
+ * PACKEDANCESTRYMAP records in device memory, the layout stp_geno_view reads: record s at
+ * d_records + s * pitch holds individual g's code at byte g/4 (pitch >= ceil(n_ind/4)). Lets
+ * a caller holding the reference's tile (extract_f2_core.cpp:113-160) use the record-based
+ * entry points, e.g. the streamed extraction with kept rows (RedecodeSource, the streamed
+ * tiers of src/device/stream_f2_blocks.hpp:44-63). */
+stp_status stp_canonical_to_records(stp_ctx* ctx, const uint8_t* packed, uint64_t bytes_per_record,
+                                    int64_t n_snp, int64_t n_ind, int32_t packed_on_device,
+                                    uint8_t* d_records, uint64_t pitch);
+
 /* ComputeBackend::decode_af_compact_filter (src/device/backend.hpp:914-925) on the
  * canonical individual-major tile (as stp_decode_af): the keep mask of stp_snp_keep_mask
  * over the tile's SNPs (total_indiv: the selection's individual count for the missing
@@ -228,6 +239,38 @@ stp_status stp_decode_af(stp_ctx* ctx, const uint8_t* packed, uint64_t bytes_per
 stp_status stp_f2_from_qvn(stp_ctx* ctx, const double* Q, const double* V, const double* N,
                            int32_t P, int64_t M, const int32_t* block_id, int32_t n_block,
                            int32_t precision, double* f2, double* vpair, int32_t* block_sizes);
+
+/* ComputeBackend::compute_f2_blocks_device (src/device/backend.hpp:694-701): the same as
+ * stp_f2_from_qvn with the result left on the device, d_f2 / d_vpair device buffers of
+ * P*P*n_block doubles (DeviceF2Blocks); Q / V / N are device pointers when qvn_on_device
+ * (a DeviceDecodeResult's q / v / n), host pointers otherwise. */
+stp_status stp_f2_from_qvn_device(stp_ctx* ctx, const double* Q, const double* V, const double* N,
+                                  int32_t P, int64_t M, const int32_t* block_id, int32_t n_block,
+                                  int32_t precision, int32_t qvn_on_device, double* d_f2, double* d_vpair,
+                                  int32_t* block_sizes);
+
+/* Receives one finished run of blocks [b0, b1) of a streamed extraction: (b1 - b0) P x P
+ * slabs of f2 and of vpair in F2BlockTensor order (slab b - b0 at f2 + (b - b0)*P*P), in
+ * host memory that stays valid until the callback returns. Runs arrive in block order on
+ * the calling thread. Return 0 to go on; anything else stops the call with
+ * STP_RUNTIME_ERROR. */
+typedef int (*stp_slab_sink)(void* user, int32_t b0, int32_t b1, const double* f2, const double* vpair);
+
+/* ComputeBackend::compute_f2_blocks_streamed (src/device/backend.hpp:724-734) over dense Q /
+ * V / N: the f2 blocks of stp_f2_from_qvn handed to `sink` in runs of blocks (the reference's
+ * StreamTarget tiers, host RAM or disk), so the whole P x P x n_block tensor never has to
+ * exist on the device or in one host buffer. Tensor-core precisions only. */
+stp_status stp_f2_from_qvn_streamed(stp_ctx* ctx, const double* Q, const double* V, const double* N,
+                                    int32_t P, int64_t M, const int32_t* block_id, int32_t n_block,
+                                    int32_t precision, stp_slab_sink sink, void* user,
+                                    int32_t* block_sizes);
+
+/* The extract-f2 hot path streamed to `sink` (the out-of-core tiers of
+ * src/device/cuda/cuda_backend_f2_blocks.cu:349-603): records (host or device) in, runs of
+ * finished blocks out, two runs in flight. block_sizes (optional host [n_block]).
+ * Tensor-core precisions only. */
+stp_status stp_f2_extract_streamed(stp_ctx* ctx, const stp_f2_request* req, stp_slab_sink sink, void* user,
+                                   int32_t* block_sizes);
 
 /* The extract-f2 hot path: packed genotypes -> ploidy -> decode -> per-block contraction
  * -> FP64 F2BlockTensor (src/app/extract_f2_core.cpp:93-407, Resident tier). With host

@@ -104,6 +104,9 @@ class SnpFilter(C.Structure):
 
 STRAND_DROP, STRAND_KEEP, STRAND_FLIP = 0, 1, 2
 
+# stp_slab_sink: int (*)(void* user, int32_t b0, int32_t b1, const double* f2, const double* vpair)
+SLAB_SINK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double))
+
 # Every symbol include/stpf2.h declares, with its ctypes signature (restype, argtypes).
 _P = C.c_void_p
 SIGNATURES = {
@@ -117,6 +120,12 @@ SIGNATURES = {
     "stp_detect_ploidy_tile": (C.c_int, [_P, _P, C.c_uint64, C.c_int64, C.c_int64, C.c_int32, _P]),
     "stp_decode_counts": (C.c_int, [_P, C.POINTER(GenoView), _P, _P, C.c_int32, _P, C.c_int32, _P, _P]),
     "stp_decode_counts_noalloc": (C.c_int, [_P, C.POINTER(GenoView), _P, _P, C.c_int32, _P, C.c_int32, _P, _P, _P]),
+    "stp_f2_from_qvn_device": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int64, _P, C.c_int32, C.c_int32, C.c_int32,
+                                         _P, _P, _P]),
+    "stp_f2_from_qvn_streamed": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int64, _P, C.c_int32, C.c_int32,
+                                           SLAB_SINK, _P, _P]),
+    "stp_f2_extract_streamed": (C.c_int, [_P, C.POINTER(F2Request), SLAB_SINK, _P, _P]),
+    "stp_canonical_to_records": (C.c_int, [_P, _P, C.c_uint64, C.c_int64, C.c_int64, C.c_int32, _P, C.c_uint64]),
     "stp_snp_keep_mask": (C.c_int, [_P, C.POINTER(GenoView), _P, _P, C.c_int32, _P, C.c_int32, _P, _P, _P,
                                     C.POINTER(SnpFilter), _P, C.POINTER(C.c_int64), _P]),
     "stp_decode_af_compact_filter": (C.c_int, [_P, _P, C.c_uint64, C.c_int64, C.c_int64, _P, C.c_int32, _P, C.c_int32,

@@ -17,7 +17,7 @@ import numpy as np
 from . import _lib as L
 from .blocks import assign_blocks
 from .eigenstrat import read_geno, read_ind, read_snp, select_pops
-from .f2dir import F2Tensor, read_f2_dir, write_f2_dir
+from .f2dir import F2DirWriter, F2Tensor, read_f2_dir, write_f2_dir
 
 PRECISIONS = {
     "fp32": L.PREC_FP32_SIMT, "fp32_simt": L.PREC_FP32_SIMT, "simt": L.PREC_FP32_SIMT,
@@ -213,11 +213,24 @@ class Context:
         return q, v, n
 
     # -- f2 ---------------------------------------------------------------------------------
-    def f2_from_qvn(self, Q, V, N, P: int, block_id, n_block: int, precision=None) -> F2Tensor:
-        """ComputeBackend::compute_f2_blocks(MatView Q, V, N, ...): flat [P x M] inputs."""
+    def f2_from_qvn(self, Q, V, N, P: int, block_id, n_block: int, precision=None, out=None) -> F2Tensor:
+        """ComputeBackend::compute_f2_blocks(MatView Q, V, N, ...): flat [P x M] inputs. With
+        out = (f2, vpair) torch CUDA tensors the result stays on the device
+        (compute_f2_blocks_device, stp_f2_from_qvn_device); Q / V / N may then be torch CUDA
+        tensors too. Returns the F2Tensor, or (f2, vpair, block_sizes) for device output."""
+        bid = _i32(block_id)
+        if out is not None:
+            on_dev = _is_torch_cuda(Q)
+            if not on_dev:
+                Q, V, N = (np.ascontiguousarray(x, dtype=np.float64) for x in (Q, V, N))
+            M = (Q.numel() if on_dev else Q.size) // P if P > 0 else 0
+            bs = np.zeros(max(n_block, 0), np.int32)
+            L.check(L.lib().stp_f2_from_qvn_device(self._h, _data_ptr(Q), _data_ptr(V), _data_ptr(N), P, M, L.ptr(bid),
+                                                   n_block, parse_precision(precision), 1 if on_dev else 0,
+                                                   _data_ptr(out[0]), _data_ptr(out[1]), L.ptr(bs)))
+            return out[0], out[1], bs
         Q, V, N = (np.ascontiguousarray(x, dtype=np.float64) for x in (Q, V, N))
         M = Q.size // P if P > 0 else 0
-        bid = _i32(block_id)
         n = P * P * n_block
         f2 = np.zeros(n)
         vp = np.zeros(n)
@@ -264,6 +277,13 @@ class Context:
                                           L.ptr(summ)))
         k = keep[:M].astype(bool)
         return (k, summ.reshape(4, M)) if summary else k
+
+    def canonical_to_records(self, packed, bytes_per_record: int, n_snp: int, n_ind: int, d_records) -> None:
+        """stp_canonical_to_records: a host canonical individual-major tile into SNP-major
+        records in the torch CUDA uint8 tensor d_records [n_snp, pitch]."""
+        pk = np.ascontiguousarray(packed, dtype=np.uint8)
+        L.check(L.lib().stp_canonical_to_records(self._h, L.ptr(pk), bytes_per_record, n_snp, n_ind, 0,
+                                                 _data_ptr(d_records), int(d_records.shape[1])))
 
     def decode_af_compact_filter(self, packed, bytes_per_record: int, n_snp: int, pop_offsets, ref, alt, chrom,
                                  filt: dict | None = None, sample_ploidy=None, ploidy: int = 2,
@@ -313,6 +333,47 @@ class Context:
         L.check(L.lib().stp_f2_extract_blocks(self._h, C.byref(r), C.byref(o)))
         t = F2Tensor(f2, vp, bs, P, n_block) if not on_dev else (f2, vp, bs)
         return (t, ploidy_out) if return_ploidy else t
+
+    def extract_streamed(self, records, n_ind: int, sel_rows, pop_offsets, block_id, n_block: int, sink,
+                         precision=None, sample_ploidy=None, ploidy="auto", kept_rows=None) -> np.ndarray:
+        """stp_f2_extract_streamed: the extraction handed to sink(b0, b1, f2, vpair) in runs of
+        finished blocks (numpy views of (b1 - b0) * P * P doubles each, valid during the
+        call), so the whole tensor never has to exist. Returns the block sizes."""
+        r = self._request(records, n_ind, sel_rows, pop_offsets, block_id, n_block, precision,
+                          sample_ploidy, ploidy, kept_rows)
+        return self._streamed(lambda cb, bs: L.lib().stp_f2_extract_streamed(self._h, C.byref(r), cb, None, L.ptr(bs)),
+                              r.n_pop, n_block, sink)
+
+    def f2_from_qvn_streamed(self, Q, V, N, P: int, block_id, n_block: int, sink, precision=None) -> np.ndarray:
+        """stp_f2_from_qvn_streamed (compute_f2_blocks_streamed over dense Q/V/N)."""
+        Q, V, N = (np.ascontiguousarray(x, dtype=np.float64) for x in (Q, V, N))
+        M = Q.size // P if P > 0 else 0
+        bid = _i32(block_id)
+        prec = parse_precision(precision)
+        return self._streamed(lambda cb, bs: L.lib().stp_f2_from_qvn_streamed(
+            self._h, L.ptr(Q), L.ptr(V), L.ptr(N), P, M, L.ptr(bid), n_block, prec, cb, None, L.ptr(bs)),
+            P, n_block, sink)
+
+    @staticmethod
+    def _streamed(call, P: int, n_block: int, sink) -> np.ndarray:
+        err: list[BaseException] = []
+
+        def cb(_user, b0, b1, f2p, vpp):
+            try:
+                n = (b1 - b0) * P * P
+                sink(b0, b1, np.ctypeslib.as_array(f2p, (n,)), np.ctypeslib.as_array(vpp, (n,)))
+                return 0
+            except BaseException as e:  # the library stops and reports; re-raised below
+                err.append(e)
+                return 1
+
+        bs = np.zeros(max(n_block, 0), np.int32)
+        keep = L.SLAB_SINK(cb)
+        st = call(keep, bs)
+        if err:
+            raise err[0]
+        L.check(st)
+        return bs
 
     def extract_batch(self, records, n_ind: int, requests, precision=None, out=None) -> list:
         """Many requests over one panel in one call (stp_f2_extract_batch). requests: a sequence
@@ -508,14 +569,20 @@ def context(device: int = 0) -> Context:
 def extract_f2(prefix, *, pops: list[str], out: str | None = None, device: int = 0, blgsize: float = 0.05,
                maf: float = 0.0, maxmiss: float = 0.0, autosomes_only: bool = True,
                drop_monomorphic: bool = False, transversions_only: bool = False, ploidy: str = "auto",
-               strand_mode: str = "drop", precision: str | None = None):
+               strand_mode: str = "drop", precision: str | None = None, tier: str = "host"):
     """Builds an f2_blocks tensor from <prefix>.{geno,snp,ind} on the GPU.
 
     The P axis is the selection sorted ascending by label (pops.txt order). Returns an
     F2Blocks handle, or writes an STPF2BK1 directory to ``out`` and returns its path.
     SNP filters (maxmiss, maf, monomorphic, autosomes, transversions, strand) are
-    applied before the block walk, from the GPU's exact per-population counts.
+    applied before the block walk, by the device keep mask over exact counts. tier="disk"
+    (with ``out``) streams finished runs of blocks straight into f2.bin, so the tensor is
+    never held in host memory (the reference's Disk output tier).
     """
+    if tier not in ("host", "disk"):
+        raise ValueError("extract_f2: tier must be 'host' or 'disk'")
+    if tier == "disk" and out is None:
+        raise ValueError("extract_f2: tier='disk' writes to `out`")
     if not pops:
         raise ValueError("extract_f2: pops needs at least one population name")
     if ploidy not in PLOIDY:
@@ -547,10 +614,7 @@ def extract_f2(prefix, *, pops: list[str], out: str | None = None, device: int =
     bid, nb = assign_blocks(snp.chrom[idx], snp.genpos[idx], blgsize, snp.physpos[idx])
     if nb <= 0:
         raise ValueError("extract_f2: assign_blocks produced 0 blocks (check blgsize and the .snp genetic positions)")
-    t = ctx.extract_blocks(rec, h.n_ind, sel, po, bid, nb, precision=prec, ploidy=ploidy,
-                           kept_rows=None if idx.size == M else idx)
-    if out is None:
-        return F2Blocks(t, labels, device)
+    kept_rows = None if idx.size == M else idx
     meta = {
         "precision_tag": PRECISION_TAGS.get(prec, ""), "blgsize_cm": blgsize * 100.0,
         "n_snp_total": h.n_snp, "n_snp_kept": int(idx.size),
@@ -560,5 +624,14 @@ def extract_f2(prefix, *, pops: list[str], out: str | None = None, device: int =
         "pop_selection": "explicit:" + ",".join(pops),
         "geno": prefix + ".geno", "snp": prefix + ".snp", "ind": prefix + ".ind",
     }
+    if tier == "disk":
+        w = F2DirWriter(out, len(labels), nb, labels, meta)
+        bs = ctx.extract_streamed(rec, h.n_ind, sel, po, bid, nb, w.slabs, precision=prec, ploidy=ploidy,
+                                  kept_rows=kept_rows)
+        w.finish(bs)
+        return str(out)
+    t = ctx.extract_blocks(rec, h.n_ind, sel, po, bid, nb, precision=prec, ploidy=ploidy, kept_rows=kept_rows)
+    if out is None:
+        return F2Blocks(t, labels, device)
     write_f2_dir(out, t, labels, meta)
     return str(out)

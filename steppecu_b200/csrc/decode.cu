@@ -800,6 +800,44 @@ __global__ void detect_ploidy_words_kernel(const uint8_t* __restrict__ records, 
 }
 }  // namespace
 
+namespace {
+// The canonical individual-major tile (record g: individual g's SNP codes, 4 per byte
+// MSB-first) to SNP-major PACKEDANCESTRYMAP records (record s: individual g's code at byte
+// g / 4, MSB-first). Thread (4 SNPs, 4 individuals): four tile bytes in, a 4x4 2-bit
+// transpose, four record bytes out (consecutive threads write consecutive bytes of a record).
+// Individuals past n_ind read as missing (code 3).
+__global__ void canonical_to_records_kernel(const uint8_t* __restrict__ packed, uint64_t bpr, int64_t n_snp,
+                                            int64_t n_ind, uint8_t* __restrict__ records, uint64_t pitch) {
+    const int64_t g4 = static_cast<int64_t>(blockIdx.y) * blockDim.x + threadIdx.x;
+    const int64_t s4 = static_cast<int64_t>(blockIdx.x) * blockDim.y + threadIdx.y;
+    if (4 * g4 >= n_ind || 4 * s4 >= n_snp) return;
+    uint32_t w = 0;  // byte j (row 0 in the top byte): individual 4*g4 + j's codes of SNPs 4*s4 .. +3
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t g = 4 * g4 + j;
+        const uint32_t b = g < n_ind ? packed[g * static_cast<int64_t>(bpr) + s4] : 0xFFu;
+        w |= b << (8 * (3 - j));
+    }
+    w = transpose4x4_2bit(w);  // byte k (top first): SNP 4*s4 + k's codes of the 4 individuals
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int64_t s = 4 * s4 + k;
+        if (s < n_snp) records[s * static_cast<int64_t>(pitch) + g4] = static_cast<uint8_t>(w >> (8 * (3 - k)));
+    }
+}
+}  // namespace
+
+void launch_canonical_to_records(Ctx& c, const uint8_t* packed, uint64_t bpr, int64_t n_snp, int64_t n_ind,
+                                 uint8_t* records, uint64_t pitch, cudaStream_t s) {
+    if (n_snp <= 0 || n_ind <= 0) return;
+    const dim3 block(64, 4);
+    const dim3 grid(static_cast<unsigned>(((n_snp + 3) / 4 + 3) / 4), static_cast<unsigned>(((n_ind + 3) / 4 + 63) / 64));
+    if (grid.y > 65535u) fail(STP_INVALID_ARGUMENT, "canonical tile: too many individuals for one transpose launch");
+    canonical_to_records_kernel<<<grid, block, 0, s>>>(packed, bpr, n_snp, n_ind, records, pitch);
+    STPF2_CUDA(cudaGetLastError());
+    c.launches++;
+}
+
 void launch_detect_ploidy_words(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_snp, int64_t n_ind,
                                 const int32_t* pos, uint32_t* sel, cudaStream_t s) {
     if (n_ind <= 0 || n_snp <= 0) return;

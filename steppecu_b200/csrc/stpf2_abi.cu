@@ -531,12 +531,11 @@ struct DrainOnError {
 // contraction waits for the download of segment k-2 from the same buffer), so the output
 // tensor itself may exceed device memory (the out-of-core tier: only the host holds all
 // P x P x B slabs).
-void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, uint8_t* d_rec, uint64_t dp) {
-    constexpr int64_t kBand = 128;  // rows per downloaded band (one contraction tile)
-    const BlockLayout& L = p.L;
+// Segments of whole blocks, each about a twelfth of the SNPs and the first at least the
+// ploidy window: bounds[k]..bounds[k+1] are segment k's blocks.
+std::vector<int> segment_bounds(const BlockLayout& L) {
     const int B = L.n_block;
     const int64_t M = L.n_snp;
-    const size_t slab = static_cast<size_t>(p.P) * static_cast<size_t>(p.P);
     const int64_t window = std::min<int64_t>(M, 1000);
     const int64_t target = std::max<int64_t>((M + 11) / 12, window);
     std::vector<int> bounds{0};
@@ -549,12 +548,39 @@ void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, u
         }
     }
     bounds.push_back(B);
+    return bounds;
+}
+
+// Where the host side of a segmented pass puts each segment's slabs: straight into the
+// caller's F2BlockTensor (f2, vpair), or into a two-segment pinned staging ring handed to
+// a callback once the segment is complete (the streamed tiers: the caller keeps or writes
+// the slabs, and no whole tensor needs to exist anywhere).
+struct SlabTarget {
+    double* f2 = nullptr;
+    double* vpair = nullptr;
+    stp_slab_sink sink = nullptr;
+    void* user = nullptr;
+};
+
+// The segmented contraction pass with host output. before(k) enqueues what segment k needs
+// on the context stream before its contraction (uploads, decode); the contraction of
+// segment k goes into a two-segment device ring (it waits for the download of segment
+// k - 2 from the same buffer), only the upper 128-row bands of each (exactly symmetric)
+// slab cross PCIe, and the host fills the lower tiles once the download has landed. With a
+// sink, at most two segments are in flight and each is handed over before its staging
+// slot is reused.
+template <class Before>
+void contract_segments(Ctx& c, UmmaPlan* up, int P, const std::vector<int>& bounds, const SlabTarget& t,
+                       Before&& before) {
+    constexpr int64_t kBand = 128;  // rows per downloaded band (one contraction tile)
+    const size_t slab = static_cast<size_t>(P) * static_cast<size_t>(P);
     const size_t nseg = bounds.size() - 1;
     size_t ring = 1;  // slabs per ring buffer: the largest segment
     for (size_t k = 0; k < nseg; ++k) ring = std::max<size_t>(ring, static_cast<size_t>(bounds[k + 1] - bounds[k]));
     c.ws_f2.reserve(2 * ring * slab * sizeof(double));
     c.ws_vpair.reserve(2 * ring * slab * sizeof(double));
-    std::vector<cudaEvent_t> ev(3 * nseg, nullptr);  // per segment: uploaded, contracted, downloaded
+    if (t.sink) c.pin_stage.reserve(4 * ring * slab * sizeof(double));
+    std::vector<cudaEvent_t> ev(2 * nseg, nullptr);  // per segment: contracted, downloaded
     struct Free {
         std::vector<cudaEvent_t>& ev;
         ~Free() {
@@ -563,55 +589,98 @@ void run_pipelined(Ctx& c, const stp_f2_request& r, stp_f2_output& o, Plan& p, u
         }
     } free_events{ev};
     for (auto& e : ev) STPF2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    int64_t snp0 = 0, rec_end = 0;
-    for (size_t k = 0; k < nseg; ++k) {
+    auto host_f2 = [&](size_t k) {
+        return t.sink ? c.pin_stage.as<double>() + (k % 2) * ring * slab : t.f2 + slab * bounds[k];
+    };
+    auto host_vp = [&](size_t k) {
+        return t.sink ? c.pin_stage.as<double>() + (2 + k % 2) * ring * slab : t.vpair + slab * bounds[k];
+    };
+    auto enqueue = [&](size_t k) {
         const int b0 = bounds[k], b1 = bounds[k + 1];
-        int64_t nsnp = 0;
-        for (int b = b0; b < b1; ++b) nsnp += L.blocks[b].k;
-        // The records this segment reads: its SNPs' rows (a run of kept rows spans from the
-        // first to the last), the first segment also the ploidy window; never a row twice.
-        int64_t r0 = snp0, r1 = snp0 + nsnp;
-        if (!p.kept.empty() && nsnp > 0) {
-            r0 = p.kept[static_cast<size_t>(snp0)];
-            r1 = p.kept[static_cast<size_t>(snp0 + nsnp - 1)] + 1;
-        }
-        if (k == 0) {
-            r0 = 0;
-            r1 = std::max<int64_t>(r1, std::min<int64_t>(p.n_rec, 1000));
-        }
-        r0 = std::max(r0, rec_end);
-        r1 = std::max(r1, r0);
-        rec_end = r1;
-        const int64_t t0 = L.blocks[b0].col / kTileK;
-        const int64_t t1 = (b1 < B ? L.blocks[b1].col : L.ld) / kTileK;
         double* f2k = c.ws_f2.as<double>() + (k % 2) * ring * slab;
         double* vpk = c.ws_vpair.as<double>() + (k % 2) * ring * slab;
-        upload_rows(r.geno, d_rec, dp, r0, r1 - r0, c.h2d);
-        STPF2_CUDA(cudaEventRecord(ev[3 * k], c.h2d));
-        STPF2_CUDA(cudaStreamWaitEvent(c.stream, ev[3 * k], 0));
-        launch_decode(p, d_rec, nullptr, nullptr, c.stream, t0, t1, k == 0);
-        if (k >= 2) STPF2_CUDA(cudaStreamWaitEvent(c.stream, ev[3 * (k - 2) + 2], 0));  // ring buffer free
-        launch_f2_umma_blocks(c, p.umma, b0, b1, f2k, vpk, c.stream, true);
-        STPF2_CUDA(cudaEventRecord(ev[3 * k + 1], c.stream));
-        STPF2_CUDA(cudaStreamWaitEvent(c.d2h, ev[3 * k + 1], 0));
-        download_upper_bands(o.f2 + slab * b0, f2k, p.P, kBand, b1 - b0, c.d2h);
-        download_upper_bands(o.vpair + slab * b0, vpk, p.P, kBand, b1 - b0, c.d2h);
-        STPF2_CUDA(cudaEventRecord(ev[3 * k + 2], c.d2h));
-        snp0 += nsnp;
-    }
-    // Every slab is exactly symmetric (the contraction stores one value at (i, j) and
-    // (j, i)), so only its upper row bands crossed PCIe; the host fills the lower tiles of
-    // each segment once its download has landed, while later segments are still in flight.
+        before(k);
+        if (k >= 2) STPF2_CUDA(cudaStreamWaitEvent(c.stream, ev[2 * (k - 2) + 1], 0));  // ring buffer free
+        launch_f2_umma_blocks(c, up, b0, b1, f2k, vpk, c.stream, true);
+        STPF2_CUDA(cudaEventRecord(ev[2 * k], c.stream));
+        STPF2_CUDA(cudaStreamWaitEvent(c.d2h, ev[2 * k], 0));
+        download_upper_bands(host_f2(k), f2k, P, kBand, b1 - b0, c.d2h);
+        download_upper_bands(host_vp(k), vpk, P, kBand, b1 - b0, c.d2h);
+        STPF2_CUDA(cudaEventRecord(ev[2 * k + 1], c.d2h));
+    };
+    const size_t depth = t.sink ? 2 : nseg;
+    size_t queued = 0;
     for (size_t k = 0; k < nseg; ++k) {
-        STPF2_CUDA(cudaEventSynchronize(ev[3 * k + 2]));
-        const int b0 = bounds[k], nb = bounds[k + 1] - bounds[k];
+        while (queued < nseg && queued < k + depth) enqueue(queued++);
+        STPF2_CUDA(cudaEventSynchronize(ev[2 * k + 1]));
+        const int nb = bounds[k + 1] - bounds[k];
+        double* f2h = host_f2(k);
+        double* vph = host_vp(k);
         parallel_for(2 * nb, [&](int u) {
-            double* base = (u % 2 == 0) ? o.f2 : o.vpair;
-            mirror_lower_tiles(base + slab * static_cast<size_t>(b0 + u / 2), p.P, kBand);
+            double* base = (u % 2 == 0) ? f2h : vph;
+            mirror_lower_tiles(base + slab * static_cast<size_t>(u / 2), P, kBand);
         });
+        if (t.sink && t.sink(t.user, bounds[k], bounds[k + 1], f2h, vph) != 0)
+            fail(STP_RUNTIME_ERROR, "the slab sink stopped the extraction");
     }
     STPF2_CUDA(cudaStreamSynchronize(c.d2h));
     STPF2_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+// Genotype records in, host output: the pass runs in segments of whole blocks so the
+// upload of segment k+1 (host records), the decode and contraction of segment k and the
+// download of segment k-1's slabs overlap on three streams. A segment's records are a
+// contiguous run of rows, its operand columns a tile range, its output a run of block
+// slabs. The device holds only two segments' slabs, so the output tensor may exceed device
+// memory (the out-of-core tiers: only the host, or the sink, sees all P x P x B slabs).
+void run_pipelined(Ctx& c, const stp_f2_request& r, const SlabTarget& t, Plan& p, uint8_t* d_rec, uint64_t dp) {
+    const BlockLayout& L = p.L;
+    const int B = L.n_block;
+    const std::vector<int> bounds = segment_bounds(L);
+    const bool upload = !r.geno.on_device;
+    std::vector<int64_t> snp0(bounds.size(), 0);
+    for (size_t k = 0; k + 1 < bounds.size(); ++k) {
+        int64_t nsnp = 0;
+        for (int b = bounds[k]; b < bounds[k + 1]; ++b) nsnp += L.blocks[b].k;
+        snp0[k + 1] = snp0[k] + nsnp;
+    }
+    std::vector<cudaEvent_t> up_ev(bounds.size() - 1, nullptr);
+    struct Free {
+        std::vector<cudaEvent_t>& ev;
+        ~Free() {
+            for (auto e : ev)
+                if (e) cudaEventDestroy(e);
+        }
+    } free_events{up_ev};
+    for (auto& e : up_ev) STPF2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    int64_t rec_end = 0;
+    contract_segments(c, p.umma, p.P, bounds, t, [&](size_t k) {
+        const int b0 = bounds[k], b1 = bounds[k + 1];
+        const int64_t nsnp = snp0[k + 1] - snp0[k];
+        if (upload) {
+            // The records this segment reads: its SNPs' rows (a run of kept rows spans from
+            // the first to the last), the first segment also the ploidy window; never a row
+            // twice.
+            int64_t r0 = snp0[k], r1 = snp0[k] + nsnp;
+            if (!p.kept.empty() && nsnp > 0) {
+                r0 = p.kept[static_cast<size_t>(snp0[k])];
+                r1 = p.kept[static_cast<size_t>(snp0[k] + nsnp - 1)] + 1;
+            }
+            if (k == 0) {
+                r0 = 0;
+                r1 = std::max<int64_t>(r1, std::min<int64_t>(p.n_rec, 1000));
+            }
+            r0 = std::max(r0, rec_end);
+            r1 = std::max(r1, r0);
+            rec_end = r1;
+            upload_rows(r.geno, d_rec, dp, r0, r1 - r0, c.h2d);
+            STPF2_CUDA(cudaEventRecord(up_ev[k], c.h2d));
+            STPF2_CUDA(cudaStreamWaitEvent(c.stream, up_ev[k], 0));
+        }
+        const int64_t t0 = L.blocks[b0].col / kTileK;
+        const int64_t t1 = (b1 < B ? L.blocks[b1].col : L.ld) / kTileK;
+        launch_decode(p, d_rec, nullptr, nullptr, c.stream, t0, t1, k == 0);
+    });
 }
 
 void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
@@ -647,7 +716,10 @@ void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
     const size_t out_elems = static_cast<size_t>(std::max(r.n_pop, 0)) * std::max(r.n_pop, 0) * std::max(r.n_block, 0);
     if (pipelined && p->umma && !p->repitch && out_elems) {
         STPF2_CUDA(cudaStreamSynchronize(s));  // the plan's tables are uploaded on s
-        run_pipelined(c, r, o, *p, c.ws_records.as<uint8_t>(), dp);
+        SlabTarget t;
+        t.f2 = o.f2;
+        t.vpair = o.vpair;
+        run_pipelined(c, r, t, *p, c.ws_records.as<uint8_t>(), dp);
     } else {
         double* d_f2 = o.f2;
         double* d_vp = o.vpair;
@@ -1265,6 +1337,28 @@ stp_status stp_snp_keep_mask(stp_ctx* ctx, const stp_geno_view* geno, const int6
     });
 }
 
+stp_status stp_canonical_to_records(stp_ctx* ctx, const uint8_t* packed, uint64_t bpr, int64_t n_snp, int64_t n_ind,
+                                    int32_t packed_on_device, uint8_t* d_records, uint64_t pitch) {
+    return guarded([&] {
+        need(ctx != nullptr, "null context");
+        use_device(*ctx);
+        if (n_snp <= 0 || n_ind <= 0) return;
+        need(packed && d_records, "null argument");
+        need(bpr * 4 >= static_cast<uint64_t>(n_snp), "bytes_per_record too small for n_snp");
+        need(pitch * 4 >= static_cast<uint64_t>(n_ind), "pitch too small for n_ind");
+        cudaStream_t s = ctx->stream;
+        DevBuf d_pk;
+        const uint8_t* pk = packed;
+        if (!packed_on_device) {
+            d_pk.reserve(static_cast<size_t>(bpr) * n_ind);
+            STPF2_CUDA(cudaMemcpyAsync(d_pk.ptr, packed, static_cast<size_t>(bpr) * n_ind, cudaMemcpyHostToDevice, s));
+            pk = d_pk.as<uint8_t>();
+        }
+        launch_canonical_to_records(*ctx, pk, bpr, n_snp, n_ind, d_records, pitch, s);
+        STPF2_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 stp_status stp_decode_af_compact_filter(stp_ctx* ctx, const uint8_t* packed, uint64_t bpr, int64_t n_snp, int64_t n_ind,
                                         const int64_t* pop_offsets, int32_t n_pop, const int32_t* sample_ploidy,
                                         int32_t ploidy, int32_t packed_on_device, const char* ref, const char* alt,
@@ -1449,70 +1543,176 @@ stp_status stp_detect_ploidy_tile(stp_ctx* ctx, const uint8_t* packed, uint64_t 
     });
 }
 
+namespace {
+
+// compute_f2_blocks over Q / V / N (host, or device when qvn_on_device): the feeder turns
+// them into operand planes, then the contraction writes f2 / vpair into t.f2 / t.vpair
+// (device buffers when out_on_device, host buffers otherwise) or, with t.sink, streams them
+// in segments of blocks to the sink (tensor-core arithmetics only).
+void f2_from_qvn(Ctx& c, const double* Q, const double* V, const double* N, int P, int64_t M, const int32_t* block_id,
+                 int n_block, int precision, bool qvn_on_device, const SlabTarget& t, bool out_on_device,
+                 int32_t* block_sizes) {
+    need(P >= 0 && M >= 0 && n_block >= 0, "negative extent");
+    need(M <= INT_MAX, "M exceeds INT_MAX (M > INT_MAX is not supported)");
+    const size_t out_elems = static_cast<size_t>(P) * P * n_block;
+    if (n_block > 0 && block_sizes) std::fill(block_sizes, block_sizes + n_block, 0);
+    if (P <= 0 || n_block <= 0) return;
+    cudaStream_t s = c.stream;
+    const OpFmt fmt = fmt_of(precision);
+    if (t.sink) need(fmt != OpFmt::F32, "streamed output needs a tensor-core precision");
+    else need(t.f2 && t.vpair, "null output");
+    if (M <= 0) {  // every block is empty: zeros (cpu_backend.cpp:234)
+        if (t.sink) {
+            std::vector<double> z(static_cast<size_t>(P) * P * n_block, 0.0);
+            if (t.sink(t.user, 0, n_block, z.data(), z.data()) != 0) fail(STP_RUNTIME_ERROR, "the slab sink stopped the extraction");
+        } else if (out_on_device) {
+            STPF2_CUDA(cudaMemsetAsync(t.f2, 0, out_elems * 8, s));
+            STPF2_CUDA(cudaMemsetAsync(t.vpair, 0, out_elems * 8, s));
+            STPF2_CUDA(cudaStreamSynchronize(s));
+        } else {
+            std::fill(t.f2, t.f2 + out_elems, 0.0);
+            std::fill(t.vpair, t.vpair + out_elems, 0.0);
+        }
+        return;
+    }
+    need(Q && V && N && block_id, "null input");
+    DrainOnError drain{c};
+    const BlockLayout L = make_block_layout(block_id, M, n_block);
+    if (block_sizes) copy_block_sizes(L, block_sizes);
+    DevBuf d_qvn, d_col, d_planes, d_blocks, d_items, d_f2, d_vp;
+    const size_t pm = static_cast<size_t>(P) * M;
+    const double *dq = Q, *dv = V, *dn = N;
+    if (!qvn_on_device) {
+        d_qvn.reserve(3 * pm * 8);
+        double* h = d_qvn.as<double>();
+        STPF2_CUDA(cudaMemcpyAsync(h, Q, pm * 8, cudaMemcpyHostToDevice, s));
+        STPF2_CUDA(cudaMemcpyAsync(h + pm, V, pm * 8, cudaMemcpyHostToDevice, s));
+        STPF2_CUDA(cudaMemcpyAsync(h + 2 * pm, N, pm * 8, cudaMemcpyHostToDevice, s));
+        dq = h;
+        dv = h + pm;
+        dn = h + 2 * pm;
+    }
+    upload(d_col, L.snp_col, s);
+    upload(d_blocks, L.blocks, s);
+    const size_t ob = operand_plane_bytes(fmt, P, L.ld);
+    d_planes.reserve(ob);
+    STPF2_CUDA(cudaMemsetAsync(d_planes.ptr, 0, ob, s));
+    OperandPlanes op;
+    bind_operand_planes(op, fmt, P, L.ld, d_planes.ptr);
+    launch_feed_qvn(c, dq, dv, dn, P, M, d_col.as<int32_t>(), op, s);
+    if (precision == STP_PREC_FP32_SIMT) {
+        double* f2 = t.f2;
+        double* vp = t.vpair;
+        if (!out_on_device) {
+            d_f2.reserve(out_elems * 8);
+            d_vp.reserve(out_elems * 8);
+            f2 = d_f2.as<double>();
+            vp = d_vp.as<double>();
+        }
+        const std::vector<WorkItem> items = make_work_items(L, P, simt_tile());
+        upload(d_items, items, s);
+        launch_f2_simt(c, d_items.as<WorkItem>(), static_cast<int>(items.size()), d_blocks.as<BlockInfo>(), op, f2, vp, s);
+        if (!out_on_device) {
+            STPF2_CUDA(cudaMemcpyAsync(t.f2, f2, out_elems * 8, cudaMemcpyDeviceToHost, s));
+            STPF2_CUDA(cudaMemcpyAsync(t.vpair, vp, out_elems * 8, cudaMemcpyDeviceToHost, s));
+        }
+        STPF2_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    std::unique_ptr<UmmaPlan, void (*)(UmmaPlan*)> up(umma_plan_create(c, op, L, chunk_stages_of(precision)),
+                                                       umma_plan_destroy);
+    if (out_on_device) {
+        launch_f2_umma(c, up.get(), t.f2, t.vpair, s);
+    } else {
+        // Host output, streamed or not: segments of blocks through the device ring.
+        STPF2_CUDA(cudaStreamSynchronize(s));
+        contract_segments(c, up.get(), P, segment_bounds(L), t, [](size_t) {});
+    }
+    STPF2_CUDA(cudaStreamSynchronize(s));
+    umma_check(up.get());
+}
+
+}  // namespace
+
 stp_status stp_f2_from_qvn(stp_ctx* ctx, const double* Q, const double* V, const double* N, int32_t P, int64_t M,
                            const int32_t* block_id, int32_t n_block, int32_t precision, double* f2,
                            double* vpair, int32_t* block_sizes) {
     return guarded([&] {
         need(ctx != nullptr, "null context");
         use_device(*ctx);
-        need(P >= 0 && M >= 0 && n_block >= 0, "negative extent");
-        const size_t out_elems = static_cast<size_t>(P) * P * n_block;
-        if (n_block > 0 && block_sizes) std::fill(block_sizes, block_sizes + n_block, 0);
-        if (P <= 0 || n_block <= 0) return;
-        need(f2 && vpair, "null output");
-        if (M <= 0) {
-            std::fill(f2, f2 + out_elems, 0.0);
-            std::fill(vpair, vpair + out_elems, 0.0);
+        SlabTarget t;
+        t.f2 = f2;
+        t.vpair = vpair;
+        f2_from_qvn(*ctx, Q, V, N, P, M, block_id, n_block, precision, false, t, false, block_sizes);
+    });
+}
+
+stp_status stp_f2_from_qvn_device(stp_ctx* ctx, const double* Q, const double* V, const double* N, int32_t P, int64_t M,
+                                  const int32_t* block_id, int32_t n_block, int32_t precision, int32_t qvn_on_device,
+                                  double* d_f2, double* d_vpair, int32_t* block_sizes) {
+    return guarded([&] {
+        need(ctx != nullptr, "null context");
+        use_device(*ctx);
+        SlabTarget t;
+        t.f2 = d_f2;
+        t.vpair = d_vpair;
+        f2_from_qvn(*ctx, Q, V, N, P, M, block_id, n_block, precision, qvn_on_device != 0, t, true, block_sizes);
+    });
+}
+
+stp_status stp_f2_from_qvn_streamed(stp_ctx* ctx, const double* Q, const double* V, const double* N, int32_t P,
+                                    int64_t M, const int32_t* block_id, int32_t n_block, int32_t precision,
+                                    stp_slab_sink sink, void* user, int32_t* block_sizes) {
+    return guarded([&] {
+        need(ctx != nullptr && sink != nullptr, "null argument");
+        use_device(*ctx);
+        SlabTarget t;
+        t.sink = sink;
+        t.user = user;
+        f2_from_qvn(*ctx, Q, V, N, P, M, block_id, n_block, precision, false, t, false, block_sizes);
+    });
+}
+
+stp_status stp_f2_extract_streamed(stp_ctx* ctx, const stp_f2_request* req, stp_slab_sink sink, void* user,
+                                   int32_t* block_sizes) {
+    return guarded([&] {
+        need(ctx && req && sink, "null argument");
+        use_device(*ctx);
+        Ctx& c = *ctx;
+        const stp_f2_request& r = *req;
+        if (r.n_block > 0 && block_sizes) std::fill(block_sizes, block_sizes + r.n_block, 0);
+        if (r.n_pop <= 0 || r.n_block <= 0) return;
+        need(r.precision != STP_PREC_FP32_SIMT, "streamed output needs a tensor-core precision");
+        if (r.geno.n_snp > INT_MAX) fail(STP_RUNTIME_ERROR, "n_snp exceeds INT_MAX (M > INT_MAX is not supported)");
+        DrainOnError drain{c};
+        uint64_t pitch = r.geno.pitch ? r.geno.pitch : r.geno.bytes_per_record;
+        need(pitch >= r.geno.bytes_per_record, "pitch < bytes_per_record");
+        need(r.geno.records != nullptr || r.geno.n_snp == 0, "records is NULL");
+        uint8_t* d_rec = const_cast<uint8_t*>(r.geno.records);
+        uint64_t dp = pitch;
+        if (!r.geno.on_device && r.geno.n_snp > 0) {
+            dp = device_pitch(r.geno);
+            c.ws_records.reserve(static_cast<size_t>(dp) * r.geno.n_snp);
+            d_rec = c.ws_records.as<uint8_t>();
+        }
+        {
+            const BlockLayout probe = make_block_layout(r.block_id, snp_axis(r), r.n_block);
+            c.ws_misc.reserve(operand_plane_bytes(fmt_of(r.precision), std::max(r.n_pop, 1), probe.ld));
+        }
+        std::unique_ptr<Plan> p = build_plan(c, r, dp, c.ws_misc.ptr, true);
+        need(!p->repitch, "streamed extraction of device records needs a 4-byte aligned pitch");
+        if (block_sizes) copy_block_sizes(p->L, block_sizes);
+        STPF2_CUDA(cudaStreamSynchronize(c.stream));
+        SlabTarget t;
+        t.sink = sink;
+        t.user = user;
+        if (p->n_snp <= 0) {  // no SNPs: every block is empty -> zeros (cpu_backend.cpp:234)
+            std::vector<double> z(static_cast<size_t>(r.n_pop) * r.n_pop * r.n_block, 0.0);
+            if (sink(user, 0, r.n_block, z.data(), z.data()) != 0) fail(STP_RUNTIME_ERROR, "the slab sink stopped the extraction");
             return;
         }
-        need(Q && V && N && block_id, "null input");
-        cudaStream_t s = ctx->stream;
-        const BlockLayout L = make_block_layout(block_id, M, n_block);
-        if (block_sizes) copy_block_sizes(L, block_sizes);
-        const OpFmt fmt = fmt_of(precision);
-        DevBuf d_qvn, d_col, d_planes, d_blocks, d_items, d_f2, d_vp;
-        const size_t pm = static_cast<size_t>(P) * M;
-        d_qvn.reserve(3 * pm * 8);
-        double* dq = d_qvn.as<double>();
-        STPF2_CUDA(cudaMemcpyAsync(dq, Q, pm * 8, cudaMemcpyHostToDevice, s));
-        STPF2_CUDA(cudaMemcpyAsync(dq + pm, V, pm * 8, cudaMemcpyHostToDevice, s));
-        STPF2_CUDA(cudaMemcpyAsync(dq + 2 * pm, N, pm * 8, cudaMemcpyHostToDevice, s));
-        upload(d_col, L.snp_col, s);
-        upload(d_blocks, L.blocks, s);
-        const size_t ob = operand_plane_bytes(fmt, P, L.ld);
-        d_planes.reserve(ob);
-        STPF2_CUDA(cudaMemsetAsync(d_planes.ptr, 0, ob, s));
-        OperandPlanes op;
-        bind_operand_planes(op, fmt, P, L.ld, d_planes.ptr);
-        launch_feed_qvn(*ctx, dq, dq + pm, dq + 2 * pm, P, M, d_col.as<int32_t>(), op, s);
-        d_f2.reserve(out_elems * 8);
-        d_vp.reserve(out_elems * 8);
-        if (precision == STP_PREC_FP32_SIMT) {
-            const std::vector<WorkItem> items = make_work_items(L, P, simt_tile());
-            upload(d_items, items, s);
-            launch_f2_simt(*ctx, d_items.as<WorkItem>(), static_cast<int>(items.size()), d_blocks.as<BlockInfo>(), op,
-                           d_f2.as<double>(), d_vp.as<double>(), s);
-        } else {
-            UmmaPlan* up = umma_plan_create(*ctx, op, L, chunk_stages_of(precision));
-            try {
-                launch_f2_umma(*ctx, up, d_f2.as<double>(), d_vp.as<double>(), s);
-            } catch (...) {
-                cudaStreamSynchronize(s);
-                umma_plan_destroy(up);
-                throw;
-            }
-            STPF2_CUDA(cudaStreamSynchronize(s));
-            try {
-                umma_check(up);
-            } catch (...) {
-                umma_plan_destroy(up);
-                throw;
-            }
-            umma_plan_destroy(up);
-        }
-        STPF2_CUDA(cudaMemcpyAsync(f2, d_f2.ptr, out_elems * 8, cudaMemcpyDeviceToHost, s));
-        STPF2_CUDA(cudaMemcpyAsync(vpair, d_vp.ptr, out_elems * 8, cudaMemcpyDeviceToHost, s));
-        STPF2_CUDA(cudaStreamSynchronize(s));
+        run_pipelined(c, r, t, *p, d_rec, dp);
+        umma_check(p->umma);
     });
 }
 

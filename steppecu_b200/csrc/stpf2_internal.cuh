@@ -120,6 +120,7 @@ struct Ctx {
     DevBuf ws_fstat;  // stp_fstats scratch
     DevBuf ws_vpc;    // grouped fixed-point batches: compact vpair tiles
     PinnedBuf pin_union, pin_tables, pin_items;
+    PinnedBuf pin_stage;  // streamed extraction: the two-segment staging ring of f2 / vpair slabs
     // Completion time of each request of the last stp_f2_extract_batch call, in ms from the
     // start of its group's device work (NaN for requests that ran on their own).
     std::vector<double> last_batch_ms;
@@ -311,6 +312,9 @@ void launch_detect_ploidy_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int
 void launch_transpose_pa(Ctx& c, const uint8_t* records, uint64_t pitch, int64_t n_ind, const TileInfo* tiles,
                          int64_t n_tiles, const int32_t* pos, int64_t n_sel, uint64_t* canon, double* center,
                          cudaStream_t s, const int32_t* row_map = nullptr);
+// Canonical individual-major tile -> SNP-major records (pitch >= ceil(n_ind / 4)).
+void launch_canonical_to_records(Ctx& c, const uint8_t* packed, uint64_t bpr, int64_t n_snp, int64_t n_ind,
+                                 uint8_t* records, uint64_t pitch, cudaStream_t s);
 // extract-f2's per-SNP keep mask (filters.cu): from packed pop-major counts (ac2 | n << 16,
 // population i, SNP s at cnt[i * ld + s]) or from FP64 q / n [P x M] (i + P * s). out4
 // (optional, device [4 * M]): pooled ref AF, pooled minor AF, missing fraction, pooled

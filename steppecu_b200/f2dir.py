@@ -103,6 +103,51 @@ def write_f2_dir(directory, t: F2Tensor, pop_labels: list[str], meta: dict | Non
     bin_path = d / "f2.bin"
     with open(bin_path, "wb") as f:
         f.write(f2_bin_bytes(t))
+    return _finish_dir(d, t.P, t.n_block, pop_labels, meta)
+
+
+class F2DirWriter:
+    """Writes an STPF2BK1 directory slab by slab (the disk tier of a streamed extraction):
+    slabs() takes runs of finished blocks in any order and writes them at their offsets in
+    f2.bin, so the P x P x n_block tensor is never held in memory; finish() writes the
+    block sizes, pops.txt and meta.json (with the sha256 cache id of the finished f2.bin)."""
+
+    def __init__(self, directory, P: int, n_block: int, pop_labels: list[str], meta: dict | None = None):
+        if P <= 0 or n_block <= 0:
+            raise F2DirError(f"F2DirWriter: degenerate f2 tensor (P={P} n_block={n_block})")
+        if len(pop_labels) != P:
+            raise F2DirError(f"F2DirWriter: pop_labels has {len(pop_labels)} entries but P={P}")
+        self.d = Path(directory)
+        self.d.mkdir(parents=True, exist_ok=True)
+        self.P, self.n_block, self.labels, self.meta = P, n_block, list(pop_labels), dict(meta or {})
+        self.slab = P * P
+        self.f = open(self.d / "f2.bin", "wb")
+        self.f.write(header_bytes(P, n_block))
+        self.f.truncate(64 + 2 * 8 * self.slab * n_block + 4 * n_block)
+        self.written = np.zeros(n_block, bool)
+
+    def slabs(self, b0: int, b1: int, f2: np.ndarray, vpair: np.ndarray) -> None:
+        n = (b1 - b0) * self.slab
+        for base, a in ((64, f2), (64 + 8 * self.slab * self.n_block, vpair)):
+            self.f.seek(base + 8 * self.slab * b0)
+            self.f.write(np.ascontiguousarray(a[:n], dtype="<f8").tobytes())
+        self.written[b0:b1] = True
+
+    def finish(self, block_sizes: np.ndarray) -> str:
+        if not self.written.all():
+            raise F2DirError("F2DirWriter: not every block was written")
+        bs = np.ascontiguousarray(block_sizes, dtype="<i4")
+        if bs.size != self.n_block:
+            raise F2DirError("F2DirWriter: block_sizes length mismatch")
+        self.f.seek(64 + 2 * 8 * self.slab * self.n_block)
+        self.f.write(bs.tobytes())
+        self.f.close()
+        return _finish_dir(self.d, self.P, self.n_block, self.labels, self.meta)
+
+
+def _finish_dir(d: Path, P: int, n_block: int, pop_labels: list[str], meta: dict) -> str:
+    """pops.txt and meta.json beside a complete f2.bin; returns the f2_cache_id."""
+    bin_path = d / "f2.bin"
     cache_id = "sha256:" + _sha256_file(bin_path)
     with open(d / "pops.txt", "w") as f:
         for s in pop_labels:
@@ -118,8 +163,8 @@ def write_f2_dir(directory, t: F2Tensor, pop_labels: list[str], meta: dict | Non
         '  "format": "STPF2BK1",',
         '  "meta_schema_version": 1,',
         f'  "steppe_version": {_jstr(meta.get("steppe_version", "stpf2-b200"))},',
-        f'  "P": {t.P},',
-        f'  "n_block": {t.n_block},',
+        f'  "P": {P},',
+        f'  "n_block": {n_block},',
         f'  "precision_tag": {_jstr(meta.get("precision_tag", ""))},',
         f'  "precision_mantissa_bits": {int(meta.get("precision_mantissa_bits", 0))},',
         f'  "blgsize_cm": {meta.get("blgsize_cm", 5)},',
