@@ -278,8 +278,13 @@ def keep_mask(Q, N, P, ref_alleles, alt_alleles, chrom, maf_min=0.0, maxmiss=1.0
     Qa = np.ascontiguousarray(Q, np.float64)
     Na = np.ascontiguousarray(N, np.float64)
     M = Qa.size // P if P > 0 else 0
-    r = np.ascontiguousarray(np.asarray(ref_alleles, dtype="S1").view(np.uint8))
-    a = np.ascontiguousarray(np.asarray(alt_alleles, dtype="S1").view(np.uint8))
+    def codes(x):  # allele characters as uint8 codes (from codes or from characters)
+        x = np.asarray(x)
+        if x.dtype in (np.uint8, np.int8):
+            return np.ascontiguousarray(x.view(np.uint8))
+        return np.ascontiguousarray(np.asarray(x, dtype="S1").view(np.uint8))
+
+    r, a = codes(ref_alleles), codes(alt_alleles)
     c = np.ascontiguousarray(chrom, np.int32)
     keep = np.zeros(max(M, 1), np.uint8)
     summ = np.zeros(4 * max(M, 1))

@@ -123,6 +123,17 @@ __device__ __forceinline__ bool waitb(unsigned long long* b, uint32_t parity, Fx
 
 __device__ __forceinline__ int stages_of(int k, int per) { return (k + per - 1) / per; }
 
+// The MMA width of a tile pair: the column tile's populations rounded up to the N step of
+// 16 (at most 128). Columns past the last population are never stored, so a short last
+// column tile costs only its own columns of tensor work.
+template <bool kGrouped>
+__device__ __forceinline__ uint32_t idesc_for(const FxArgs& a, const WorkItem& w, const BlockInfo& bi) {
+    const int P = kGrouped ? a.groups[bi.grp].P : a.P;
+    const int cols = min(kTile, P - w.tj * kTile);
+    const uint32_t n = static_cast<uint32_t>((cols + 15) & ~15);
+    return (a.idesc & ~(0x3Fu << 17)) | ((n >> 3) << 17);
+}
+
 // Work items in list order from a global counter (costliest block first, a block's tile
 // pairs together), handed from the producer to the other roles through a small ring.
 __device__ __forceinline__ int take_item(const FxArgs& a, FxCtl* ctl, uint32_t gi, bool& ok) {
@@ -193,15 +204,17 @@ abort:
         waitb(&ctl->full[k % kStages], (k / kStages) & 1u, ctl, a, false);
 }
 
+template <bool kGrouped>
 __device__ void fx_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t tmem) {
     uint32_t g = 0, cs = 0;
     const uint32_t V3 = tmem, V4 = tmem + 128u, V5 = tmem + 256u, V6 = tmem + 384u;
-    const uint32_t id = a.idesc;
     for (uint32_t gi = 0;; ++gi) {
         const int it = read_item(a, ctl, gi);
         if (it < 0) break;
         const WorkItem w = a.items[it];
-        const int nst = stages_of(a.blocks[w.blk].k, kStageK);
+        const BlockInfo bi = a.blocks[w.blk];
+        const int nst = stages_of(bi.k, kStageK);
+        const uint32_t id = idesc_for<kGrouped>(a, w, bi);
         const bool diag = w.ti == w.tj;
         for (int st = 0; st < nst; ++st, ++g) {
             const int sseg = st % kSegStages;
@@ -432,7 +445,7 @@ f2_fx_kernel(const __grid_constant__ FxArgs a) {
     const uint32_t tmem = ctl->tmem_base;
     if (warp < kEpiWarp0) {
         if (warp == 0 && lane == 0) fx_producer<kGrouped>(a, smem, ctl);
-        if (warp == 1 && lane == 0) fx_issuer(a, smem, ctl, tmem);
+        if (warp == 1 && lane == 0) fx_issuer<kGrouped>(a, smem, ctl, tmem);
     } else {
         fx_epilogue<kGrouped>(a, ctl, tmem, warp, lane,
                               reinterpret_cast<double*>(smem + kStages * kStageBytes + kCtlBytes) +
@@ -487,14 +500,17 @@ abort:
         waitb(&ctl->full[k % kVpStages], (k / kVpStages) & 1u, ctl, a, false);
 }
 
+template <bool kGrouped>
 __device__ void vp_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t tmem) {
     uint32_t g = 0, n_acc = 0;
     for (uint32_t gi = 0;; ++gi) {
         const int it = read_item(a, ctl, gi);
         if (it < 0) break;
         const WorkItem w = a.items[it];
-        const int nch = stages_of(a.blocks[w.blk].k, kStageK);
+        const BlockInfo bi = a.blocks[w.blk];
+        const int nch = stages_of(bi.k, kStageK);
         if (nch == 0) continue;
+        const uint32_t id = idesc_for<kGrouped>(a, w, bi);
         const bool diag = w.ti == w.tj;
         const int b = static_cast<int>(n_acc % kVpAcc);
         if (!waitb(&ctl->acc_empty[b], ((n_acc / kVpAcc) & 1u) ^ 1u, ctl, a)) goto done;
@@ -510,7 +526,7 @@ __device__ void vp_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t t
                 const int n = min(kVpChunks, nch - c0);
                 for (int j = 0; j < n; ++j)
                     mma_i8(d, smem_desc(sa + static_cast<uint32_t>(j) * 4096u, 256, 6),
-                           smem_desc(sb + static_cast<uint32_t>(j) * 4096u, 256, 6), a.idesc, (c0 + j) > 0 ? 1u : 0u);
+                           smem_desc(sb + static_cast<uint32_t>(j) * 4096u, 256, 6), id, (c0 + j) > 0 ? 1u : 0u);
                 mma_commit(&ctl->empty[slot]);
             }
         }
@@ -584,7 +600,7 @@ __global__ void __launch_bounds__(kVpThreads, 1) vpair_fx_kernel(const __grid_co
     const uint32_t tmem = ctl->tmem_base;
     if (warp < 2) {
         if (warp == 0 && lane == 0) vp_producer<kGrouped>(a, smem, ctl);
-        if (warp == 1 && lane == 0) vp_issuer(a, smem, ctl, tmem);
+        if (warp == 1 && lane == 0) vp_issuer<kGrouped>(a, smem, ctl, tmem);
     } else {
         vp_epilogue(a, ctl, tmem, warp, lane);
     }
