@@ -275,13 +275,23 @@ def cpu_sample(workload: str, threads: int, seed_rank: int = 0, gen_device: str 
     kind = "reference" if oracle.ref_available() else "port"
     lib = "ref" if kind == "reference" else "port"
     t0 = time.perf_counter()
-    pl = oracle.detect_ploidy_pa(rec, sel)
-    ac2, n = oracle.decode_counts_pa(rec, sel, po, pl)
-    q, v, nd = oracle.counts_to_qvn(ac2, n)
+    if lib == "ref":
+        # The reference end to end: its CpuBackend detects ploidy and decodes q / v / n from
+        # the canonical individual-major tile (cpu_backend.cpp:73-95, 267-319), then reduces
+        # the blocks (:217-264). Laying the records out as that tile is the reference's
+        # reader's job (GenoReader); here the C restatement does it, inside the timing.
+        tile, bpr_c = oracle.transpose_pa_to_canonical(rec, sel)
+        q, v, nd = oracle.decode_af_canonical(tile, bpr_c, n_snp, po, detect=True, lib="ref")
+    else:
+        pl = oracle.detect_ploidy_pa(rec, sel)
+        ac2, n = oracle.decode_counts_pa(rec, sel, po, pl)
+        q, v, nd = oracle.counts_to_qvn(ac2, n)
     f2, vp, _ = oracle.compute_f2_blocks_sharded(q, v, nd, p.n_pop, bid, threads, threads=threads, lib=lib)
     dt = time.perf_counter() - t0
+    legs = ("ploidy detection, decode and f2 by the reference CpuBackend (records laid out as its canonical "
+            "tile by the C restatement)" if lib == "ref" else "decode and f2 by the C restatement")
     desc = (f"{threads} blocks x {per_block} SNPs of the {workload} panel model (P={p.n_pop}, "
-            f"N={p.n_ind}), decode + f2 on {threads} threads, one block per thread")
+            f"N={p.n_ind}); {legs}; f2 on {threads} threads, one block per thread")
     if keep:
         return units(p.n_pop, n_snp), dt, kind, desc, (p, bid, threads, f2, vp)
     return units(p.n_pop, n_snp), dt, kind, desc
@@ -554,6 +564,9 @@ def main():
                     help="skip the many-requests (grouped batch) measurement")
     ap.add_argument("--no-other-configs", dest="other_configs", action="store_false",
                     help="skip the 100-population and uneven-block config measurements")
+    ap.add_argument("--block-snps", type=int, default=None,
+                    help="uniform jackknife blocks of this many SNPs instead of the 5 cM walk (profiling cases: "
+                         "--snps 115000 --block-snps 1611 keeps the headline block size at a tenth of the SNPs)")
     ap.add_argument("--precision-step", type=int, default=10,
                     help="per-block f2 error of the headline pass against the CPU oracle on the pairs of every "
                          "n-th population, all blocks (1: all pairs, several minutes of host time at 1,000 "
@@ -603,6 +616,11 @@ def main():
             dist.destroy_process_group()
         return
     panel = make_panel(args.workload, rank, dev, n_snp=args.snps)
+    if args.block_snps:
+        import numpy as np
+
+        panel.block_id = (np.arange(panel.n_snp) // args.block_snps).astype(np.int32)
+        panel.n_block = int(panel.block_id[-1]) + 1 if panel.n_snp else 0
     sel, po = panel.selection()
     P, M, B = panel.n_pop, panel.n_snp, panel.n_block
     ctx = sb.Context(local)
@@ -767,7 +785,7 @@ def main():
             "vs_baseline": None, "dtype": DTYPES.get(args.precision, "f32"),
             "data": "synthetic",
             "config": {"workload": args.workload, "populations": P, "samples": panel.n_ind, "snps": M,
-                       "blocks": B, "precision": args.precision, "l2": "inputs larger than L2 (no flush)",
+                       "blocks": B, "block_snps": args.block_snps or "5 cM walk", "precision": args.precision, "l2": "inputs larger than L2 (no flush)",
                        "cuda_graph": True,
                        "parallelism": f"block-sharded x{world}" if world > 1 else "1 GPU"},
             "gpu_launches": int(launches), "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,

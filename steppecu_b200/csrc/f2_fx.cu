@@ -231,26 +231,28 @@ __device__ void fx_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t t
                 auto dA = [&](int t) { return smem_desc(sa + static_cast<uint32_t>(t) * 4096u, 256, 6); };
                 auto dB = [&](int t) { return smem_desc(sb + static_cast<uint32_t>(t) * 4096u, 256, 6); };
                 const uint32_t f = sseg == 0 ? 0u : 1u;  // the first stage of a segment overwrites
-                // X digit products of weight >= 256^3, grouped by A operand.
-                mma_i8(V3, dA(3), dB(0), id, f);
-                mma_i8(V4, dA(3), dB(1), id, f);
-                mma_i8(V5, dA(3), dB(2), id, f);
-                mma_i8(V6, dA(3), dB(3), id, f);
-                mma_i8(V3, dA(2), dB(1), id, 1u);
-                mma_i8(V4, dA(2), dB(2), id, 1u);
-                mma_i8(V5, dA(2), dB(3), id, 1u);
-                mma_i8(V3, dA(1), dB(2), id, 1u);
-                mma_i8(V4, dA(1), dB(3), id, 1u);
-                mma_i8(V3, dA(0), dB(3), id, 1u);
+                using C = CollectorA;
+                // X digit products of weight >= 256^3, grouped by A operand: a group reads its
+                // A tile from shared memory once and keeps it in the collector buffer.
+                mma_i8_c<C::kFill>(V3, dA(3), dB(0), id, f);
+                mma_i8_c<C::kUse>(V4, dA(3), dB(1), id, f);
+                mma_i8_c<C::kUse>(V5, dA(3), dB(2), id, f);
+                mma_i8_c<C::kLastUse>(V6, dA(3), dB(3), id, f);
+                mma_i8_c<C::kFill>(V3, dA(2), dB(1), id, 1u);
+                mma_i8_c<C::kUse>(V4, dA(2), dB(2), id, 1u);
+                mma_i8_c<C::kLastUse>(V5, dA(2), dB(3), id, 1u);
+                mma_i8_c<C::kFill>(V3, dA(1), dB(2), id, 1u);
+                mma_i8_c<C::kLastUse>(V4, dA(1), dB(3), id, 1u);
+                mma_i8_c<C::kDiscard>(V3, dA(0), dB(3), id, 1u);
                 // M(i) E_w(j) and E_w(i) M(j): tiles 4..7 are E_3..E_6, tile 8 is M.
-                mma_i8(V3, dA(8), dB(4), id, 1u);
-                mma_i8(V4, dA(8), dB(5), id, 1u);
-                mma_i8(V5, dA(8), dB(6), id, 1u);
-                mma_i8(V6, dA(8), dB(7), id, 1u);
-                mma_i8(V3, dA(4), dB(8), id, 1u);
-                mma_i8(V4, dA(5), dB(8), id, 1u);
-                mma_i8(V5, dA(6), dB(8), id, 1u);
-                mma_i8(V6, dA(7), dB(8), id, 1u);
+                mma_i8_c<C::kFill>(V3, dA(8), dB(4), id, 1u);
+                mma_i8_c<C::kUse>(V4, dA(8), dB(5), id, 1u);
+                mma_i8_c<C::kUse>(V5, dA(8), dB(6), id, 1u);
+                mma_i8_c<C::kLastUse>(V6, dA(8), dB(7), id, 1u);
+                mma_i8_c<C::kDiscard>(V3, dA(4), dB(8), id, 1u);
+                mma_i8_c<C::kDiscard>(V4, dA(5), dB(8), id, 1u);
+                mma_i8_c<C::kDiscard>(V5, dA(6), dB(8), id, 1u);
+                mma_i8_c<C::kDiscard>(V6, dA(7), dB(8), id, 1u);
             }
             mma_commit(&ctl->empty[slot]);
             if (sseg == kSegStages - 1 || st == nst - 1) {

@@ -96,6 +96,36 @@ __device__ __forceinline__ void mma_i8(uint32_t d, uint64_t a, uint64_t b, uint3
         : "memory");
 }
 
+// kind::i8 with the A operand kept in the MMA's collector buffer: kFill reads A from shared
+// memory and keeps it, kUse / kLastUse take it from the buffer (the descriptor must name the
+// same A; kLastUse releases it), kDiscard is the plain form.
+enum class CollectorA { kDiscard, kFill, kUse, kLastUse };
+
+template <CollectorA kC>
+__device__ __forceinline__ void mma_i8_c(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    if constexpr (kC == CollectorA::kFill) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8.collector::a::fill [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+            "l"(a), "l"(b), "r"(idesc), "r"(acc)
+            : "memory");
+    } else if constexpr (kC == CollectorA::kUse) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8.collector::a::use [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+            "l"(a), "l"(b), "r"(idesc), "r"(acc)
+            : "memory");
+    } else if constexpr (kC == CollectorA::kLastUse) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8.collector::a::lastuse [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+            "l"(a), "l"(b), "r"(idesc), "r"(acc)
+            : "memory");
+    } else {
+        mma_i8(d, a, b, idesc, acc);
+    }
+}
+
 __device__ __forceinline__ void mma_commit(unsigned long long* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");

@@ -42,7 +42,11 @@ def test_streamed_extraction_equals_one_shot(ctx, panel, mode, on_device):
     p, sel, po, rec = panel
     want = ctx.extract_blocks(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision=mode)
     f2, vp, runs, sink = _collect(p.n_pop, p.n_block)
-    src = torch.as_tensor(rec).cuda() if on_device else rec
+    src = rec
+    if on_device:  # device records at a 16-byte pitch (the streamed path reads them in place)
+        pitch = (rec.shape[1] + 15) // 16 * 16
+        src = torch.zeros((rec.shape[0], pitch), dtype=torch.uint8, device="cuda")
+        src[:, :rec.shape[1]] = torch.as_tensor(rec).cuda()
     bs = ctx.extract_streamed(src, p.n_ind, sel, po, p.block_id, p.n_block, sink, precision=mode)
     assert len(runs) > 2 and runs[0][0] == 0 and runs[-1][1] == p.n_block
     assert all(a[1] == b[0] for a, b in zip(runs, runs[1:]))  # in block order, contiguous
