@@ -57,7 +57,7 @@ constexpr int kItemRing = 4;
 constexpr int kVpTileInts = kTile * kTile;  // one compact vpair tile: (row r, column c) at c * 128 + r
 
 // ---- f2 kernel constants ----
-constexpr int kStages = 2;
+constexpr int kStages = 3;
 constexpr uint32_t kSide = static_cast<uint32_t>(kFxImageBytes);  // 36 KiB
 constexpr uint32_t kStageBytes = 2 * kSide;
 constexpr int kEpiWarps = 16;
@@ -66,8 +66,6 @@ constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);  // 576
 constexpr int kCols = 4 * kTile / kEpiWarps;            // 32 tile columns per epilogue thread
 constexpr int kSegStages = 512;  // 16,384 SNPs: |V_3| < 81,920 per SNP stays below 2^31
 constexpr uint32_t kTmemCols = 512;
-constexpr int kStagePitch = 9;
-constexpr int kStageDoubles = 32 * kStagePitch;
 constexpr uint32_t kCtlBytes = 256;
 
 // ---- vpair kernel constants ----
@@ -309,8 +307,43 @@ __device__ __forceinline__ void stamp(const FxArgs& a, int grp, int lane) {
     }
 }
 
+__device__ __forceinline__ void st_cs_v2(double* p, double x, double y) {
+    asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(x), "d"(y) : "memory");
+}
+
+__device__ __forceinline__ void st_cs_v4(double* p, double x, double y, double z, double w) {
+    asm volatile("st.global.cs.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(x), "d"(y), "d"(z), "d"(w) : "memory");
+}
+
+// Eight consecutive doubles v[0..7] to p, where p's element offset is kP modulo 4 (the run
+// starts kP elements past a 32-byte boundary): scalar and 16-byte stores up to the boundary,
+// then 32-byte stores, then the tail. Each 32-byte store fills one sector.
+template <int kP>
+__device__ __forceinline__ void store_run8(double* p, const double (&v)[8]) {
+    constexpr int head = (4 - kP) & 3;  // elements before the first 32-byte boundary
+    int k = 0;
+    if constexpr (head & 1) { __stcs(p, v[0]); k = 1; }
+    if constexpr (head & 2) { st_cs_v2(p + k, v[k], v[k + 1]); k += 2; }
+    st_cs_v4(p + k, v[k], v[k + 1], v[k + 2], v[k + 3]);
+    if constexpr (head == 0) st_cs_v4(p + 4, v[4], v[5], v[6], v[7]);
+    else {
+        k += 4;
+        if constexpr (((8 - head - 4) & 2) != 0) { st_cs_v2(p + k, v[k], v[k + 1]); k += 2; }
+        if constexpr (((8 - head - 4) & 1) != 0) __stcs(p + k, v[k]);
+    }
+}
+
+__device__ __forceinline__ void store_run8(double* p, const double (&v)[8]) {
+    switch (static_cast<int>((reinterpret_cast<uintptr_t>(p) >> 3) & 3u)) {
+        case 0: store_run8<0>(p, v); break;
+        case 1: store_run8<1>(p, v); break;
+        case 2: store_run8<2>(p, v); break;
+        default: store_run8<3>(p, v); break;
+    }
+}
+
 template <bool kGrouped>
-__device__ void fx_epilogue(const FxArgs& a, FxCtl* ctl, uint32_t tmem, int warp, int lane, double* stage) {
+__device__ void fx_epilogue(const FxArgs& a, FxCtl* ctl, uint32_t tmem, int warp, int lane) {
     const int e = warp - kEpiWarp0;
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int h = e >> 2;    // column part of the tile
@@ -353,17 +386,21 @@ __device__ void fx_epilogue(const FxArgs& a, FxCtl* ctl, uint32_t tmem, int warp
             if (!ok) return;
             tc_fence_after();
 #pragma unroll
-            for (int w = 0; w < 4; ++w) {
-                const double ws = w == 0 ? 1.0 : (w == 1 ? 256.0 : (w == 2 ? 65536.0 : 16777216.0));
+            for (int g8 = 0; g8 < kCols / 8; ++g8) {
+                // Columns g8*8.. of V_3..V_6, one wait for the four loads.
+                uint32_t v[4][8];
 #pragma unroll
-                for (int g8 = 0; g8 < kCols / 8; ++g8) {
-                    uint32_t v[8];
+                for (int w = 0; w < 4; ++w)
                     tmem_ld8(tmem + lane_addr + static_cast<uint32_t>(w) * 128u + col_addr + static_cast<uint32_t>(g8) * 8u,
-                             v);
-                    tmem_wait_ld();
+                             v[w]);
+                tmem_wait_ld();
 #pragma unroll
-                    for (int c = 0; c < 8; ++c)
-                        acc[g8 * 8 + c] = fma(static_cast<double>(static_cast<int32_t>(v[c])), ws, acc[g8 * 8 + c]);
+                for (int c = 0; c < 8; ++c) {
+                    double x = acc[g8 * 8 + c];
+                    x = fma(static_cast<double>(static_cast<int32_t>(v[0][c])), 1.0, x);
+                    x = fma(static_cast<double>(static_cast<int32_t>(v[1][c])), 256.0, x);
+                    x = fma(static_cast<double>(static_cast<int32_t>(v[2][c])), 65536.0, x);
+                    acc[g8 * 8 + c] = fma(static_cast<double>(static_cast<int32_t>(v[3][c])), 16777216.0, x);
                 }
             }
             tc_fence_before();
@@ -372,44 +409,46 @@ __device__ void fx_epilogue(const FxArgs& a, FxCtl* ctl, uint32_t tmem, int warp
             ++cs;
         }
         // Output: (i, j) straight from registers (32 consecutive i per store: full sectors);
-        // (j, i) through this warp's staging tile (4 rows x 8 consecutive j per store).
+        // (j, i) from the same registers, as this row's run of 8 consecutive j per column
+        // group (32-byte stores where the run allows; per element at the tile's diagonal
+        // and right edge).
         const ItemOut o = item_out<kGrouped>(a, it, r, h, kCols);
-        const int P = o.P, i = o.i, i0 = o.i0, j0 = o.j0;
+        const int P = o.P, i = o.i, j0 = o.j0;
         const bool diag = o.diag;
         const int64_t row_i = o.slab + i;
-        const int64_t row_j0 = o.slab + static_cast<int64_t>(P) * i0;
+        const int64_t col_i = o.slab + static_cast<int64_t>(P) * i;
 #pragma unroll
         for (int q8 = 0; q8 < kCols / 8; ++q8) {
             int32_t vpi[8];
 #pragma unroll
             for (int c = 0; c < 8; ++c) vpi[c] = __ldg(vpt + (q8 * 8 + c) * kTile + lane);
+            double f8[8], v8[8];
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
                 const int col = q8 * 8 + c;
                 const int j = j0 + col;
                 const int32_t vk = vpi[c] < a.rcp_max ? vpi[c] : a.rcp_max;
-                acc[col] = vk > 0 ? acc[col] * kFxNumScale * __ldg(a.rcp + vk) : 0.0;  // f2, in place
+                f8[c] = vk > 0 ? acc[col] * kFxNumScale * __ldg(a.rcp + vk) : 0.0;
+                v8[c] = static_cast<double>(vpi[c]);
                 if (i < P && j < P && !(diag && j < i)) {
                     const int64_t ij = row_i + static_cast<int64_t>(P) * j;
-                    __stcs(o.f2 + ij, acc[col]);
-                    __stcs(o.vp + ij, static_cast<double>(vpi[c]));
+                    __stcs(o.f2 + ij, f8[c]);
+                    __stcs(o.vp + ij, v8[c]);
                 }
             }
-            const int jj = j0 + q8 * 8 + (lane & 7);
+            const int jr = j0 + q8 * 8;  // the run's first j
+            if (i < P && jr + 7 < P && !(diag && jr <= i)) {
+                store_run8(o.f2 + col_i + jr, f8);
+                store_run8(o.vp + col_i + jr, v8);
+            } else if (i < P) {
 #pragma unroll
-            for (int part = 0; part < 2; ++part) {
-                double* out = part == 0 ? o.f2 : o.vp;
-#pragma unroll
-                for (int c = 0; c < 8; ++c)
-                    stage[lane * kStagePitch + c] = part == 0 ? acc[q8 * 8 + c] : static_cast<double>(vpi[c]);
-                __syncwarp();
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int rr = 4 * k + (lane >> 3);
-                    if (i0 + rr < P && jj < P && !(diag && jj <= i0 + rr))
-                        __stcs(out + row_j0 + static_cast<int64_t>(P) * rr + jj, stage[rr * kStagePitch + (lane & 7)]);
+                for (int c = 0; c < 8; ++c) {
+                    const int j = jr + c;
+                    if (j < P && !(diag && j <= i)) {
+                        __stcs(o.f2 + col_i + j, f8[c]);
+                        __stcs(o.vp + col_i + j, v8[c]);
+                    }
                 }
-                __syncwarp();
             }
             // Keep the next group's count loads after this group's stores (they would
             // otherwise all be hoisted, and held, at once).
@@ -449,9 +488,7 @@ f2_fx_kernel(const __grid_constant__ FxArgs a) {
         if (warp == 0 && lane == 0) fx_producer<kGrouped>(a, smem, ctl);
         if (warp == 1 && lane == 0) fx_issuer<kGrouped>(a, smem, ctl, tmem);
     } else {
-        fx_epilogue<kGrouped>(a, ctl, tmem, warp, lane,
-                              reinterpret_cast<double*>(smem + kStages * kStageBytes + kCtlBytes) +
-                                  (warp - kEpiWarp0) * kStageDoubles);
+        fx_epilogue<kGrouped>(a, ctl, tmem, warp, lane);
     }
     tc_fence_before();
     __syncthreads();
@@ -459,7 +496,7 @@ f2_fx_kernel(const __grid_constant__ FxArgs a) {
     if (warp == 1) tmem_dealloc(tmem, kTmemCols);
 }
 
-constexpr size_t kFxSmemBytes = kStages * kStageBytes + kCtlBytes + kEpiWarps * kStageDoubles * sizeof(double) + 1024;
+constexpr size_t kFxSmemBytes = kStages * kStageBytes + kCtlBytes + 1024;
 
 // ============================== vpair kernel ==============================================
 
