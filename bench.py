@@ -244,10 +244,12 @@ def units(P: int, M: int) -> float:
     return float(M) * P * (P - 1) / 2.0
 
 
-def band_d2h_bytes(P: int, B: int, band: int = 128) -> int:
-    """Bytes the host-output extraction downloads per call: f2 and vpair, the upper row bands
-    of every P x P slab (band t: rows [t*band, t*band + band) x columns [t*band, P))."""
-    return 2 * 8 * B * sum(min(band, P - r0) * (P - r0) for r0 in range(0, P, band))
+def host_d2h_bytes(P: int, B: int, wide: bool = False, tile: int = 128) -> int:
+    """Bytes the host-output extraction downloads per call: every f2 slab whole (FP64), and
+    the vpair slabs as their upper tile x tile tiles (row tile <= column tile) of 16-bit
+    counts (32-bit when a block has 65,536 SNPs or more)."""
+    t = -(-P // tile)
+    return 8 * B * P * P + (4 if wide else 2) * B * (t * (t + 1) // 2) * tile * tile
 
 
 def make_panel(workload: str, rank: int, device: str, n_snp: int | None = None):
@@ -357,6 +359,7 @@ def run_reference(args, rank: int, world: int):
 def run_e2e(args, ctx, rec, panel, sel, po, bpr, n_out, barrier, dist, dev, P, M, B, world):
     """End to end through the C ABI with pinned host buffers: H2D of the genotypes,
     extraction, D2H of the FP64 f2 and vpair tensors, every step."""
+    import numpy as np
     import torch
 
     rec_h = torch.empty((M, bpr), dtype=torch.uint8, pin_memory=True)
@@ -377,10 +380,11 @@ def run_e2e(args, ctx, rec, panel, sel, po, bpr, n_out, barrier, dist, dev, P, M
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    # Host output through the tensor-core path: only the upper 128-row bands of every
-    # (exactly symmetric) slab cross PCIe and the library fills the lower tiles on the host.
-    banded = args.precision != "fp32" and B >= 2 and P > 0
-    d2h = band_d2h_bytes(P, B) if banded else 2 * n_out * 8
+    # Host output through the tensor-core path: the f2 slabs cross PCIe whole and the vpair
+    # slabs as packed upper tiles of counts, which the library widens on the host.
+    segmented = args.precision != "fp32" and B >= 2 and P > 0
+    wide = int(np.bincount(panel.block_id).max()) > 65535 if segmented else False
+    d2h = host_d2h_bytes(P, B, wide) if segmented else 2 * n_out * 8
     e2e = {"value": units(P, M) * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(rec_h.numel()),
            "d2h_bytes_per_step": int(d2h), "output_bytes_per_step": int(2 * n_out * 8),
            "ms_per_step": 1000.0 * e2e_s, "steps": e2e_steps}
@@ -551,8 +555,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c5: only the many-requests measurement (grouped batch vs serial)")
-    ap.add_argument("--precision", default="split_f16")
-    ap.add_argument("--also", default="split_f16,fixed_i8,split_bf16,split_f16_fine",
+    ap.add_argument("--precision", default="fixed_i8")
+    ap.add_argument("--also", default="split_f16,split_bf16,split_f16_fine",
                     help="other tensor-core arithmetics timed beside the headline (comma-separated, or none)")
     ap.add_argument("--compare-simt", action="store_true", default=True)
     ap.add_argument("--no-compare-simt", dest="compare_simt", action="store_false")

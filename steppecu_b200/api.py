@@ -28,7 +28,7 @@ PRECISIONS = {
 }
 PRECISION_TAGS = {L.PREC_FP32_SIMT: "fp32_simt", L.PREC_SPLIT_BF16: "split_bf16", L.PREC_SPLIT_F16: "split_f16",
                   L.PREC_SPLIT_F16_FINE: "split_f16_fine", L.PREC_FIXED_I8: "fixed_i8"}
-DEFAULT_PRECISION = "split_f16"
+DEFAULT_PRECISION = "fixed_i8"
 
 PLOIDY = {"auto": L.PLOIDY_AUTO, "1": L.PLOIDY_PSEUDO, "pseudo": L.PLOIDY_PSEUDO,
           "pseudo_haploid": L.PLOIDY_PSEUDO, "2": L.PLOIDY_DIPLOID, "diploid": L.PLOIDY_DIPLOID}

@@ -491,25 +491,6 @@ void parallel_for(int n, F&& f) {
         if (e) std::rethrow_exception(e);
 }
 
-// Copies the upper row bands of slabs [0, nb) of a device slab run into the host run: per
-// row tile, one 3-D copy of rows [r0, r0 + T) x columns [r0, P) x every slab.
-void download_upper_bands(double* host, const double* dev, int64_t P, int64_t T, int64_t nb, cudaStream_t st) {
-    for (int64_t r0 = 0; r0 < P; r0 += T) {
-        const int64_t nr = std::min(T, P - r0);
-        cudaMemcpy3DParms m{};
-        m.srcPtr = make_cudaPitchedPtr(const_cast<double*>(dev), static_cast<size_t>(P) * sizeof(double),
-                                       static_cast<size_t>(P) * sizeof(double), static_cast<size_t>(P));
-        m.dstPtr = make_cudaPitchedPtr(host, static_cast<size_t>(P) * sizeof(double),
-                                       static_cast<size_t>(P) * sizeof(double), static_cast<size_t>(P));
-        m.srcPos = make_cudaPos(static_cast<size_t>(r0) * sizeof(double), static_cast<size_t>(r0), 0);
-        m.dstPos = m.srcPos;
-        m.extent = make_cudaExtent(static_cast<size_t>(nr) * sizeof(double), static_cast<size_t>(P - r0),
-                                   static_cast<size_t>(nb));
-        m.kind = cudaMemcpyDeviceToHost;
-        STPF2_CUDA(cudaMemcpy3DAsync(&m, st));
-    }
-}
-
 // On an error, copies between the device and the caller's buffers may still be in flight:
 // drains the context's streams before the error reaches the caller (who may free them).
 struct DrainOnError {
@@ -531,23 +512,55 @@ struct DrainOnError {
 // contraction waits for the download of segment k-2 from the same buffer), so the output
 // tensor itself may exceed device memory (the out-of-core tier: only the host holds all
 // P x P x B slabs).
-// Segments of whole blocks, each about a twelfth of the SNPs and the first at least the
-// ploidy window: bounds[k]..bounds[k+1] are segment k's blocks.
+// Segments of whole blocks: bounds[k]..bounds[k+1] are segment k's blocks. Most hold about
+// a twelfth of the SNPs; the first two and the last two ramp (1/48, 1/24 of the SNPs), so
+// the first download starts soon after the call and the host's work on the last segment
+// is short. The first segment covers at least the ploidy window.
 std::vector<int> segment_bounds(const BlockLayout& L) {
     const int B = L.n_block;
     const int64_t M = L.n_snp;
     const int64_t window = std::min<int64_t>(M, 1000);
-    const int64_t target = std::max<int64_t>((M + 11) / 12, window);
-    std::vector<int> bounds{0};
-    int64_t acc = 0;
-    for (int b = 0; b < B; ++b) {
-        acc += L.blocks[b].k;
-        if (acc >= target && b + 1 < B) {
-            bounds.push_back(b + 1);
-            acc = 0;
+    const int64_t full = std::max<int64_t>((M + 11) / 12, window);
+    const int64_t ramp[2] = {std::max<int64_t>((M + 47) / 48, window), std::max<int64_t>((M + 23) / 24, window)};
+    // The tail: the last blocks, walked backwards, into segments of 1/48 and 1/24.
+    std::vector<int> tail;  // first block of each tail segment, last segment first
+    {
+        int64_t acc = 0;
+        int t = 0;
+        for (int b = B - 1; b > 0 && t < 2; --b) {
+            acc += L.blocks[b].k;
+            if (acc >= ramp[t]) {
+                tail.push_back(b);
+                acc = 0;
+                ++t;
+            }
         }
     }
+    const int tail_begin = tail.empty() ? B : tail.back();
+    std::vector<int> bounds{0};
+    int64_t acc = 0;
+    int seg = 0;
+    for (int b = 0; b < tail_begin; ++b) {
+        acc += L.blocks[b].k;
+        const int64_t target = seg < 2 ? ramp[seg] : full;
+        if (acc >= target && b + 1 < tail_begin) {
+            bounds.push_back(b + 1);
+            acc = 0;
+            ++seg;
+        }
+    }
+    // The first segment must still reach the ploidy window when the head is all there is.
+    for (auto it = tail.rbegin(); it != tail.rend(); ++it)
+        if (*it > bounds.back()) bounds.push_back(*it);
     bounds.push_back(B);
+    // The ploidy window: merge leading segments until the first spans it.
+    int64_t first = 0;
+    size_t merge = 1;
+    for (; merge + 1 < bounds.size(); ++merge) {
+        for (int b = bounds[merge - 1]; b < bounds[merge]; ++b) first += L.blocks[b].k;
+        if (first >= window) break;
+    }
+    if (merge > 1) bounds.erase(bounds.begin() + 1, bounds.begin() + static_cast<long>(merge));
     return bounds;
 }
 
@@ -564,23 +577,34 @@ struct SlabTarget {
 
 // The segmented contraction pass with host output. before(k) enqueues what segment k needs
 // on the context stream before its contraction (uploads, decode); the contraction of
-// segment k goes into a two-segment device ring (it waits for the download of segment
-// k - 2 from the same buffer), only the upper 128-row bands of each (exactly symmetric)
-// slab cross PCIe, and the host fills the lower tiles once the download has landed. With a
-// sink, at most two segments are in flight and each is handed over before its staging
-// slot is reused.
+// segment k goes into a two-segment device ring (it waits for the downloads of segment
+// k - 2 from the same buffers). The f2 slabs cross PCIe whole (one contiguous copy per
+// segment); the vpair slabs cross as packed 16-bit upper tiles (counts_pack.cu), which
+// the host widens into both halves of each slab once they have landed. The split keeps
+// both PCIe and the host's memory traffic near their floors: f2 is 8 bytes per element
+// either way, and counts are integers of at most a block's SNP count. With a sink, at most
+// two segments are in flight and each is handed over before its staging slot is reused.
 template <class Before>
-void contract_segments(Ctx& c, UmmaPlan* up, int P, const std::vector<int>& bounds, const SlabTarget& t,
-                       Before&& before) {
-    constexpr int64_t kBand = 128;  // rows per downloaded band (one contraction tile)
+void contract_segments(Ctx& c, UmmaPlan* up, int P, const BlockLayout& L, const std::vector<int>& bounds,
+                       const SlabTarget& t, Before&& before) {
     const size_t slab = static_cast<size_t>(P) * static_cast<size_t>(P);
     const size_t nseg = bounds.size() - 1;
     size_t ring = 1;  // slabs per ring buffer: the largest segment
     for (size_t k = 0; k < nseg; ++k) ring = std::max<size_t>(ring, static_cast<size_t>(bounds[k + 1] - bounds[k]));
+    int32_t kmax = 0;
+    for (const BlockInfo& b : L.blocks) kmax = std::max(kmax, b.k);
+    const bool wide = kmax > 65535;  // counts past 16 bits: 32-bit packing
+    const size_t cnt_slab = packed_counts_bytes(P, 1, wide);
     c.ws_f2.reserve(2 * ring * slab * sizeof(double));
     c.ws_vpair.reserve(2 * ring * slab * sizeof(double));
-    if (t.sink) c.pin_stage.reserve(4 * ring * slab * sizeof(double));
-    std::vector<cudaEvent_t> ev(2 * nseg, nullptr);  // per segment: contracted, downloaded
+    c.ws_counts.reserve(2 * ring * cnt_slab);
+    if (t.sink) {
+        c.pin_stage.reserve(4 * ring * slab * sizeof(double));
+        c.pin_counts.reserve(2 * ring * cnt_slab);
+    } else {
+        c.pin_counts.reserve(static_cast<size_t>(L.n_block) * cnt_slab);
+    }
+    std::vector<cudaEvent_t> ev(2 * nseg, nullptr);  // per segment: contracted and packed, downloaded
     struct Free {
         std::vector<cudaEvent_t>& ev;
         ~Free() {
@@ -595,17 +619,23 @@ void contract_segments(Ctx& c, UmmaPlan* up, int P, const std::vector<int>& boun
     auto host_vp = [&](size_t k) {
         return t.sink ? c.pin_stage.as<double>() + (2 + k % 2) * ring * slab : t.vpair + slab * bounds[k];
     };
+    auto host_cnt = [&](size_t k) {
+        return c.pin_counts.as<uint8_t>() + (t.sink ? (k % 2) * ring : static_cast<size_t>(bounds[k])) * cnt_slab;
+    };
     auto enqueue = [&](size_t k) {
         const int b0 = bounds[k], b1 = bounds[k + 1];
+        const size_t nb = static_cast<size_t>(b1 - b0);
         double* f2k = c.ws_f2.as<double>() + (k % 2) * ring * slab;
         double* vpk = c.ws_vpair.as<double>() + (k % 2) * ring * slab;
+        uint8_t* cntk = c.ws_counts.as<uint8_t>() + (k % 2) * ring * cnt_slab;
         before(k);
-        if (k >= 2) STPF2_CUDA(cudaStreamWaitEvent(c.stream, ev[2 * (k - 2) + 1], 0));  // ring buffer free
+        if (k >= 2) STPF2_CUDA(cudaStreamWaitEvent(c.stream, ev[2 * (k - 2) + 1], 0));  // ring buffers free
         launch_f2_umma_blocks(c, up, b0, b1, f2k, vpk, c.stream, true);
+        launch_pack_counts(c, vpk, P, static_cast<int64_t>(nb), wide, cntk, c.stream);
         STPF2_CUDA(cudaEventRecord(ev[2 * k], c.stream));
         STPF2_CUDA(cudaStreamWaitEvent(c.d2h, ev[2 * k], 0));
-        download_upper_bands(host_f2(k), f2k, P, kBand, b1 - b0, c.d2h);
-        download_upper_bands(host_vp(k), vpk, P, kBand, b1 - b0, c.d2h);
+        STPF2_CUDA(cudaMemcpyAsync(host_f2(k), f2k, nb * slab * sizeof(double), cudaMemcpyDeviceToHost, c.d2h));
+        STPF2_CUDA(cudaMemcpyAsync(host_cnt(k), cntk, nb * cnt_slab, cudaMemcpyDeviceToHost, c.d2h));
         STPF2_CUDA(cudaEventRecord(ev[2 * k + 1], c.d2h));
     };
     const size_t depth = t.sink ? 2 : nseg;
@@ -616,10 +646,8 @@ void contract_segments(Ctx& c, UmmaPlan* up, int P, const std::vector<int>& boun
         const int nb = bounds[k + 1] - bounds[k];
         double* f2h = host_f2(k);
         double* vph = host_vp(k);
-        parallel_for(2 * nb, [&](int u) {
-            double* base = (u % 2 == 0) ? f2h : vph;
-            mirror_lower_tiles(base + slab * static_cast<size_t>(u / 2), P, kBand);
-        });
+        const uint8_t* cnt = host_cnt(k);
+        parallel_for(nb, [&](int u) { expand_counts(cnt + u * cnt_slab, wide, vph + slab * static_cast<size_t>(u), P); });
         if (t.sink && t.sink(t.user, bounds[k], bounds[k + 1], f2h, vph) != 0)
             fail(STP_RUNTIME_ERROR, "the slab sink stopped the extraction");
     }
@@ -654,7 +682,7 @@ void run_pipelined(Ctx& c, const stp_f2_request& r, const SlabTarget& t, Plan& p
     } free_events{up_ev};
     for (auto& e : up_ev) STPF2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     int64_t rec_end = 0;
-    contract_segments(c, p.umma, p.P, bounds, t, [&](size_t k) {
+    contract_segments(c, p.umma, p.P, L, bounds, t, [&](size_t k) {
         const int b0 = bounds[k], b1 = bounds[k + 1];
         const int64_t nsnp = snp0[k + 1] - snp0[k];
         if (upload) {
@@ -683,6 +711,82 @@ void run_pipelined(Ctx& c, const stp_f2_request& r, const SlabTarget& t, Plan& p
     });
 }
 
+// The plan of the last one-shot extraction, kept on the context with a copy of everything
+// it was built from: a later call whose request is identical (same shapes, selection,
+// ploidy, block ids and kept rows, compared element by element, and the same workspace
+// the plan borrows) reuses its validated tables instead of building and uploading them
+// again. The records are not part of the key: every pass re-detects ploidy and re-decodes.
+struct PlanCache {
+    std::unique_ptr<Plan> plan;
+    int32_t n_pop = 0, n_block = 0, precision = 0, ploidy_mode = 0;
+    int64_t n_snp = 0, n_ind = 0, n_kept = 0;
+    uint64_t bpr = 0, pitch = 0;
+    int32_t on_device = 0;
+    std::vector<int64_t> sel_rows, pop_offsets, kept_rows;
+    std::vector<int32_t> sample_ploidy, block_id;
+    const void* ws[3] = {nullptr, nullptr, nullptr};
+
+    template <class T>
+    static bool same(const std::vector<T>& v, const T* a, size_t n) {
+        if (a == nullptr) return v.empty() && n == 0;
+        return v.size() == n && (n == 0 || std::memcmp(v.data(), a, n * sizeof(T)) == 0);
+    }
+    bool matches(const Ctx& c, const stp_f2_request& r, uint64_t dpitch) const {
+        const int64_t n_sel = r.n_pop > 0 ? r.pop_offsets[r.n_pop] : 0;
+        const size_t n_axis = static_cast<size_t>(r.kept_rows ? r.n_kept : r.geno.n_snp);
+        return plan && r.n_pop == n_pop && r.n_block == n_block && r.precision == precision &&
+               r.ploidy_mode == ploidy_mode && r.geno.n_snp == n_snp && r.geno.n_ind == n_ind &&
+               r.n_kept == n_kept && r.geno.bytes_per_record == bpr && dpitch == pitch &&
+               r.geno.on_device == on_device && ws[0] == c.ws_misc.ptr && ws[1] == c.ws_canon.ptr &&
+               ws[2] == c.ws_center.ptr && n_sel >= 0 &&
+               same(pop_offsets, r.pop_offsets, r.n_pop > 0 ? static_cast<size_t>(r.n_pop) + 1 : 0) &&
+               same(sel_rows, r.sel_rows, static_cast<size_t>(n_sel)) &&
+               same(sample_ploidy, r.sample_ploidy, r.sample_ploidy ? static_cast<size_t>(n_sel) : 0) &&
+               same(kept_rows, r.kept_rows, r.kept_rows ? static_cast<size_t>(r.n_kept) : 0) &&
+               same(block_id, r.block_id, n_axis);
+    }
+};
+
+// The cached plan for this request, or null (the cache is emptied either way: a plan is
+// owned by one call at a time).
+std::unique_ptr<Plan> take_cached_plan(Ctx& c, const stp_f2_request& r, uint64_t dpitch) {
+    auto pc = std::static_pointer_cast<PlanCache>(c.plan_cache);
+    if (!pc || !pc->matches(c, r, dpitch)) return nullptr;
+    return std::move(pc->plan);
+}
+
+// Keeps a plan that a call has finished with, keyed by the request it was built from.
+void keep_plan(Ctx& c, const stp_f2_request& r, uint64_t dpitch, std::unique_ptr<Plan> p, bool hit) {
+    auto pc = std::static_pointer_cast<PlanCache>(c.plan_cache);
+    if (hit && pc) {  // the key is unchanged
+        pc->plan = std::move(p);
+        return;
+    }
+    pc = std::make_shared<PlanCache>();
+    const int64_t n_sel = r.n_pop > 0 ? r.pop_offsets[r.n_pop] : 0;
+    const size_t n_axis = static_cast<size_t>(r.kept_rows ? r.n_kept : r.geno.n_snp);
+    pc->n_pop = r.n_pop;
+    pc->n_block = r.n_block;
+    pc->precision = r.precision;
+    pc->ploidy_mode = r.ploidy_mode;
+    pc->n_snp = r.geno.n_snp;
+    pc->n_ind = r.geno.n_ind;
+    pc->n_kept = r.n_kept;
+    pc->bpr = r.geno.bytes_per_record;
+    pc->pitch = dpitch;
+    pc->on_device = r.geno.on_device;
+    if (r.n_pop > 0) pc->pop_offsets.assign(r.pop_offsets, r.pop_offsets + r.n_pop + 1);
+    if (n_sel > 0) pc->sel_rows.assign(r.sel_rows, r.sel_rows + n_sel);
+    if (r.sample_ploidy && n_sel > 0) pc->sample_ploidy.assign(r.sample_ploidy, r.sample_ploidy + n_sel);
+    if (r.kept_rows && r.n_kept > 0) pc->kept_rows.assign(r.kept_rows, r.kept_rows + r.n_kept);
+    if (r.block_id && n_axis > 0) pc->block_id.assign(r.block_id, r.block_id + n_axis);
+    pc->ws[0] = c.ws_misc.ptr;
+    pc->ws[1] = c.ws_canon.ptr;
+    pc->ws[2] = c.ws_center.ptr;
+    pc->plan = std::move(p);
+    c.plan_cache = pc;
+}
+
 void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
     // The padded SNP axis is 32-bit: refuse M > INT_MAX before reading or allocating
     // anything (the reference throws std::runtime_error for it).
@@ -706,12 +810,15 @@ void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
         d_rec = c.ws_records.as<uint8_t>();
         pitch = dp;
     }
-    // Operand planes borrow the context's grow-only workspace.
-    {
+    // A repeated request reuses its plan (whose operand planes already sit in the
+    // workspace); otherwise the operand planes borrow the context's grow-only workspace.
+    std::unique_ptr<Plan> p = take_cached_plan(c, r, pitch);
+    const bool hit = p != nullptr;
+    if (!hit) {
         const BlockLayout probe = make_block_layout(r.block_id, snp_axis(r), r.n_block);
         c.ws_misc.reserve(operand_plane_bytes(fmt_of(r.precision), std::max(r.n_pop, 1), probe.ld));
+        p = build_plan(c, r, pitch, c.ws_misc.ptr, true);
     }
-    std::unique_ptr<Plan> p = build_plan(c, r, pitch, c.ws_misc.ptr, true);
     if (o.block_sizes) copy_block_sizes(p->L, o.block_sizes);
     const size_t out_elems = static_cast<size_t>(std::max(r.n_pop, 0)) * std::max(r.n_pop, 0) * std::max(r.n_block, 0);
     if (pipelined && p->umma && !p->repitch && out_elems) {
@@ -744,6 +851,7 @@ void extract_one(Ctx& c, const stp_f2_request& r, stp_f2_output& o) {
     }
     STPF2_CUDA(cudaStreamSynchronize(s));
     umma_check(p->umma);
+    keep_plan(c, r, pitch, std::move(p), hit);
 }
 
 // ---- grouped batch ----------------------------------------------------------------------
@@ -1626,7 +1734,7 @@ void f2_from_qvn(Ctx& c, const double* Q, const double* V, const double* N, int 
     } else {
         // Host output, streamed or not: segments of blocks through the device ring.
         STPF2_CUDA(cudaStreamSynchronize(s));
-        contract_segments(c, up.get(), P, segment_bounds(L), t, [](size_t) {});
+        contract_segments(c, up.get(), P, L, segment_bounds(L), t, [](size_t) {});
     }
     STPF2_CUDA(cudaStreamSynchronize(s));
     umma_check(up.get());

@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include "../../include/stpf2.h"
@@ -121,9 +122,14 @@ struct Ctx {
     DevBuf ws_vpc;    // grouped fixed-point batches: compact vpair tiles
     PinnedBuf pin_union, pin_tables, pin_items;
     PinnedBuf pin_stage;  // streamed extraction: the two-segment staging ring of f2 / vpair slabs
+    DevBuf ws_counts;      // host-output path: packed vpair tiles of two segments
+    PinnedBuf pin_counts;  // their host staging (every segment, or a two-segment ring with a sink)
     // Completion time of each request of the last stp_f2_extract_batch call, in ms from the
     // start of its group's device work (NaN for requests that ran on their own).
     std::vector<double> last_batch_ms;
+    // The plan of the last one-shot extraction with its request, reused by the next call
+    // with an identical request (stpf2_abi.cu: PlanCache).
+    std::shared_ptr<void> plan_cache;
 };
 
 // ---- block layout ---------------------------------------------------------------------
@@ -421,9 +427,12 @@ void launch_fstat_assemble(Ctx& c, const double* f2, int P, const int32_t* surv,
 void launch_jackknife(Ctx& c, const double* x, const int32_t* block_sizes, int64_t m, int nb,
                       double* est, double* var, cudaStream_t s);
 
-// Fills the lower tiles of a symmetric P x P column-major slab whose upper row bands of T
-// rows (band t: rows [t*T, t*T + T) x columns [t*T, P)) are in place (host_mirror.cpp).
-void mirror_lower_tiles(double* S, int64_t P, int64_t T);
+// Host-output vpair transfer (counts_pack.cu, host_expand.cpp): the upper 128 x 128 tiles of
+// nb count slabs packed as 16-bit (wide: 32-bit) integers, and their widening on the host
+// into both halves of one P x P FP64 slab.
+size_t packed_counts_bytes(int P, int64_t nb, bool wide);
+void launch_pack_counts(Ctx& c, const double* vp, int P, int64_t nb, bool wide, void* out, cudaStream_t s);
+void expand_counts(const void* packed, bool wide, double* S, int64_t P);
 
 // Allocation-free count decode (noalloc.cu): every intermediate lives in one static
 // device array of kNoAllocScratchBytes.

@@ -1,6 +1,6 @@
 """The bench line's arithmetic, on CPU: the metric's units, the issued tensor work of the
 split contraction counted from its MMA schedule, and the bytes the host-output extraction
-downloads (its upper row bands, emulated element by element)."""
+downloads (whole f2 slabs and packed upper tiles of counts)."""
 from __future__ import annotations
 
 import importlib.util
@@ -35,12 +35,14 @@ def test_issued_work_matches_mma_count(P):
 
 
 @pytest.mark.parametrize("P", [1, 5, 128, 129, 300, 1000])
-def test_band_bytes_match_band_copies(P):
+def test_host_d2h_bytes_match_the_copies(P):
     B = 3
-    covered = np.zeros((P, P), bool)  # [row i, column j]
+    upper = np.zeros((P, P), bool)  # [row i, column j]: the packed upper tiles
     for r0 in range(0, P, 128):
-        covered[r0:r0 + 128, r0:P] = True
-    assert bench.band_d2h_bytes(P, B) == 2 * 8 * B * int(covered.sum())
-    assert np.all(covered | covered.T)  # the bands and their transposes cover every element
-    if P <= 128:
-        assert bench.band_d2h_bytes(P, B) == 2 * 8 * B * P * P
+        upper[r0:r0 + 128, r0:P] = True
+    assert np.all(upper | upper.T)  # the tiles and their transposes cover every element
+    t = -(-P // 128)
+    packed = t * (t + 1) // 2 * 128 * 128  # counts per slab, with each tile padded to 128 x 128
+    assert packed >= int(upper.sum())
+    assert bench.host_d2h_bytes(P, B) == B * (8 * P * P + 2 * packed)
+    assert bench.host_d2h_bytes(P, B, wide=True) == B * (8 * P * P + 4 * packed)

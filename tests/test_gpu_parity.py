@@ -32,7 +32,7 @@ TOL = {
     "fixed_i8": (1e-6, 1e-9),
 }
 MODES = ["fp32", "split_bf16", "split_f16", "split_f16_fine", "fixed_i8"]
-TC_DEFAULT = "split_f16"
+TC_DEFAULT = "fixed_i8"
 
 
 def oracle_f2(panel, sel, po, ploidy=None, block_id=None, n_block=None):
@@ -381,18 +381,23 @@ def test_int_max_and_device_oom_statuses(ctx):
     assert t.f2.size == 16 * p.n_block
 
 
-@pytest.mark.parametrize("n_pop,misalign", [(600, False), (603, False), (600, True)])
-def test_host_band_download_equals_device_output(n_pop, misalign):
-    """Host outputs receive only the upper 128-row bands of each slab over PCIe and the
-    library fills the lower tiles on the host: with 4 x 4 register transposes when P % 4 == 0
-    and the output is 32-byte aligned, else with scalar copies (P = 603, and an output that
+@pytest.mark.parametrize("n_pop,misalign,wide", [(600, False, False), (603, False, False), (600, True, False),
+                                                  (130, False, True)])
+def test_host_output_equals_device_output(n_pop, misalign, wide):
+    """Host outputs receive every f2 slab whole and the vpair slabs as packed upper tiles of
+    16-bit counts (32-bit when a block has 65,536 SNPs or more), which the library widens
+    into both halves of each slab on the host: with AVX2 streaming stores when P % 4 == 0 and
+    the output is 32-byte aligned, else element by element (P = 603, and an output that
     starts 8 bytes past an aligned address). Each equals the device-output extraction bit
     for bit."""
     import torch
 
     from steppecu_b200 import Context
 
-    p = synth.generate("c3", seed=n_pop, n_snp=6_000, n_pop=n_pop)
+    p = synth.generate("c3", seed=n_pop, n_snp=70_000 if wide else 6_000, n_pop=n_pop)
+    if wide:  # one block of 66,000 SNPs, then one of 4,000
+        p.block_id = (np.arange(p.n_snp) >= 66_000).astype(np.int32)
+        p.n_block = 2
     sel, po = p.selection()
     rec = p.records_numpy()
     P, B = p.n_pop, p.n_block
@@ -409,12 +414,15 @@ def test_host_band_download_equals_device_output(n_pop, misalign):
         f2h, vph = np.zeros(n), np.zeros(n)
     f2d = torch.zeros(n, dtype=torch.float64, device="cuda")
     vpd = torch.zeros_like(f2d)
-    with Context(0) as c:
-        c.extract_blocks(rec, p.n_ind, sel, po, p.block_id, B, precision="split_f16", out=(f2h, vph))
-        c.extract_blocks(torch.from_numpy(rec).cuda(), p.n_ind, sel, po, p.block_id, B, precision="split_f16",
-                         out=(f2d, vpd))
-    assert np.array_equal(f2h, f2d.cpu().numpy())
-    assert np.array_equal(vph, vpd.cpu().numpy())
+    for mode in ("fixed_i8", "split_f16"):
+        with Context(0) as c:
+            c.extract_blocks(rec, p.n_ind, sel, po, p.block_id, B, precision=mode, out=(f2h, vph))
+            c.extract_blocks(torch.from_numpy(rec).cuda(), p.n_ind, sel, po, p.block_id, B, precision=mode,
+                             out=(f2d, vpd))
+        assert np.array_equal(f2h, f2d.cpu().numpy())
+        assert np.array_equal(vph, vpd.cpu().numpy())
+    if wide:
+        assert vph.max() > 65535
 
 
 def test_host_streaming_bounds_device_output_memory():
