@@ -42,7 +42,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # bytes the decode writes per (population, SNP) in it.
 DTYPES = {"split_bf16": "bf16x3", "split_f16": "f16x3", "split_f16_fine": "f16x3", "fixed_i8": "i8x4 (int32 exact)",
           "fp32": "f32"}
-OPERAND_BYTES = {"split_bf16": 11, "split_f16": 11, "split_f16_fine": 11, "fixed_i8": 10, "fp32": 9}
+OPERAND_BYTES = {"split_bf16": 11, "split_f16": 11, "split_f16_fine": 11, "fixed_i8": 9, "fp32": 9}
 # dram__bytes_read.sum + dram__bytes_write.sum of one f2_umma_kernel launch (ncu, one pass).
 CONTRACTION_TRAFFIC = {("c3", "split_f16"): 13.58e9 + 12.24e9}
 

@@ -259,10 +259,6 @@ __device__ __forceinline__ void emit8_fx(const OperandPlanes& op, int i, int64_t
         else mv.y |= b << (8 * (c - 4));
     }
     *reinterpret_cast<uint2*>(img + 8 * kTile8Bytes) = mv;
-    // The separate M tiles hold m itself (0/1): the vpair contraction counts exactly.
-    mv.x = (mv.x >> 6) & 0x01010101u;
-    mv.y = (mv.y >> 6) & 0x01010101u;
-    *reinterpret_cast<uint2*>(op.mtiles + tile * kTile8Bytes + tile8_offset(r, k)) = mv;
 }
 
 // One element (the Q/V/N feeder): q, n as FP64.
@@ -283,7 +279,6 @@ __device__ __forceinline__ void emit_fx(const OperandPlanes& op, int i, int64_t 
     }
     const uint8_t m = valid ? uint8_t(kFxM) : uint8_t(0);
     img[8 * kTile8Bytes] = m;
-    op.mtiles[tile * kTile8Bytes + tile8_offset(r, k)] = valid ? 1 : 0;
 }
 
 // ---- canonical genotypes -------------------------------------------------------------------

@@ -17,18 +17,20 @@
 //                                                       i.e. 1.7e-10, per SNP)
 //     V_w += E_w(i) M(j) + M(i) E_w(j)                  (E_3..E_6: the digits of -A)
 // i.e. 18 kind::i8 MMAs (M = N = 128, K = 32) per 32-SNP stage, all integer and exact.
-// The epilogue forms W = sum_w V_w 256^(w-3) in FP64 once per tile (every 16,384 SNPs of
-// a longer block, the int32 bound), f2 = W * kFxNumScale / vpair (0 when vpair = 0,
-// f2_estimator.hpp:42-46), and stores (i,j) and (j,i) of the block's slab.
+// The epilogue forms W = sum_w V_w 256^(w-3) exactly in int64 once per tile (every 16,384
+// SNPs of a longer block, the int32 bound; segments add in FP64), f2 = W * kFxNumScale /
+// vpair (0 when vpair = 0, f2_estimator.hpp:42-46), and stores (i,j) and (j,i) of the
+// block's slab.
 //
 // Error against exact arithmetic, per SNP and pair: the two roundings of x (2^-32.0 each,
 // times |x| <= 1/2, twice), of a (2^-33, twice) and the dropped digit products: under
 // 7e-10 on T; a block mean over K SNPs averages independent roundings (~1e-10 / sqrt(K)).
 //
 // vpair_fx_kernel runs first over the same items: the exact both-present counts
-// m_i . m_j (one kind::i8 MMA per 32 SNPs on the separate 0/1 M tiles, 128 SNPs per
-// stage, a ring of four TMEM accumulators) written as one compact int32 128x128 tile per
-// item, which the f2 epilogue reads for its divide and its vpair stores. (The four f2
+// m_i . m_j (one kind::i8 MMA per 32 SNPs on the images' M planes, 64 m on both sides, so
+// 4096 per SNP; 128 SNPs per stage, a ring of four TMEM accumulators, at most 524,160
+// SNPs per accumulation) written as one compact int32 128x128 tile per item, which the f2
+// epilogue reads for its divide and its vpair stores. (The four f2
 // accumulators fill TMEM's 512 columns, so the counts cannot share the f2 kernel.)
 //
 //   f2_fx_kernel:   warp 0 producer (one 36 KiB bulk copy per stage side, no tensor maps, no
@@ -77,10 +79,13 @@ constexpr int kVpAcc = 4;  // TMEM ring of 128-column accumulators
 constexpr int kVpEpiWarps = 8;
 constexpr int kVpThreads = 32 * (2 + kVpEpiWarps);  // 320
 constexpr int kVpCols = 4 * kTile / kVpEpiWarps;   // 64
+// 32-SNP chunks per accumulation: M = 64 on both sides adds 4096 per both-present SNP, so
+// an int32 accumulator holds 524,160 SNPs (a multiple of the stage's four chunks).
+constexpr int kVpPartChunks = 16380;
+static_assert(4096ll * 32 * kVpPartChunks < (1ll << 31) && kVpPartChunks % kVpChunks == 0, "vpair part");
 
 struct FxArgs {
     const uint8_t* images;  // (row tile t, chunk c) image at (t * n_ck + c) * kFxImageBytes
-    const uint8_t* mtiles;  // (row tile t, chunk c) M tile at (t * n_ck + c) * 4 KiB
     int64_t n_ck;
     const WorkItem* items;
     int n_items;
@@ -307,6 +312,17 @@ __device__ __forceinline__ void stamp(const FxArgs& a, int grp, int lane) {
     }
 }
 
+// int64 -> FP64 without a conversion instruction: each 32-bit half is placed in the
+// mantissa of 2^52 (2^52 + 2^31 for the signed high half) by its bit pattern and the bias
+// subtracted exactly; hi * 2^32 + lo then rounds once (a correctly rounded conversion).
+__device__ __forceinline__ double i64_to_f64(int64_t w) {
+    const int lo = static_cast<int>(static_cast<uint32_t>(w));
+    const int hi = static_cast<int>(static_cast<uint32_t>(static_cast<uint64_t>(w) >> 32) ^ 0x80000000u);
+    const double dl = __hiloint2double(0x43300000, lo) - 4503599627370496.0;  // 2^52
+    const double dh = __hiloint2double(0x43300000, hi) - 4503601774854144.0;  // 2^52 + 2^31
+    return fma(dh, 4294967296.0, dl);
+}
+
 __device__ __forceinline__ void st_cs_v2(double* p, double x, double y) {
     asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(x), "d"(y) : "memory");
 }
@@ -396,11 +412,12 @@ __device__ void fx_epilogue(const FxArgs& a, FxCtl* ctl, uint32_t tmem, int warp
                 tmem_wait_ld();
 #pragma unroll
                 for (int c = 0; c < 8; ++c) {
-                    double x = acc[g8 * 8 + c];
-                    x = fma(static_cast<double>(static_cast<int32_t>(v[0][c])), 1.0, x);
-                    x = fma(static_cast<double>(static_cast<int32_t>(v[1][c])), 256.0, x);
-                    x = fma(static_cast<double>(static_cast<int32_t>(v[2][c])), 65536.0, x);
-                    acc[g8 * 8 + c] = fma(static_cast<double>(static_cast<int32_t>(v[3][c])), 16777216.0, x);
+                    // W of the segment, exact in int64 (|W| < 2^56), then one rounding to FP64.
+                    const int64_t w = static_cast<int64_t>(static_cast<int32_t>(v[0][c])) +
+                                      (static_cast<int64_t>(static_cast<int32_t>(v[1][c])) << 8) +
+                                      (static_cast<int64_t>(static_cast<int32_t>(v[2][c])) << 16) +
+                                      (static_cast<int64_t>(static_cast<int32_t>(v[3][c])) << 24);
+                    acc[g8 * 8 + c] += i64_to_f64(w);
                 }
             }
             tc_fence_before();
@@ -513,23 +530,29 @@ __device__ void vp_producer(const FxArgs& a, uint8_t* smem, FxCtl* ctl) {
             const BlockInfo bi = a.blocks[w.blk];
             const int nch = stages_of(bi.k, kStageK);
             const bool diag = w.ti == w.tj;
-            const uint8_t* mt = a.mtiles;
+            const uint8_t* images = a.images;
             int64_t n_ck = a.n_ck;
             if constexpr (kGrouped) {
-                mt = a.groups[bi.grp].mtiles;
+                images = a.groups[bi.grp].images;
                 n_ck = a.groups[bi.grp].n_ck;
             }
+            // The M tile (plane 8) of each 32-SNP image: one 4 KiB copy per chunk and side.
+            const uint8_t* mi = images + static_cast<int64_t>(w.ti) * n_ck * kFxImageBytes + 8 * kTile8Bytes;
+            const uint8_t* mj = images + static_cast<int64_t>(w.tj) * n_ck * kFxImageBytes + 8 * kTile8Bytes;
             for (int c0 = 0; c0 < nch; c0 += kVpChunks, ++g) {
-                const uint32_t bytes = static_cast<uint32_t>(min(kVpChunks, nch - c0)) * static_cast<uint32_t>(kTile8Bytes);
+                const int n = min(kVpChunks, nch - c0);
+                const uint32_t bytes = static_cast<uint32_t>(n) * static_cast<uint32_t>(kTile8Bytes);
                 const int slot = static_cast<int>(g % kVpStages);
                 if (!waitb(&ctl->empty[slot], ((g / kVpStages) & 1u) ^ 1u, ctl, a)) goto abort;
                 uint8_t* sb = smem + slot * kVpStageBytes;
                 mbar_expect_tx(&ctl->full[slot], diag ? bytes : 2 * bytes);
                 const int64_t chunk = bi.col / kStageK + c0;
-                bulk_load(sb, mt + (static_cast<int64_t>(w.ti) * n_ck + chunk) * kTile8Bytes, bytes, &ctl->full[slot]);
-                if (!diag)
-                    bulk_load(sb + kVpSide, mt + (static_cast<int64_t>(w.tj) * n_ck + chunk) * kTile8Bytes, bytes,
-                              &ctl->full[slot]);
+                for (int j = 0; j < n; ++j) {
+                    bulk_load(sb + j * kTile8Bytes, mi + (chunk + j) * kFxImageBytes, kTile8Bytes, &ctl->full[slot]);
+                    if (!diag)
+                        bulk_load(sb + kVpSide + j * kTile8Bytes, mj + (chunk + j) * kFxImageBytes, kTile8Bytes,
+                                  &ctl->full[slot]);
+                }
             }
         }
     }
@@ -551,12 +574,14 @@ __device__ void vp_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t t
         if (nch == 0) continue;
         const uint32_t id = idesc_for<kGrouped>(a, w, bi);
         const bool diag = w.ti == w.tj;
-        const int b = static_cast<int>(n_acc % kVpAcc);
-        if (!waitb(&ctl->acc_empty[b], ((n_acc / kVpAcc) & 1u) ^ 1u, ctl, a)) goto done;
-        tc_fence_after();
-        {
+        // One accumulator per part of at most kVpPartChunks chunks (the int32 bound).
+        for (int p0 = 0; p0 < nch; p0 += kVpPartChunks) {
+            const int p1 = min(nch, p0 + kVpPartChunks);
+            const int b = static_cast<int>(n_acc % kVpAcc);
+            if (!waitb(&ctl->acc_empty[b], ((n_acc / kVpAcc) & 1u) ^ 1u, ctl, a)) goto done;
+            tc_fence_after();
             const uint32_t d = tmem + static_cast<uint32_t>(b) * 128u;
-            for (int c0 = 0; c0 < nch; c0 += kVpChunks, ++g) {
+            for (int c0 = p0; c0 < p1; c0 += kVpChunks, ++g) {
                 const int slot = static_cast<int>(g % kVpStages);
                 if (!waitb(&ctl->full[slot], (g / kVpStages) & 1u, ctl, a)) goto done;
                 tc_fence_after();
@@ -565,12 +590,12 @@ __device__ void vp_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t t
                 const int n = min(kVpChunks, nch - c0);
                 for (int j = 0; j < n; ++j)
                     mma_i8(d, smem_desc(sa + static_cast<uint32_t>(j) * 4096u, 256, 6),
-                           smem_desc(sb + static_cast<uint32_t>(j) * 4096u, 256, 6), id, (c0 + j) > 0 ? 1u : 0u);
+                           smem_desc(sb + static_cast<uint32_t>(j) * 4096u, 256, 6), id, (c0 + j) > p0 ? 1u : 0u);
                 mma_commit(&ctl->empty[slot]);
             }
+            mma_commit(&ctl->acc_full[b]);
+            ++n_acc;
         }
-        mma_commit(&ctl->acc_full[b]);
-        ++n_acc;
     }
 done:
     mma_commit(&ctl->drain);
@@ -587,27 +612,36 @@ __device__ void vp_epilogue(const FxArgs& a, FxCtl* ctl, uint32_t tmem, int warp
         if (lane == 0) it = read_item(a, ctl, gi);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it < 0) return;
-        if (stages_of(a.blocks[a.items[it].blk].k, kStageK) == 0) continue;  // the f2 kernel writes zeros
-        const int b = static_cast<int>(n_acc % kVpAcc);
-        bool ok = true;
-        if (lane == 0) ok = waitb(&ctl->acc_full[b], (n_acc / kVpAcc) & 1u, ctl, a);
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (!ok) return;
-        tc_fence_after();
+        const int nch = stages_of(a.blocks[a.items[it].blk].k, kStageK);
+        if (nch == 0) continue;  // the f2 kernel writes zeros
         int32_t* dst = a.vpc + static_cast<int64_t>(it) * kVpTileInts + (h * kVpCols) * kTile + q * 32 + lane;
+        for (int p0 = 0; p0 < nch; p0 += kVpPartChunks) {
+            const int b = static_cast<int>(n_acc % kVpAcc);
+            bool ok = true;
+            if (lane == 0) ok = waitb(&ctl->acc_full[b], (n_acc / kVpAcc) & 1u, ctl, a);
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) return;
+            tc_fence_after();
 #pragma unroll
-        for (int half = 0; half < kVpCols / 32; ++half) {
-            uint32_t v[32];
-            tmem_ld32(tmem + lane_addr + static_cast<uint32_t>(b) * 128u + static_cast<uint32_t>(h * kVpCols + half * 32),
-                      v);
-            tmem_wait_ld();
+            for (int half = 0; half < kVpCols / 32; ++half) {
+                uint32_t v[32];
+                tmem_ld32(tmem + lane_addr + static_cast<uint32_t>(b) * 128u +
+                              static_cast<uint32_t>(h * kVpCols + half * 32),
+                          v);
+                tmem_wait_ld();
+                // M = 64 on both sides: each both-present SNP adds 4096.
 #pragma unroll
-            for (int c = 0; c < 32; ++c) dst[(half * 32 + c) * kTile] = static_cast<int32_t>(v[c]);
+                for (int c = 0; c < 32; ++c) {
+                    const int32_t cnt = static_cast<int32_t>(v[c]) >> 12;
+                    int32_t* o = dst + (half * 32 + c) * kTile;
+                    *o = p0 == 0 ? cnt : *o + cnt;
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&ctl->acc_empty[b]);
+            ++n_acc;
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&ctl->acc_empty[b]);
-        ++n_acc;
     }
 }
 
@@ -673,7 +707,6 @@ void launch_fx(Ctx& c, const FxLaunch& L, cudaStream_t s) {
     if (L.n_items <= 0) return;
     FxArgs a{};
     a.images = L.images;
-    a.mtiles = L.mtiles;
     a.n_ck = L.n_ck;
     a.items = L.items;
     a.n_items = L.n_items;

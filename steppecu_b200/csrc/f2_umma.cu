@@ -526,7 +526,6 @@ void launch_kernel(int chunk_stages, bool grouped, int grid, const UmmaArgs& a, 
 
 struct UmmaPlan {
     const uint8_t* images = nullptr;
-    const uint8_t* mtiles = nullptr;  // FX: the 0/1 m tiles of the vpair contraction
     int64_t n_ck = 0;
     DevBuf items, blocks, err, rcp, block_items, counter;
     DevBuf vpc;  // FX: compact vpair tiles, one per item of the largest launch
@@ -582,7 +581,6 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
     p->images = static_cast<const uint8_t*>(op.planes);
     p->n_ck = op.n_ck;
     if (op.fmt == OpFmt::FX) {
-        p->mtiles = op.mtiles;
         p->vpc.reserve(fx_vpc_bytes(p->n_items));
         fx_prepare();
     } else {
@@ -622,7 +620,6 @@ void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, 
     if (p->fmt == OpFmt::FX) {
         FxLaunch L;
         L.images = p->images;
-        L.mtiles = p->mtiles;
         L.n_ck = p->n_ck;
         L.items = items;
         L.n_items = n_items;
@@ -744,7 +741,6 @@ void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stage
         fx_prepare();
         FxLaunch L;
         L.images = info[ord[0]].images;
-        L.mtiles = info[ord[0]].mtiles;
         L.n_ck = info[ord[0]].n_ck;
         L.P = info[ord[0]].P;
         L.f2 = info[ord[0]].f2;

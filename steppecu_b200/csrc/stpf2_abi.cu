@@ -129,7 +129,7 @@ size_t operand_plane_bytes(OpFmt f, int P, int64_t ld) {
         return align256(2 * pl * 4) + align256(pl);
     }
     const size_t tiles = static_cast<size_t>((P + kTileRows - 1) / kTileRows) * static_cast<size_t>(ld / kTileK);
-    if (f == OpFmt::FX) return align256(tiles * (kFxImageBytes + kTile8Bytes));  // images, then the M tiles
+    if (f == OpFmt::FX) return align256(tiles * kFxImageBytes);
     return align256(tiles * kImageBytes);
 }
 
@@ -148,8 +148,6 @@ void bind_operand_planes(OperandPlanes& op, OpFmt f, int P, int64_t ld, void* ba
         op.n_rt = (P + kTileRows - 1) / kTileRows;
         op.n_ck = ld / kTileK;
         op.m_u8 = nullptr;  // the int8 M tiles live inside the operand images
-        op.mtiles = f == OpFmt::FX ? static_cast<uint8_t*>(base) + static_cast<size_t>(op.n_rt) * op.n_ck * kFxImageBytes
-                                   : nullptr;
     }
 }
 
@@ -1197,7 +1195,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
                 oo += p.out_bytes / 2;
             }
             specs[w].L = &p.L;
-            specs[w].info = GroupInfo{static_cast<const uint8_t*>(p.op.planes), f2, vp, p.op.n_ck, p.P, 0, p.op.mtiles};
+            specs[w].info = GroupInfo{static_cast<const uint8_t*>(p.op.planes), f2, vp, p.op.n_ck, p.P, 0};
             if (o.block_sizes) copy_block_sizes(p.L, o.block_sizes);
         }
         std::vector<unsigned long long> stamps;

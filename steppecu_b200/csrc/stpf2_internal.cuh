@@ -155,7 +155,6 @@ struct GroupInfo {
     int64_t n_ck;
     int32_t P;
     int32_t pad_;
-    const uint8_t* mtiles;  // FX: the request's separate M tiles
 };
 
 struct BlockLayout {
@@ -217,7 +216,6 @@ struct OperandPlanes {
     int64_t ld = 0;
     void* planes = nullptr;
     uint8_t* m_u8 = nullptr;  // FP32 form only: row-major int8 M
-    uint8_t* mtiles = nullptr;  // FX only: the 0/1 m tiles, (row tile, chunk) 4 KiB each
     double scale_inv = 1.0;  // numerator scale undo (F16 planes are pre-scaled)
     int n_rt = 0;            // tiled: row tiles of 128 populations
     int64_t n_ck = 0;        // tiled: column chunks of 32
@@ -243,11 +241,10 @@ constexpr int kF16PtShift = 7;  // F16: Pt scaled by 2^7, Ah by 2^14 (num by 2^1
 // int8 tiles [X0][X1][X2][X3][E3][E4][E5][E6][M] (128 rows x 32 bytes each, the 32-byte
 // swizzle of tile8_offset), where X0..X3 are the balanced base-256 digits of X =
 // round((q - 1/2) * kFxScale), least significant first, E3..E6 those of -A with A =
-// round((x^2 - h) * kFxAScale), and M = kFxM * [n > 0]. The images of all row tiles come
-// first; after them the 0/1 tiles of m = [n > 0] alone, (row tile, chunk) at mtiles +
-// (t * n_ck + c) * 4 KiB,
-// for the vpair contraction. kFxScale = 127 * 2^25 keeps |X| <= 127 * 2^24 (|x| <= 1/2) and
-// kFxAScale = kFxScale^2 / 2^31 keeps |A| < 2^31 (|a| <= 1/4).
+// round((x^2 - h) * kFxAScale), and M = kFxM * [n > 0] (the vpair contraction counts on
+// the M planes too: 64 * 64 per both-present SNP). kFxScale = 127 * 2^25 keeps
+// |X| <= 127 * 2^24 (|x| <= 1/2) and kFxAScale = kFxScale^2 / 2^31 keeps |A| < 2^31
+// (|a| <= 1/4).
 constexpr int kFxPlanes = 9;
 constexpr int64_t kFxImageBytes = kFxPlanes * kTile8Bytes;  // 36 KiB
 constexpr double kFxScale = 127.0 * 33554432.0;     // 127 * 2^25
@@ -379,7 +376,6 @@ void launch_copy_union_ploidy(Ctx& c, uint32_t* desc, const int32_t* umap, int64
 // items. vpc holds fx_vpc_bytes(n_items); counters two ints; groups non-null for a batch.
 struct FxLaunch {
     const uint8_t* images = nullptr;
-    const uint8_t* mtiles = nullptr;
     int64_t n_ck = 0;
     const WorkItem* items = nullptr;
     int n_items = 0;
