@@ -329,6 +329,14 @@ stp_status stp_last_batch_times(stp_ctx* ctx, double* ms, int32_t n);
  * off. Per context. */
 stp_status stp_set_wait_bounds(stp_ctx* ctx, uint64_t timeout_ns, int64_t withhold_stage);
 
+/* Tile classes of the fixed-point contraction (the per-size-class choices of
+ * cuda_backend_f2_blocks.cu:55-74, made per work item here): bit k of partial_feed_mask set
+ * makes an operand tile side with 8k+1 .. 8k+8 valid populations (of 128 rows) stage only its
+ * valid 8-row groups per plane (nine copies) instead of the whole 36 KiB side (two copies).
+ * Results do not depend on it. The default is the measured table that
+ * steppecu_b200/autotune.py writes (steppecu_b200/tile_classes.json). Per context. */
+stp_status stp_set_tile_classes(stp_ctx* ctx, uint32_t partial_feed_mask);
+
 /* Block jackknife over per-block values (cpu_backend.cpp:2674-2720, :2273-2306), FP64 on
  * the device: x[k + m*b] with m = P*P -> est[m], var[m]. Host pointers. */
 stp_status stp_f2_jackknife(stp_ctx* ctx, const double* x, const int32_t* block_sizes, int64_t m,

@@ -116,6 +116,7 @@ SIGNATURES = {
     "stp_destroy": (None, [_P]),
     "stp_launch_count": (C.c_uint64, [_P]),
     "stp_set_wait_bounds": (C.c_int, [_P, C.c_uint64, C.c_int64]),
+    "stp_set_tile_classes": (C.c_int, [_P, C.c_uint32]),
     "stp_detect_ploidy": (C.c_int, [_P, C.POINTER(GenoView), _P, C.c_int64, _P]),
     "stp_detect_ploidy_tile": (C.c_int, [_P, _P, C.c_uint64, C.c_int64, C.c_int64, C.c_int32, _P]),
     "stp_decode_counts": (C.c_int, [_P, C.POINTER(GenoView), _P, _P, C.c_int32, _P, C.c_int32, _P, _P]),

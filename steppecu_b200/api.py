@@ -91,6 +91,11 @@ class Context:
         if not self._h:
             raise L.StpError(st.value, L.lib().stp_last_error().decode())
         self.device = device
+        from steppecu_b200.autotune import load_mask
+
+        mask = load_mask()  # the measured tile-class table, when one is committed
+        if mask is not None:
+            self.set_tile_classes(mask)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -117,6 +122,11 @@ class Context:
         """stp_set_wait_bounds: the device-side wait bound of the fixed-point contraction
         (0 = default) and its test hook (withhold_stage >= 0 starves the MMA issuer)."""
         L.check(L.lib().stp_set_wait_bounds(self._h, int(timeout_ns), int(withhold_stage)))
+
+    def set_tile_classes(self, partial_feed_mask: int) -> None:
+        """stp_set_tile_classes: bit k makes a tile side of 8k+1 .. 8k+8 valid populations stage
+        only its valid rows (steppecu_b200/autotune.py measures the choice)."""
+        L.check(L.lib().stp_set_tile_classes(self._h, int(partial_feed_mask) & 0xFFFF))
 
     # -- genotype views ---------------------------------------------------------------
     @staticmethod

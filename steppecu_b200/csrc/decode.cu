@@ -258,7 +258,7 @@ __device__ __forceinline__ void emit8_fx(const OperandPlanes& op, int i, int64_t
         if (c < 4) mv.x |= b << (8 * c);
         else mv.y |= b << (8 * (c - 4));
     }
-    *reinterpret_cast<uint2*>(img + 8 * kTile8Bytes) = mv;
+    *reinterpret_cast<uint2*>(op.mplanes + tile * kTile8Bytes + tile8_offset(r, k)) = mv;
 }
 
 // One element (the Q/V/N feeder): q, n as FP64.
@@ -278,7 +278,7 @@ __device__ __forceinline__ void emit_fx(const OperandPlanes& op, int i, int64_t 
         img[(4 + d) * kTile8Bytes] = static_cast<uint8_t>(dn >> (8 * d));
     }
     const uint8_t m = valid ? uint8_t(kFxM) : uint8_t(0);
-    img[8 * kTile8Bytes] = m;
+    op.mplanes[tile * kTile8Bytes + tile8_offset(r, k)] = m;
 }
 
 // ---- canonical genotypes -------------------------------------------------------------------

@@ -27,14 +27,14 @@
 // 7e-10 on T; a block mean over K SNPs averages independent roundings (~1e-10 / sqrt(K)).
 //
 // vpair_fx_kernel runs first over the same items: the exact both-present counts
-// m_i . m_j (one kind::i8 MMA per 32 SNPs on the images' M planes, 64 m on both sides, so
-// 4096 per SNP; 128 SNPs per stage, a ring of four TMEM accumulators, at most 524,160
+// m_i . m_j (one kind::i8 MMA per 32 SNPs on the M tiles, 64 m on both sides, so 4096 per
+// SNP; 128 SNPs per stage, a ring of four TMEM accumulators, at most 524,160
 // SNPs per accumulation) written as one compact int32 128x128 tile per item, which the f2
 // epilogue reads for its divide and its vpair stores. (The four f2
 // accumulators fill TMEM's 512 columns, so the counts cannot share the f2 kernel.)
 //
-//   f2_fx_kernel:   warp 0 producer (one 36 KiB bulk copy per stage side, no tensor maps, no
-//                   multicast), warp 1 TMEM owner + single-thread MMA issuer, warps 2-17
+//   f2_fx_kernel:   warp 0 producer (a 32 KiB image and a 4 KiB M copy per stage side, no
+//                   tensor maps, no multicast), warp 1 TMEM owner + single-thread MMA issuer, warps 2-17
 //                   epilogue (four per TMEM lane quarter, 32 tile columns each).
 //   vpair_fx_kernel: warp 0 producer (16 KiB per stage side), warp 1 issuer, warps 2-9
 //                   epilogue (two per lane quarter, 64 columns each).
@@ -60,7 +60,7 @@ constexpr int kVpTileInts = kTile * kTile;  // one compact vpair tile: (row r, c
 
 // ---- f2 kernel constants ----
 constexpr int kStages = 3;
-constexpr uint32_t kSide = static_cast<uint32_t>(kFxImageBytes);  // 36 KiB
+constexpr uint32_t kSide = static_cast<uint32_t>(kFxPlanes * kTile8Bytes);  // 36 KiB: image and M
 constexpr uint32_t kStageBytes = 2 * kSide;
 constexpr int kEpiWarps = 16;
 constexpr int kEpiWarp0 = 2;
@@ -85,7 +85,8 @@ constexpr int kVpPartChunks = 16380;
 static_assert(4096ll * 32 * kVpPartChunks < (1ll << 31) && kVpPartChunks % kVpChunks == 0, "vpair part");
 
 struct FxArgs {
-    const uint8_t* images;  // (row tile t, chunk c) image at (t * n_ck + c) * kFxImageBytes
+    const uint8_t* images;   // (row tile t, chunk c) image at (t * n_ck + c) * kFxImageBytes
+    const uint8_t* mplanes;  // (row tile t, chunk c) M tile at (t * n_ck + c) * 4 KiB
     int64_t n_ck;
     const WorkItem* items;
     int n_items;
@@ -102,6 +103,7 @@ struct FxArgs {
     uint32_t idesc;
     unsigned long long timeout_ns;
     long long withhold;  // test hook: the producer stops before its stage of this index (-1: never)
+    uint32_t partial_feed;  // bit k: a side with 8k+1 .. 8k+8 valid rows copies those rows only
     const GroupInfo* groups;  // grouped launch: per-request images / outputs (null for one request)
     int* grp_done;
     unsigned long long* grp_ns;
@@ -167,6 +169,33 @@ __device__ __forceinline__ void init_ring(FxCtl* ctl, int consumers) {
 
 // ============================== f2 kernel ================================================
 
+// 8-row groups a stage copies of an operand side with `rows` valid populations: all 16
+// (the whole tile in one copy per region), or only the groups holding valid rows when the
+// side's row class is marked for partial copies. Rows past the valid ones are never read
+// into a stored result: A rows past them make accumulator rows past P, B rows make columns
+// past P, and the epilogue stores neither, so whatever the stage slot held there is harmless.
+__device__ __forceinline__ uint32_t feed_groups(const FxArgs& a, int rows) {
+    const int cls = (rows + 7) / 8 - 1;  // 0..15
+    return ((a.partial_feed >> cls) & 1u) ? static_cast<uint32_t>(cls + 1) : 16u;
+}
+
+// One stage side: image planes 0..7 and the M tile (plane 8), `g` 8-row groups of each.
+__device__ __forceinline__ uint32_t side_bytes(uint32_t g) { return g == 16 ? kSide : 9u * g * 256u; }
+
+__device__ __forceinline__ void copy_side(uint8_t* dst, const uint8_t* img, const uint8_t* mt, uint32_t g,
+                                          unsigned long long* bar) {
+    constexpr uint32_t kImg = static_cast<uint32_t>(kFxImageBytes), kM = static_cast<uint32_t>(kTile8Bytes);
+    if (g == 16) {
+        bulk_load(dst, img, kImg, bar);      // planes 0..7
+        bulk_load(dst + kImg, mt, kM, bar);  // plane 8
+        return;
+    }
+    const uint32_t b = g * 256u;
+#pragma unroll 1
+    for (int pl = 0; pl < 8; ++pl) bulk_load(dst + pl * kM, img + pl * kM, b, bar);
+    bulk_load(dst + kImg, mt, b, bar);
+}
+
 template <bool kGrouped>
 __device__ void fx_producer(const FxArgs& a, uint8_t* smem, FxCtl* ctl) {
     uint32_t g = 0;
@@ -181,22 +210,29 @@ __device__ void fx_producer(const FxArgs& a, uint8_t* smem, FxCtl* ctl) {
             const int nst = stages_of(bi.k, kStageK);
             const bool diag = w.ti == w.tj;
             const uint8_t* images = a.images;
+            const uint8_t* mplanes = a.mplanes;
             int64_t n_ck = a.n_ck;
             if constexpr (kGrouped) {
                 images = a.groups[bi.grp].images;
+                mplanes = a.groups[bi.grp].mplanes;
                 n_ck = a.groups[bi.grp].n_ck;
             }
+            const int P = kGrouped ? a.groups[bi.grp].P : a.P;
+            const uint32_t gA = feed_groups(a, min(kTile, P - w.ti * kTile));
+            const uint32_t gB = feed_groups(a, min(kTile, P - w.tj * kTile));
+            const uint32_t bytes = diag ? side_bytes(gA) : side_bytes(gA) + side_bytes(gB);
             for (int st = 0; st < nst; ++st, ++g) {
                 if (static_cast<long long>(g) == a.withhold) return;  // test hook: stop feeding
                 const int slot = static_cast<int>(g % kStages);
                 if (!waitb(&ctl->empty[slot], ((g / kStages) & 1u) ^ 1u, ctl, a)) goto abort;
                 uint8_t* sb = smem + slot * kStageBytes;
-                mbar_expect_tx(&ctl->full[slot], diag ? kSide : kStageBytes);
-                const int64_t chunk = bi.col / kStageK + st;
-                bulk_load(sb, images + (static_cast<int64_t>(w.ti) * n_ck + chunk) * kSide, kSide, &ctl->full[slot]);
-                if (!diag)
-                    bulk_load(sb + kSide, images + (static_cast<int64_t>(w.tj) * n_ck + chunk) * kSide, kSide,
-                              &ctl->full[slot]);
+                mbar_expect_tx(&ctl->full[slot], bytes);
+                const int64_t ci = static_cast<int64_t>(w.ti) * n_ck + bi.col / kStageK + st;
+                copy_side(sb, images + ci * kFxImageBytes, mplanes + ci * kTile8Bytes, gA, &ctl->full[slot]);
+                if (!diag) {
+                    const int64_t cj = static_cast<int64_t>(w.tj) * n_ck + bi.col / kStageK + st;
+                    copy_side(sb + kSide, images + cj * kFxImageBytes, mplanes + cj * kTile8Bytes, gB, &ctl->full[slot]);
+                }
             }
         }
     }
@@ -530,28 +566,36 @@ __device__ void vp_producer(const FxArgs& a, uint8_t* smem, FxCtl* ctl) {
             const BlockInfo bi = a.blocks[w.blk];
             const int nch = stages_of(bi.k, kStageK);
             const bool diag = w.ti == w.tj;
-            const uint8_t* images = a.images;
+            const uint8_t* mt = a.mplanes;
             int64_t n_ck = a.n_ck;
             if constexpr (kGrouped) {
-                images = a.groups[bi.grp].images;
+                mt = a.groups[bi.grp].mplanes;
                 n_ck = a.groups[bi.grp].n_ck;
             }
-            // The M tile (plane 8) of each 32-SNP image: one 4 KiB copy per chunk and side.
-            const uint8_t* mi = images + static_cast<int64_t>(w.ti) * n_ck * kFxImageBytes + 8 * kTile8Bytes;
-            const uint8_t* mj = images + static_cast<int64_t>(w.tj) * n_ck * kFxImageBytes + 8 * kTile8Bytes;
+            // The M tiles of up to four consecutive chunks: one copy per side, or per chunk the
+            // valid 8-row groups of a partial side (feed_groups).
+            const int P = kGrouped ? a.groups[bi.grp].P : a.P;
+            const uint32_t gA = feed_groups(a, min(kTile, P - w.ti * kTile));
+            const uint32_t gB = feed_groups(a, min(kTile, P - w.tj * kTile));
             for (int c0 = 0; c0 < nch; c0 += kVpChunks, ++g) {
                 const int n = min(kVpChunks, nch - c0);
-                const uint32_t bytes = static_cast<uint32_t>(n) * static_cast<uint32_t>(kTile8Bytes);
                 const int slot = static_cast<int>(g % kVpStages);
                 if (!waitb(&ctl->empty[slot], ((g / kVpStages) & 1u) ^ 1u, ctl, a)) goto abort;
                 uint8_t* sb = smem + slot * kVpStageBytes;
-                mbar_expect_tx(&ctl->full[slot], diag ? bytes : 2 * bytes);
+                const uint32_t bA = static_cast<uint32_t>(n) * (gA == 16 ? 4096u : gA * 256u);
+                const uint32_t bB = static_cast<uint32_t>(n) * (gB == 16 ? 4096u : gB * 256u);
+                mbar_expect_tx(&ctl->full[slot], diag ? bA : bA + bB);
                 const int64_t chunk = bi.col / kStageK + c0;
-                for (int j = 0; j < n; ++j) {
-                    bulk_load(sb + j * kTile8Bytes, mi + (chunk + j) * kFxImageBytes, kTile8Bytes, &ctl->full[slot]);
-                    if (!diag)
-                        bulk_load(sb + kVpSide + j * kTile8Bytes, mj + (chunk + j) * kFxImageBytes, kTile8Bytes,
-                                  &ctl->full[slot]);
+                const uint8_t* si = mt + (static_cast<int64_t>(w.ti) * n_ck + chunk) * kTile8Bytes;
+                const uint8_t* sj = mt + (static_cast<int64_t>(w.tj) * n_ck + chunk) * kTile8Bytes;
+                if (gA == 16) bulk_load(sb, si, bA, &ctl->full[slot]);
+                else
+                    for (int j = 0; j < n; ++j) bulk_load(sb + j * 4096, si + j * 4096, gA * 256u, &ctl->full[slot]);
+                if (!diag) {
+                    if (gB == 16) bulk_load(sb + kVpSide, sj, bB, &ctl->full[slot]);
+                    else
+                        for (int j = 0; j < n; ++j)
+                            bulk_load(sb + kVpSide + j * 4096, sj + j * 4096, gB * 256u, &ctl->full[slot]);
                 }
             }
         }
@@ -707,6 +751,7 @@ void launch_fx(Ctx& c, const FxLaunch& L, cudaStream_t s) {
     if (L.n_items <= 0) return;
     FxArgs a{};
     a.images = L.images;
+    a.mplanes = L.mplanes;
     a.n_ck = L.n_ck;
     a.items = L.items;
     a.n_items = L.n_items;
@@ -722,6 +767,7 @@ void launch_fx(Ctx& c, const FxLaunch& L, cudaStream_t s) {
     a.idesc = idesc_s8_s32();
     a.timeout_ns = c.fx_tuning.timeout_ns;
     a.withhold = -1;
+    a.partial_feed = c.fx_tuning.partial_feed;
     a.groups = L.groups;
     a.grp_done = L.grp_done;
     a.grp_ns = L.grp_ns;

@@ -526,6 +526,7 @@ void launch_kernel(int chunk_stages, bool grouped, int grid, const UmmaArgs& a, 
 
 struct UmmaPlan {
     const uint8_t* images = nullptr;
+    const uint8_t* mplanes = nullptr;  // FX: the M tiles
     int64_t n_ck = 0;
     DevBuf items, blocks, err, rcp, block_items, counter;
     DevBuf vpc;  // FX: compact vpair tiles, one per item of the largest launch
@@ -581,6 +582,7 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
     p->images = static_cast<const uint8_t*>(op.planes);
     p->n_ck = op.n_ck;
     if (op.fmt == OpFmt::FX) {
+        p->mplanes = op.mplanes;
         p->vpc.reserve(fx_vpc_bytes(p->n_items));
         fx_prepare();
     } else {
@@ -620,6 +622,7 @@ void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, 
     if (p->fmt == OpFmt::FX) {
         FxLaunch L;
         L.images = p->images;
+        L.mplanes = p->mplanes;
         L.n_ck = p->n_ck;
         L.items = items;
         L.n_items = n_items;
@@ -741,6 +744,7 @@ void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stage
         fx_prepare();
         FxLaunch L;
         L.images = info[ord[0]].images;
+        L.mplanes = info[ord[0]].mplanes;
         L.n_ck = info[ord[0]].n_ck;
         L.P = info[ord[0]].P;
         L.f2 = info[ord[0]].f2;

@@ -129,7 +129,7 @@ size_t operand_plane_bytes(OpFmt f, int P, int64_t ld) {
         return align256(2 * pl * 4) + align256(pl);
     }
     const size_t tiles = static_cast<size_t>((P + kTileRows - 1) / kTileRows) * static_cast<size_t>(ld / kTileK);
-    if (f == OpFmt::FX) return align256(tiles * kFxImageBytes);
+    if (f == OpFmt::FX) return align256(tiles * (kFxImageBytes + kTile8Bytes));  // images, then the M tiles
     return align256(tiles * kImageBytes);
 }
 
@@ -147,7 +147,9 @@ void bind_operand_planes(OperandPlanes& op, OpFmt f, int P, int64_t ld, void* ba
     } else {
         op.n_rt = (P + kTileRows - 1) / kTileRows;
         op.n_ck = ld / kTileK;
-        op.m_u8 = nullptr;  // the int8 M tiles live inside the operand images
+        op.m_u8 = nullptr;  // the int8 M tiles live inside the operand images (FX: after them)
+        op.mplanes = f == OpFmt::FX ? static_cast<uint8_t*>(base) + static_cast<size_t>(op.n_rt) * op.n_ck * kFxImageBytes
+                                    : nullptr;
     }
 }
 
@@ -1195,7 +1197,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
                 oo += p.out_bytes / 2;
             }
             specs[w].L = &p.L;
-            specs[w].info = GroupInfo{static_cast<const uint8_t*>(p.op.planes), f2, vp, p.op.n_ck, p.P, 0};
+            specs[w].info = GroupInfo{static_cast<const uint8_t*>(p.op.planes), f2, vp, p.op.n_ck, p.P, 0, p.op.mplanes};
             if (o.block_sizes) copy_block_sizes(p.L, o.block_sizes);
         }
         std::vector<unsigned long long> stamps;
@@ -1959,6 +1961,13 @@ stp_status stp_set_wait_bounds(stp_ctx* ctx, uint64_t timeout_ns, int64_t withho
         need(withhold_stage >= -1, "withhold_stage must be -1 or a stage index");
         ctx->fx_tuning.timeout_ns = timeout_ns ? timeout_ns : FxTuning{}.timeout_ns;
         ctx->fx_tuning.withhold_stage = withhold_stage;
+    });
+}
+
+stp_status stp_set_tile_classes(stp_ctx* ctx, uint32_t partial_feed_mask) {
+    return guarded([&] {
+        need(ctx != nullptr, "null context");
+        ctx->fx_tuning.partial_feed = partial_feed_mask & 0xFFFFu;
     });
 }
 

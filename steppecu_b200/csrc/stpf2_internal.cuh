@@ -99,9 +99,15 @@ struct Packing {
 // Bounded-wait settings of the fixed-point contraction. timeout_ns bounds every device-side
 // wait; withhold_stage >= 0 makes the f2 kernel's producer stop before that stage (a test
 // hook: the issuer's wait then runs out and the call reports STP_DEVICE_TIMEOUT).
+// Row classes of an operand tile side: class k holds 8k+1 .. 8k+8 valid populations (of
+// the tile's 128 rows). kDefaultPartialFeed: the classes whose stage copies carry only
+// their valid 8-row groups (the measured choice, steppecu_b200/tile_classes.json).
+constexpr uint32_t kDefaultPartialFeed = 0xBFFFu;  // measured on B200: all but 113-120 rows
+
 struct FxTuning {
     unsigned long long timeout_ns = 4000000000ull;
     long long withhold_stage = -1;
+    uint32_t partial_feed = kDefaultPartialFeed;  // bit k: row class k copies valid rows only
 };
 
 struct Ctx {
@@ -155,6 +161,7 @@ struct GroupInfo {
     int64_t n_ck;
     int32_t P;
     int32_t pad_;
+    const uint8_t* mplanes;  // FX: the request's M tiles
 };
 
 struct BlockLayout {
@@ -216,6 +223,7 @@ struct OperandPlanes {
     int64_t ld = 0;
     void* planes = nullptr;
     uint8_t* m_u8 = nullptr;  // FP32 form only: row-major int8 M
+    uint8_t* mplanes = nullptr;  // FX only: the M tiles, (row tile, chunk) 4 KiB each
     double scale_inv = 1.0;  // numerator scale undo (F16 planes are pre-scaled)
     int n_rt = 0;            // tiled: row tiles of 128 populations
     int64_t n_ck = 0;        // tiled: column chunks of 32
@@ -237,16 +245,18 @@ __host__ __device__ inline uint32_t tile8_offset(int r, int k) {
 
 constexpr int kF16PtShift = 7;  // F16: Pt scaled by 2^7, Ah by 2^14 (num by 2^14)
 
-// FX (fixed point, exact integer accumulation): one image per (row tile, chunk) of nine
-// int8 tiles [X0][X1][X2][X3][E3][E4][E5][E6][M] (128 rows x 32 bytes each, the 32-byte
+// FX (fixed point, exact integer accumulation): one image per (row tile, chunk) of eight
+// int8 tiles [X0][X1][X2][X3][E3][E4][E5][E6] (128 rows x 32 bytes each, the 32-byte
 // swizzle of tile8_offset), where X0..X3 are the balanced base-256 digits of X =
-// round((q - 1/2) * kFxScale), least significant first, E3..E6 those of -A with A =
-// round((x^2 - h) * kFxAScale), and M = kFxM * [n > 0] (the vpair contraction counts on
-// the M planes too: 64 * 64 per both-present SNP). kFxScale = 127 * 2^25 keeps
-// |X| <= 127 * 2^24 (|x| <= 1/2) and kFxAScale = kFxScale^2 / 2^31 keeps |A| < 2^31
-// (|a| <= 1/4).
-constexpr int kFxPlanes = 9;
-constexpr int64_t kFxImageBytes = kFxPlanes * kTile8Bytes;  // 36 KiB
+// round((q - 1/2) * kFxScale), least significant first, and E3..E6 those of -A with A =
+// round((x^2 - h) * kFxAScale); the images of all row tiles first, then one M tile per
+// (row tile, chunk), M = kFxM * [n > 0], at mplanes + (t * n_ck + c) * 4 KiB (the f2
+// contraction stages it as a ninth plane after the image; the vpair contraction reads the
+// M tiles of consecutive chunks in one copy and counts 64 * 64 per both-present SNP).
+// kFxScale = 127 * 2^25 keeps |X| <= 127 * 2^24 (|x| <= 1/2) and kFxAScale = kFxScale^2 /
+// 2^31 keeps |A| < 2^31 (|a| <= 1/4).
+constexpr int kFxPlanes = 9;                                      // staged: the image and M
+constexpr int64_t kFxImageBytes = (kFxPlanes - 1) * kTile8Bytes;  // 32 KiB in memory
 constexpr double kFxScale = 127.0 * 33554432.0;     // 127 * 2^25
 constexpr double kFxAScale = 16129.0 * 524288.0;    // kFxScale^2 / 2^31 = 127^2 * 2^19
 constexpr double kFxRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
@@ -376,6 +386,7 @@ void launch_copy_union_ploidy(Ctx& c, uint32_t* desc, const int32_t* umap, int64
 // items. vpc holds fx_vpc_bytes(n_items); counters two ints; groups non-null for a batch.
 struct FxLaunch {
     const uint8_t* images = nullptr;
+    const uint8_t* mplanes = nullptr;
     int64_t n_ck = 0;
     const WorkItem* items = nullptr;
     int n_items = 0;

@@ -127,3 +127,20 @@ def test_fixed_i8_wait_timeout_reports_and_context_recovers():
             got = c.extract_blocks(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision="fixed_i8",
                                    sample_ploidy=pl)
             _check(got, want)
+
+
+@pytest.mark.parametrize("P", [41, 150, 250])
+def test_tile_classes_do_not_change_results(ctx, P):
+    """The partial-feed tile classes (stp_set_tile_classes) only change which rows a stage
+    copies: every class mask gives the same f2 and vpair, bit for bit."""
+    p = synth.generate("c4", seed=300 + P, n_snp=20_000, n_pop=P)
+    sel, po = p.selection()
+    rec = p.records_numpy()
+    outs = []
+    for mask in (0, 0xFFFF, 0x5555):
+        ctx.set_tile_classes(mask)
+        t = ctx.extract_blocks(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision="fixed_i8")
+        outs.append(t)
+    ctx.set_tile_classes(0x7FFF)
+    for t in outs[1:]:
+        assert np.array_equal(t.f2, outs[0].f2) and np.array_equal(t.vpair, outs[0].vpair)
