@@ -28,7 +28,7 @@
 //
 // vpair_fx_kernel runs first over the same items: the exact both-present counts
 // m_i . m_j (one kind::i8 MMA per 32 SNPs on the M tiles, 64 m on both sides, so 4096 per
-// SNP; 128 SNPs per stage, a ring of four TMEM accumulators, at most 524,160
+// SNP; 256 SNPs per stage, a ring of four TMEM accumulators, at most 524,032
 // SNPs per accumulation) written as one compact int32 128x128 tile per item, which the f2
 // epilogue reads for its divide and its vpair stores. (The four f2
 // accumulators fill TMEM's 512 columns, so the counts cannot share the f2 kernel.)
@@ -36,7 +36,7 @@
 //   f2_fx_kernel:   warp 0 producer (a 32 KiB image and a 4 KiB M copy per stage side, no
 //                   tensor maps, no multicast), warp 1 TMEM owner + single-thread MMA issuer, warps 2-17
 //                   epilogue (four per TMEM lane quarter, 32 tile columns each).
-//   vpair_fx_kernel: warp 0 producer (16 KiB per stage side), warp 1 issuer, warps 2-9
+//   vpair_fx_kernel: warp 0 producer (32 KiB per stage side), warp 1 issuer, warps 2-9
 //                   epilogue (two per lane quarter, 64 columns each).
 // Every wait is bounded (FxTuning::timeout_ns); on expiry the kernel raises an error flag
 // the host turns into STP_DEVICE_TIMEOUT, lets its copies and MMAs finish, frees TMEM and
@@ -71,17 +71,17 @@ constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kCtlBytes = 256;
 
 // ---- vpair kernel constants ----
-constexpr int kVpChunks = 4;  // 32-SNP chunks per stage
-constexpr uint32_t kVpSide = kVpChunks * static_cast<uint32_t>(kTile8Bytes);  // 16 KiB
+constexpr int kVpChunks = 8;  // 32-SNP chunks per stage
+constexpr uint32_t kVpSide = kVpChunks * static_cast<uint32_t>(kTile8Bytes);  // 32 KiB
 constexpr uint32_t kVpStageBytes = 2 * kVpSide;
-constexpr int kVpStages = 4;
+constexpr int kVpStages = 3;
 constexpr int kVpAcc = 4;  // TMEM ring of 128-column accumulators
 constexpr int kVpEpiWarps = 8;
 constexpr int kVpThreads = 32 * (2 + kVpEpiWarps);  // 320
 constexpr int kVpCols = 4 * kTile / kVpEpiWarps;   // 64
 // 32-SNP chunks per accumulation: M = 64 on both sides adds 4096 per both-present SNP, so
-// an int32 accumulator holds 524,160 SNPs (a multiple of the stage's four chunks).
-constexpr int kVpPartChunks = 16380;
+// an int32 accumulator holds 524,032 SNPs (a multiple of the stage's eight chunks).
+constexpr int kVpPartChunks = 16376;
 static_assert(4096ll * 32 * kVpPartChunks < (1ll << 31) && kVpPartChunks % kVpChunks == 0, "vpair part");
 
 struct FxArgs {
@@ -572,7 +572,7 @@ __device__ void vp_producer(const FxArgs& a, uint8_t* smem, FxCtl* ctl) {
                 mt = a.groups[bi.grp].mplanes;
                 n_ck = a.groups[bi.grp].n_ck;
             }
-            // The M tiles of up to four consecutive chunks: one copy per side, or per chunk the
+            // The M tiles of up to eight consecutive chunks: one copy per side, or per chunk the
             // valid 8-row groups of a partial side (feed_groups).
             const int P = kGrouped ? a.groups[bi.grp].P : a.P;
             const uint32_t gA = feed_groups(a, min(kTile, P - w.ti * kTile));

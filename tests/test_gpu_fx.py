@@ -107,6 +107,21 @@ def test_fixed_i8_long_blocks_span_accumulator_segments(ctx, out_on_device):
     _check(got, want)
 
 
+def test_fixed_i8_block_longer_than_one_count_accumulation(ctx):
+    """A block of 530,000 SNPs: the vpair kernel's int32 accumulator holds 524,032 SNPs of
+    64 x 64 products, so the block's counts come from two accumulations (and its f2 from 33
+    segments of 16,384 SNPs); a short block follows."""
+    p = synth.generate("c1", seed=21, n_snp=531_000, n_pop=9)
+    sel, po = p.selection()
+    rec = p.records_numpy()
+    bid = (np.arange(p.n_snp) >= 530_000).astype(np.int32)
+    pl = oracle.detect_ploidy_pa(rec, sel)
+    want = _oracle(rec, sel, po, bid, 2, pl)
+    got = ctx.extract_blocks(rec, p.n_ind, sel, po, bid, 2, precision="fixed_i8", sample_ploidy=pl)
+    assert want.vpair.max() > 524_032
+    _check(got, want)
+
+
 def test_fixed_i8_wait_timeout_reports_and_context_recovers():
     """A wait that runs out (the hook stops the f2 kernel's feed) ends the call with
     STP_DEVICE_TIMEOUT; the kernel frees its tensor memory and exits, and the same context
