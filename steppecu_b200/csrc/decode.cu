@@ -911,7 +911,7 @@ emit_counts_kernel(const uint32_t* __restrict__ counts, int64_t cnt_ld, const in
         for (int c = 0; c < 8; ++c) {
             const int32_t s = __ldg(col_snp + col0 + c);
             v[c] = s >= 0 ? __ldg(row + s) : 0u;
-            cen[c] = s >= 0 ? __ldg(center_snp + s) : 0.5;
+            if constexpr (F != OpFmt::FX) cen[c] = s >= 0 ? __ldg(center_snp + s) : 0.5;  // the fixed point needs none
         }
         if constexpr (F == OpFmt::FX)
             emit8_fx(op, i, col0, fx_terms8_from_counts(v, rec_n, rec_nm1));

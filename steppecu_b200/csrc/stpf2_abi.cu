@@ -491,6 +491,42 @@ void parallel_for(int n, F&& f) {
         if (e) std::rethrow_exception(e);
 }
 
+// Fork of independent launches from stream s onto the context's side streams, round robin,
+// and their join back into s (events; destruction joins too, so an error path leaves no
+// side-stream work unordered after s).
+struct SideFork {
+    Ctx& c;
+    cudaStream_t s;
+    cudaEvent_t ev[Ctx::kSideStreams + 1] = {};
+    int k = 0;
+    bool joined = false;
+    SideFork(Ctx& c_, cudaStream_t s_) : c(c_), s(s_) {
+        for (auto& e : ev) STPF2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        STPF2_CUDA(cudaEventRecord(ev[0], s));
+        for (cudaStream_t x : c.side) STPF2_CUDA(cudaStreamWaitEvent(x, ev[0], 0));
+    }
+    cudaStream_t next() { return c.side[k++ % Ctx::kSideStreams]; }
+    void join() {
+        if (joined) return;
+        joined = true;
+        for (int i = 0; i < Ctx::kSideStreams; ++i) {
+            STPF2_CUDA(cudaEventRecord(ev[i + 1], c.side[i]));
+            STPF2_CUDA(cudaStreamWaitEvent(s, ev[i + 1], 0));
+        }
+    }
+    ~SideFork() {
+        if (!joined) {
+            joined = true;
+            for (int i = 0; i < Ctx::kSideStreams; ++i) {
+                cudaEventRecord(ev[i + 1], c.side[i]);
+                cudaStreamWaitEvent(s, ev[i + 1], 0);
+            }
+        }
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
 // On an error, copies between the device and the caller's buffers may still be in flight:
 // drains the context's streams before the error reaches the caller (who may free them).
 struct DrainOnError {
@@ -1181,6 +1217,10 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
         }
         std::vector<GroupSpec> specs(wave.size());
         size_t io = 0, oo = 0;
+        // The emissions are independent (each writes its own request's images): they run on
+        // the side streams, round robin, so one launch's tail overlaps the next; the
+        // contraction waits for all of them.
+        SideFork fork(c, s);
         for (size_t w = 0; w < wave.size(); ++w) {
             BatchMember& p = mem[wave[w]];
             const MemberOffsets& q = mo[wave[w]];
@@ -1188,7 +1228,8 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
             bind_operand_planes(p.op, fmt, p.P, p.L.ld, c.ws_batch.as<uint8_t>() + io);
             io += p.img_bytes;
             launch_emit_counts(c, d_counts, M, reinterpret_cast<const int32_t*>(T + q.upop), p.P, p.L.ld / kTileK,
-                               reinterpret_cast<const int32_t*>(T + q.cols), d_center_u, d_rn, d_rnm1, p.op, s);
+                               reinterpret_cast<const int32_t*>(T + q.cols), d_center_u, d_rn, d_rnm1, p.op,
+                               fork.next());
             double* f2 = o.f2;
             double* vp = o.vpair;
             if (!o.on_device) {
@@ -1200,6 +1241,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
             specs[w].info = GroupInfo{static_cast<const uint8_t*>(p.op.planes), f2, vp, p.op.n_ck, p.P, 0, p.op.mplanes};
             if (o.block_sizes) copy_block_sizes(p.L, o.block_sizes);
         }
+        fork.join();
         std::vector<unsigned long long> stamps;
         launch_f2_umma_grouped(c, fmt, mem[wave[0]].op.scale_inv, chunk_stages_of(prec), specs, s, &stamps);
         if (t0 == 0) STPF2_CUDA(cudaMemcpy(&t0, d_t0, sizeof(t0), cudaMemcpyDeviceToHost));
@@ -1264,6 +1306,7 @@ stp_ctx* stp_create(int device, stp_status* status) {
         STPF2_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         STPF2_CUDA(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
         STPF2_CUDA(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+        for (auto& x : c->side) STPF2_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
         out = c.release();
     });
     if (status) *status = st;
@@ -1273,7 +1316,7 @@ stp_ctx* stp_create(int device, stp_status* status) {
 void stp_destroy(stp_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    for (cudaStream_t s : {ctx->stream, ctx->h2d, ctx->d2h}) {
+    for (cudaStream_t s : {ctx->stream, ctx->h2d, ctx->d2h, ctx->side[0], ctx->side[1], ctx->side[2], ctx->side[3]}) {
         if (s) {
             cudaStreamSynchronize(s);
             cudaStreamDestroy(s);

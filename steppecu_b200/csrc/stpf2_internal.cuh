@@ -117,6 +117,8 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     std::atomic<uint64_t> launches{0};
     cudaStream_t h2d = nullptr, d2h = nullptr;  // copy streams of the pipelined host-buffer path
+    static constexpr int kSideStreams = 4;
+    cudaStream_t side[kSideStreams] = {};  // grouped batches: the requests' image emissions run concurrently
     // Grow-only scratch reused across calls of the host-buffer entry points, so repeated
     // extractions do not pay cudaMalloc each time.
     DevBuf ws_records, ws_f2, ws_vpair, ws_misc, ws_canon, ws_center;
