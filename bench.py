@@ -247,11 +247,13 @@ def units(P: int, M: int) -> float:
 
 
 def host_d2h_bytes(P: int, B: int, wide: bool = False, tile: int = 128) -> int:
-    """Bytes the host-output extraction downloads per call: every f2 slab whole (FP64), and
-    the vpair slabs as their upper tile x tile tiles (row tile <= column tile) of 16-bit
-    counts (32-bit when a block has 65,536 SNPs or more)."""
+    """Bytes the host-output extraction downloads per call: the upper tile x tile tiles (row
+    tile <= column tile, diagonal tiles whole) of every f2 slab in FP64, and of every vpair
+    slab as packed 16-bit counts (32-bit when a block has 65,536 SNPs or more; packed tiles
+    are whole tile x tile squares)."""
     t = -(-P // tile)
-    return 8 * B * P * P + (4 if wide else 2) * B * (t * (t + 1) // 2) * tile * tile
+    upper = sum(min(tile, P - r0) * (P - r0) for r0 in range(0, P, tile))
+    return 8 * B * upper + (4 if wide else 2) * B * (t * (t + 1) // 2) * tile * tile
 
 
 def make_panel(workload: str, rank: int, device: str, n_snp: int | None = None):
@@ -382,8 +384,8 @@ def run_e2e(args, ctx, rec, panel, sel, po, bpr, n_out, barrier, dist, dev, P, M
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    # Host output through the tensor-core path: the f2 slabs cross PCIe whole and the vpair
-    # slabs as packed upper tiles of counts, which the library widens on the host.
+    # Host output through the tensor-core path: the upper tiles of every (exactly symmetric)
+    # slab cross PCIe, f2 in FP64 and vpair as packed counts; the library fills the rest.
     segmented = args.precision != "fp32" and B >= 2 and P > 0
     wide = int(np.bincount(panel.block_id).max()) > 65535 if segmented else False
     d2h = host_d2h_bytes(P, B, wide) if segmented else 2 * n_out * 8

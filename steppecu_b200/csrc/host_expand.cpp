@@ -1,14 +1,18 @@
 // steppecu_b200/csrc/host_expand.cpp
 //
-// Host side of the host-output path's vpair transfer (stpf2_abi.cu: contract_segments): the
-// upper 128 x 128 tiles of each P x P count slab arrive packed as 16-bit (or 32-bit)
-// integers in counts_pack.cu's order, and are widened here to FP64 into both halves of the
-// exactly symmetric, column-major slab (element (i, j) at i + P * j): tile (ti, tj) to rows
-// ti*128.. x columns tj*128.., and off the diagonal its transpose as well.
+// Host side of the host-output path (stpf2_abi.cu: contract_segments). Every P x P slab is
+// exactly symmetric and column-major (element (i, j) at i + P * j), so only its upper
+// 128 x 128 tiles (row tile <= column tile, diagonal tiles whole) cross PCIe:
+// - f2: the upper tiles land in place and mirror_lower_tiles fills the rest by
+//   transposition (rows past each band x the band's columns are the transpose of the block
+//   right of the band's diagonal tile);
+// - vpair: the upper tiles arrive packed as 16-bit (or 32-bit) counts in counts_pack.cu's
+//   order, and expand_counts widens them to FP64 into both halves: tile (ti, tj) to rows
+//   ti*128.. x columns tj*128.., and off the diagonal its transpose as well.
 //
-// With AVX2, 32-byte aligned slabs and P % 4 == 0, four counts are widened per instruction
-// and written with streaming stores (no read-for-ownership of the lines being written);
-// otherwise element by element.
+// With AVX2, 32-byte aligned slabs and P % 4 == 0, both use 4-wide vector code with
+// streaming stores (no read-for-ownership of the lines being written: 4 x 4 register
+// transposes, 4 counts widened per instruction); otherwise element by element.
 #include <immintrin.h>
 
 #include <algorithm>
@@ -18,6 +22,48 @@
 namespace stpf2 {
 
 namespace {
+
+void mirror_scalar(double* S, int64_t P, int64_t T) {
+    for (int64_t r0 = 0; r0 < P; r0 += T) {
+        const int64_t r1 = std::min(P, r0 + T);
+        for (int64_t i0 = r1; i0 < P; i0 += 32)
+            for (int64_t j0 = r0; j0 < r1; j0 += 32) {
+                const int64_t i1 = std::min(P, i0 + 32), j1 = std::min(r1, j0 + 32);
+                for (int64_t j = j0; j < j1; ++j)
+                    for (int64_t i = i0; i < i1; ++i) S[i + P * j] = S[j + P * i];
+            }
+    }
+}
+
+#if defined(__x86_64__)
+// Requires P % 4 == 0, T % 4 == 0 and S 32-byte aligned: every range below is then a
+// multiple of 4 and every destination S[i + P * j] with i % 4 == 0 is 32-byte aligned.
+__attribute__((target("avx2"))) void mirror_avx2(double* S, int64_t P, int64_t T) {
+    for (int64_t r0 = 0; r0 < P; r0 += T) {
+        const int64_t r1 = std::min(P, r0 + T);
+        for (int64_t i0 = r1; i0 < P; i0 += 32)
+            for (int64_t j0 = r0; j0 < r1; j0 += 32) {
+                const int64_t i1 = std::min(P, i0 + 32), j1 = std::min(r1, j0 + 32);
+                for (int64_t j = j0; j < j1; j += 4)
+                    for (int64_t i = i0; i < i1; i += 4) {
+                        // rows j..j+3 of columns i..i+3 (contiguous in the column)
+                        const __m256d a0 = _mm256_loadu_pd(S + j + P * (i + 0));
+                        const __m256d a1 = _mm256_loadu_pd(S + j + P * (i + 1));
+                        const __m256d a2 = _mm256_loadu_pd(S + j + P * (i + 2));
+                        const __m256d a3 = _mm256_loadu_pd(S + j + P * (i + 3));
+                        const __m256d t0 = _mm256_unpacklo_pd(a0, a1), t1 = _mm256_unpackhi_pd(a0, a1);
+                        const __m256d t2 = _mm256_unpacklo_pd(a2, a3), t3 = _mm256_unpackhi_pd(a2, a3);
+                        // column j + m, rows i..i+3
+                        _mm256_stream_pd(S + i + P * (j + 0), _mm256_permute2f128_pd(t0, t2, 0x20));
+                        _mm256_stream_pd(S + i + P * (j + 1), _mm256_permute2f128_pd(t1, t3, 0x20));
+                        _mm256_stream_pd(S + i + P * (j + 2), _mm256_permute2f128_pd(t0, t2, 0x31));
+                        _mm256_stream_pd(S + i + P * (j + 3), _mm256_permute2f128_pd(t1, t3, 0x31));
+                    }
+            }
+    }
+    _mm_sfence();
+}
+#endif
 
 // Widening of packed counts (counts_pack.cu): 4 counts at a time with AVX2.
 template <class In>
@@ -93,6 +139,17 @@ void expand_counts(const void* packed, bool wide, double* S, int64_t P) {
 #if defined(__x86_64__)
     if (avx2) _mm_sfence();
 #endif
+}
+
+void mirror_lower_tiles(double* S, int64_t P, int64_t T) {
+#if defined(__x86_64__)
+    static const bool avx2 = __builtin_cpu_supports("avx2");
+    if (avx2 && P % 4 == 0 && T % 4 == 0 && reinterpret_cast<uintptr_t>(S) % 32 == 0) {
+        mirror_avx2(S, P, T);
+        return;
+    }
+#endif
+    mirror_scalar(S, P, T);
 }
 
 }  // namespace stpf2

@@ -491,6 +491,27 @@ void parallel_for(int n, F&& f) {
         if (e) std::rethrow_exception(e);
 }
 
+// Copies the upper tiles (row tile <= column tile, the diagonal tiles whole) of slabs
+// [0, nb) of a device slab run into the host run: per column tile, one 3-D copy of rows
+// [0, c0 + T) x columns [c0, c0 + T) x every slab. Element (i, j) is at i + P * j, so each
+// column of a copy is one contiguous run of c0 + T doubles.
+void download_upper_tiles(double* host, const double* dev, int64_t P, int64_t T, int64_t nb, cudaStream_t st) {
+    for (int64_t c0 = 0; c0 < P; c0 += T) {
+        const int64_t nr = std::min(P, c0 + T), nc = std::min(T, P - c0);
+        cudaMemcpy3DParms m{};
+        m.srcPtr = make_cudaPitchedPtr(const_cast<double*>(dev), static_cast<size_t>(P) * sizeof(double),
+                                       static_cast<size_t>(P) * sizeof(double), static_cast<size_t>(P));
+        m.dstPtr = make_cudaPitchedPtr(host, static_cast<size_t>(P) * sizeof(double),
+                                       static_cast<size_t>(P) * sizeof(double), static_cast<size_t>(P));
+        m.srcPos = make_cudaPos(0, static_cast<size_t>(c0), 0);
+        m.dstPos = m.srcPos;
+        m.extent = make_cudaExtent(static_cast<size_t>(nr) * sizeof(double), static_cast<size_t>(nc),
+                                   static_cast<size_t>(nb));
+        m.kind = cudaMemcpyDeviceToHost;
+        STPF2_CUDA(cudaMemcpy3DAsync(&m, st));
+    }
+}
+
 // Fork of independent launches from stream s onto the context's side streams, round robin,
 // and their join back into s (events; destruction joins too, so an error path leaves no
 // side-stream work unordered after s).
@@ -614,12 +635,13 @@ struct SlabTarget {
 // The segmented contraction pass with host output. before(k) enqueues what segment k needs
 // on the context stream before its contraction (uploads, decode); the contraction of
 // segment k goes into a two-segment device ring (it waits for the downloads of segment
-// k - 2 from the same buffers). The f2 slabs cross PCIe whole (one contiguous copy per
-// segment); the vpair slabs cross as packed 16-bit upper tiles (counts_pack.cu), which
-// the host widens into both halves of each slab once they have landed. The split keeps
-// both PCIe and the host's memory traffic near their floors: f2 is 8 bytes per element
-// either way, and counts are integers of at most a block's SNP count. With a sink, at most
-// two segments are in flight and each is handed over before its staging slot is reused.
+// k - 2 from the same buffers). Every slab is exactly symmetric (the contraction stores one
+// value at (i, j) and (j, i)), so only its upper 128 x 128 tiles cross PCIe: f2's in place
+// (one 3-D copy per column tile), vpair's as packed 16-bit counts (counts_pack.cu). Once a
+// segment has landed, host threads fill each f2 slab's lower tiles by transposition and
+// widen its counts into both halves of the vpair slab (host_expand.cpp). With a sink, at
+// most two segments are in flight and each is handed over before its staging slot is
+// reused.
 template <class Before>
 void contract_segments(Ctx& c, UmmaPlan* up, int P, const BlockLayout& L, const std::vector<int>& bounds,
                        const SlabTarget& t, Before&& before) {
@@ -670,7 +692,7 @@ void contract_segments(Ctx& c, UmmaPlan* up, int P, const BlockLayout& L, const 
         launch_pack_counts(c, vpk, P, static_cast<int64_t>(nb), wide, cntk, c.stream);
         STPF2_CUDA(cudaEventRecord(ev[2 * k], c.stream));
         STPF2_CUDA(cudaStreamWaitEvent(c.d2h, ev[2 * k], 0));
-        STPF2_CUDA(cudaMemcpyAsync(host_f2(k), f2k, nb * slab * sizeof(double), cudaMemcpyDeviceToHost, c.d2h));
+        download_upper_tiles(host_f2(k), f2k, P, 128, static_cast<int64_t>(nb), c.d2h);
         STPF2_CUDA(cudaMemcpyAsync(host_cnt(k), cntk, nb * cnt_slab, cudaMemcpyDeviceToHost, c.d2h));
         STPF2_CUDA(cudaEventRecord(ev[2 * k + 1], c.d2h));
     };
@@ -683,7 +705,10 @@ void contract_segments(Ctx& c, UmmaPlan* up, int P, const BlockLayout& L, const 
         double* f2h = host_f2(k);
         double* vph = host_vp(k);
         const uint8_t* cnt = host_cnt(k);
-        parallel_for(nb, [&](int u) { expand_counts(cnt + u * cnt_slab, wide, vph + slab * static_cast<size_t>(u), P); });
+        parallel_for(2 * nb, [&](int u) {
+            if (u % 2 == 0) mirror_lower_tiles(f2h + slab * static_cast<size_t>(u / 2), P, 128);
+            else expand_counts(cnt + (u / 2) * cnt_slab, wide, vph + slab * static_cast<size_t>(u / 2), P);
+        });
         if (t.sink && t.sink(t.user, bounds[k], bounds[k + 1], f2h, vph) != 0)
             fail(STP_RUNTIME_ERROR, "the slab sink stopped the extraction");
     }

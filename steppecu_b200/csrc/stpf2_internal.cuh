@@ -436,12 +436,15 @@ void launch_fstat_assemble(Ctx& c, const double* f2, int P, const int32_t* surv,
 void launch_jackknife(Ctx& c, const double* x, const int32_t* block_sizes, int64_t m, int nb,
                       double* est, double* var, cudaStream_t s);
 
-// Host-output vpair transfer (counts_pack.cu, host_expand.cpp): the upper 128 x 128 tiles of
-// nb count slabs packed as 16-bit (wide: 32-bit) integers, and their widening on the host
-// into both halves of one P x P FP64 slab.
+// Host-output transfer (counts_pack.cu, host_expand.cpp): the upper 128 x 128 tiles of nb
+// count slabs packed as 16-bit (wide: 32-bit) integers, and their widening on the host into
+// both halves of one P x P FP64 slab.
 size_t packed_counts_bytes(int P, int64_t nb, bool wide);
 void launch_pack_counts(Ctx& c, const double* vp, int P, int64_t nb, bool wide, void* out, cudaStream_t s);
 void expand_counts(const void* packed, bool wide, double* S, int64_t P);
+// Fills the lower tiles of a symmetric P x P column-major slab whose upper T x T tiles are in
+// place (host_expand.cpp).
+void mirror_lower_tiles(double* S, int64_t P, int64_t T);
 
 // Allocation-free count decode (noalloc.cu): every intermediate lives in one static
 // device array of kNoAllocScratchBytes.

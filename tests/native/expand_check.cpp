@@ -1,6 +1,10 @@
 // Checker for steppecu_b200/csrc/host_expand.cpp, built and run by tests/test_host_expand.py.
 //
-// For each P, both count widths and a 32-byte aligned and a misaligned slab (so that both the
+// mirror_lower_tiles: for each P (and a 32-byte aligned and a misaligned slab), a symmetric
+// P x P column-major slab is kept only in its upper 128 x 128 tiles (what the download
+// copies), the rest set to -1; the mirror must restore the full slab bit for bit.
+//
+// expand_counts: for each P, both count widths and a 32-byte aligned and a misaligned slab (so that both the
 // AVX2 path and the element path run where the CPU has AVX2), it draws a symmetric P x P
 // integer slab, packs its upper 128 x 128 tiles the way counts_pack.cu does (upper tile u in
 // row-major order of ti <= tj, then column c, then row r; zero past the last population),
@@ -13,6 +17,7 @@
 
 namespace stpf2 {
 void expand_counts(const void* packed, bool wide, double* S, int64_t P);
+void mirror_lower_tiles(double* S, int64_t P, int64_t T);
 }
 
 template <class T>
@@ -56,6 +61,24 @@ int main() {
                     std::printf("mismatch P=%lld wide=%d offset=%d\n", static_cast<long long>(P), wide, off);
                     return 1;
                 }
+            }
+        }
+    for (int64_t P : sizes)
+        for (int off = 0; off < 2; ++off) {
+            std::vector<double> buf(static_cast<size_t>(P * P + 8));
+            const uintptr_t base = (reinterpret_cast<uintptr_t>(buf.data()) + 31) & ~uintptr_t(31);
+            double* S = reinterpret_cast<double*>(base) + off;
+            std::vector<double> full(static_cast<size_t>(P * P));
+            for (int64_t j = 0; j < P; ++j)
+                for (int64_t i = 0; i <= j; ++i) full[i + P * j] = full[j + P * i] = next(1ull << 40) * 0x1.0p-40;
+            for (int64_t k = 0; k < P * P; ++k) S[k] = -1.0;
+            for (int64_t r0 = 0; r0 < P; r0 += 128)
+                for (int64_t j = r0; j < P; ++j)
+                    for (int64_t i = r0; i < r0 + 128 && i < P; ++i) S[i + P * j] = full[i + P * j];
+            stpf2::mirror_lower_tiles(S, P, 128);
+            if (std::memcmp(S, full.data(), static_cast<size_t>(P * P) * sizeof(double)) != 0) {
+                std::printf("mirror mismatch P=%lld offset=%d\n", static_cast<long long>(P), off);
+                return 1;
             }
         }
     std::printf("ok\n");

@@ -1,6 +1,6 @@
 """The bench line's arithmetic, on CPU: the metric's units, the issued tensor work of the
 split contraction counted from its MMA schedule, and the bytes the host-output extraction
-downloads (whole f2 slabs and packed upper tiles of counts)."""
+downloads (upper tiles: f2 in FP64, vpair as packed counts)."""
 from __future__ import annotations
 
 import importlib.util
@@ -44,5 +44,5 @@ def test_host_d2h_bytes_match_the_copies(P):
     t = -(-P // 128)
     packed = t * (t + 1) // 2 * 128 * 128  # counts per slab, with each tile padded to 128 x 128
     assert packed >= int(upper.sum())
-    assert bench.host_d2h_bytes(P, B) == B * (8 * P * P + 2 * packed)
-    assert bench.host_d2h_bytes(P, B, wide=True) == B * (8 * P * P + 4 * packed)
+    assert bench.host_d2h_bytes(P, B) == B * (8 * int(upper.sum()) + 2 * packed)
+    assert bench.host_d2h_bytes(P, B, wide=True) == B * (8 * int(upper.sum()) + 4 * packed)

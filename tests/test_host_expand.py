@@ -1,8 +1,9 @@
-"""The host side of the host-output vpair transfer (steppecu_b200/csrc/host_expand.cpp), on
-CPU: it is plain C++, so it is compiled here with tests/native/expand_check.cpp, which packs
-random symmetric count slabs in the device packer's order and checks the widened slabs bit
-for bit, for P from 1 to 1,001, 16- and 32-bit counts, on 32-byte aligned slabs (the AVX2
-path where the CPU has AVX2) and misaligned ones (the element path)."""
+"""The host side of the host-output transfer (steppecu_b200/csrc/host_expand.cpp), on CPU: it
+is plain C++, so it is compiled here with tests/native/expand_check.cpp. It packs random
+symmetric count slabs in the device packer's order and checks the widened slabs, and fills
+the lower tiles of symmetric FP64 slabs from their upper tiles, bit for bit, for P from 1 to
+1,001, 16- and 32-bit counts, on 32-byte aligned slabs (the AVX2 paths where the CPU has
+AVX2) and misaligned ones (the element paths)."""
 from __future__ import annotations
 
 import shutil
@@ -14,7 +15,7 @@ import pytest
 ROOT = Path(__file__).resolve().parents[1]
 
 
-def test_expand_counts_fills_both_halves_exactly(tmp_path):
+def test_expand_and_mirror_fill_both_halves_exactly(tmp_path):
     gxx = shutil.which("g++")
     if gxx is None:
         pytest.skip("g++ not available")
