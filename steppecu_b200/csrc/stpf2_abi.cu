@@ -494,9 +494,12 @@ void parallel_for(int n, F&& f) {
 // Copies the upper tiles (row tile <= column tile, the diagonal tiles whole) of slabs
 // [0, nb) of a device slab run into the host run: per column tile, one 3-D copy of rows
 // [0, c0 + T) x columns [c0, c0 + T) x every slab. Element (i, j) is at i + P * j, so each
-// column of a copy is one contiguous run of c0 + T doubles.
-void download_upper_tiles(double* host, const double* dev, int64_t P, int64_t T, int64_t nb, cudaStream_t st) {
+// column of a copy is one contiguous run of c0 + T doubles. The column tiles alternate
+// between two streams: runs this short keep one copy engine at ~30 GB/s, two run together.
+void download_upper_tiles(double* host, const double* dev, int64_t P, int64_t T, int64_t nb, cudaStream_t st0,
+                          cudaStream_t st1) {
     for (int64_t c0 = 0; c0 < P; c0 += T) {
+        const cudaStream_t st = ((c0 / T) & 1) ? st1 : st0;
         const int64_t nr = std::min(P, c0 + T), nc = std::min(T, P - c0);
         cudaMemcpy3DParms m{};
         m.srcPtr = make_cudaPitchedPtr(const_cast<double*>(dev), static_cast<size_t>(P) * sizeof(double),
@@ -557,6 +560,7 @@ struct DrainOnError {
         cudaStreamSynchronize(c.h2d);
         cudaStreamSynchronize(c.stream);
         cudaStreamSynchronize(c.d2h);
+        for (cudaStream_t x : c.side) cudaStreamSynchronize(x);
     }
 };
 
@@ -663,14 +667,16 @@ void contract_segments(Ctx& c, UmmaPlan* up, int P, const BlockLayout& L, const 
         c.pin_counts.reserve(static_cast<size_t>(L.n_block) * cnt_slab);
     }
     std::vector<cudaEvent_t> ev(2 * nseg, nullptr);  // per segment: contracted and packed, downloaded
+    std::vector<cudaEvent_t> ev2(nseg, nullptr);     // per segment: the second copy queue done
     struct Free {
         std::vector<cudaEvent_t>& ev;
         ~Free() {
             for (auto e : ev)
                 if (e) cudaEventDestroy(e);
         }
-    } free_events{ev};
+    } free_events{ev}, free_events2{ev2};
     for (auto& e : ev) STPF2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : ev2) STPF2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     auto host_f2 = [&](size_t k) {
         return t.sink ? c.pin_stage.as<double>() + (k % 2) * ring * slab : t.f2 + slab * bounds[k];
     };
@@ -692,8 +698,11 @@ void contract_segments(Ctx& c, UmmaPlan* up, int P, const BlockLayout& L, const 
         launch_pack_counts(c, vpk, P, static_cast<int64_t>(nb), wide, cntk, c.stream);
         STPF2_CUDA(cudaEventRecord(ev[2 * k], c.stream));
         STPF2_CUDA(cudaStreamWaitEvent(c.d2h, ev[2 * k], 0));
-        download_upper_tiles(host_f2(k), f2k, P, 128, static_cast<int64_t>(nb), c.d2h);
+        STPF2_CUDA(cudaStreamWaitEvent(c.side[0], ev[2 * k], 0));
+        download_upper_tiles(host_f2(k), f2k, P, 128, static_cast<int64_t>(nb), c.d2h, c.side[0]);
         STPF2_CUDA(cudaMemcpyAsync(host_cnt(k), cntk, nb * cnt_slab, cudaMemcpyDeviceToHost, c.d2h));
+        STPF2_CUDA(cudaEventRecord(ev2[k], c.side[0]));  // the second copy queue joins the first
+        STPF2_CUDA(cudaStreamWaitEvent(c.d2h, ev2[k], 0));
         STPF2_CUDA(cudaEventRecord(ev[2 * k + 1], c.d2h));
     };
     const size_t depth = t.sink ? 2 : nseg;
