@@ -16,7 +16,9 @@
 //                                                       dropped: under 3.1 * 2^30 / S^2,
 //                                                       i.e. 1.7e-10, per SNP)
 //     V_w += E_w(i) M(j) + M(i) E_w(j)                  (E_3..E_6: the digits of -A)
-// i.e. 18 kind::i8 MMAs (M = N = 128, K = 32) per 32-SNP stage, all integer and exact.
+// i.e. 18 kind::i8 products (M = N = 128, K = 32) per 32-SNP stage, all integer and exact,
+// issued as 12 MMAs: where two products of one A operand go into adjacent weights from
+// adjacent B planes, one MMA of N = 256 covers both.
 // The epilogue forms W = sum_w V_w 256^(w-3) exactly in int64 once per tile (every 16,384
 // SNPs of a longer block, the int32 bound; segments add in FP64), f2 = W * kFxNumScale /
 // vpair (0 when vpair = 0, f2_estimator.hpp:42-46), and stores (i,j) and (j,i) of the
@@ -254,6 +256,8 @@ __device__ void fx_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t t
         const BlockInfo bi = a.blocks[w.blk];
         const int nst = stages_of(bi.k, kStageK);
         const uint32_t id = idesc_for<kGrouped>(a, w, bi);
+        // The same shape with N = 128 + n: two adjacent B planes into two adjacent weights.
+        const uint32_t id2 = (id & ~(0x3Fu << 17)) | ((((id >> 17) & 0x3Fu) + 16u) << 17);
         const bool diag = w.ti == w.tj;
         for (int st = 0; st < nst; ++st, ++g) {
             const int sseg = st % kSegStages;
@@ -271,27 +275,25 @@ __device__ void fx_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t t
                 auto dB = [&](int t) { return smem_desc(sb + static_cast<uint32_t>(t) * 4096u, 256, 6); };
                 const uint32_t f = sseg == 0 ? 0u : 1u;  // the first stage of a segment overwrites
                 using C = CollectorA;
-                // X digit products of weight >= 256^3, grouped by A operand: a group reads its
-                // A tile from shared memory once and keeps it in the collector buffer.
-                mma_i8_c<C::kFill>(V3, dA(3), dB(0), id, f);
-                mma_i8_c<C::kUse>(V4, dA(3), dB(1), id, f);
-                mma_i8_c<C::kUse>(V5, dA(3), dB(2), id, f);
-                mma_i8_c<C::kLastUse>(V6, dA(3), dB(3), id, f);
-                mma_i8_c<C::kFill>(V3, dA(2), dB(1), id, 1u);
-                mma_i8_c<C::kUse>(V4, dA(2), dB(2), id, 1u);
-                mma_i8_c<C::kLastUse>(V5, dA(2), dB(3), id, 1u);
-                mma_i8_c<C::kFill>(V3, dA(1), dB(2), id, 1u);
-                mma_i8_c<C::kLastUse>(V4, dA(1), dB(3), id, 1u);
-                mma_i8_c<C::kDiscard>(V3, dA(0), dB(3), id, 1u);
-                // M(i) E_w(j) and E_w(i) M(j): tiles 4..7 are E_3..E_6, tile 8 is M.
-                mma_i8_c<C::kFill>(V3, dA(8), dB(4), id, 1u);
-                mma_i8_c<C::kUse>(V4, dA(8), dB(5), id, 1u);
-                mma_i8_c<C::kUse>(V5, dA(8), dB(6), id, 1u);
-                mma_i8_c<C::kLastUse>(V6, dA(8), dB(7), id, 1u);
-                mma_i8_c<C::kDiscard>(V3, dA(4), dB(8), id, 1u);
-                mma_i8_c<C::kDiscard>(V4, dA(5), dB(8), id, 1u);
-                mma_i8_c<C::kDiscard>(V5, dA(6), dB(8), id, 1u);
-                mma_i8_c<C::kDiscard>(V6, dA(7), dB(8), id, 1u);
+                // Planes are 4 KiB apart and V_3..V_6 128 TMEM columns apart, so an MMA of
+                // N = 128 + n on two adjacent B planes fills two adjacent weights at once
+                // (columns 0..n-1 from the first plane, 128.. from the second): 12 MMAs per
+                // stage for the 18 digit products, A kept in the collector buffer across the
+                // two MMAs of one shape that share it.
+                mma_i8_c<C::kFill>(V3, dA(3), dB(0), id2, f);     // X3 [X0;X1] -> V3,V4
+                mma_i8_c<C::kLastUse>(V5, dA(3), dB(2), id2, f);  // X3 [X2;X3] -> V5,V6
+                mma_i8(V3, dA(2), dB(1), id2, 1u);                // X2 [X1;X2] -> V3,V4
+                mma_i8(V5, dA(2), dB(3), id, 1u);                 // X2 X3      -> V5
+                mma_i8(V3, dA(1), dB(2), id2, 1u);                // X1 [X2;X3] -> V3,V4
+                mma_i8(V3, dA(0), dB(3), id, 1u);                 // X0 X3      -> V3
+                // M(i) E_w(j) on the stacked E planes, and E_w(i) M(j): tiles 4..7 are
+                // E_3..E_6, tile 8 is M.
+                mma_i8_c<C::kFill>(V3, dA(8), dB(4), id2, 1u);     // M [E3;E4] -> V3,V4
+                mma_i8_c<C::kLastUse>(V5, dA(8), dB(6), id2, 1u);  // M [E5;E6] -> V5,V6
+                mma_i8(V3, dA(4), dB(8), id, 1u);
+                mma_i8(V4, dA(5), dB(8), id, 1u);
+                mma_i8(V5, dA(6), dB(8), id, 1u);
+                mma_i8(V6, dA(7), dB(8), id, 1u);
             }
             mma_commit(&ctl->empty[slot]);
             if (sseg == kSegStages - 1 || st == nst - 1) {
