@@ -46,7 +46,7 @@ OPERAND_BYTES = {"split_bf16": 11, "split_f16": 11, "split_f16_fine": 11, "fixed
 # dram__bytes_read.sum + dram__bytes_write.sum per contraction (all its launches) at C3, from
 # ncu captures summarised under profiles/ (split_f16: one pass on the full workload;
 # fixed_i8: the 115k-SNP case scaled by its SNPs and blocks, 10x).
-CONTRACTION_TRAFFIC = {("c3", "split_f16"): 13.58e9 + 12.24e9, ("c3", "fixed_i8"): 27.9e9 + 2.4e9}
+CONTRACTION_TRAFFIC = {("c3", "split_f16"): 13.58e9 + 12.24e9, ("c3", "fixed_i8"): 27.2e9 + 2.4e9}
 
 
 def issued_tensor_work(P: int, block_id, n_block: int, con_ms: float, peak: float) -> dict:
