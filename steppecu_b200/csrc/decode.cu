@@ -209,9 +209,21 @@ struct FxTerms8 {
 };
 
 __device__ __forceinline__ FxTerms8 fx_terms8_from_counts(const uint32_t (&v)[8], const double* __restrict__ rec_n,
-                                                          const double* __restrict__ rec_nm1) {
+                                                          const double* __restrict__ rec_nm1,
+                                                          const uint2* __restrict__ table = nullptr, int ld = 0) {
     FxTerms8 t;
     t.mbits = 0;
+    if (table) {  // the precomputed digit words of (n, a2): the same function, evaluated once
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const uint32_t n = v[c] >> 16, a2 = v[c] & 0xFFFFu;
+            const uint2 e = __ldg(table + static_cast<int64_t>(n) * ld + a2);
+            t.x[c] = e.x;
+            t.na[c] = e.y;
+            t.mbits |= (n > 0 ? 1u : 0u) << c;
+        }
+        return t;
+    }
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         const uint32_t n = v[c] >> 16, a2 = v[c] & 0xFFFFu;
@@ -657,7 +669,7 @@ decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t
 #pragma unroll
         for (int c = 0; c < 8; ++c) v[c] = cnt[c * kCntCol];
         if constexpr (F == OpFmt::FX)
-            emit8_fx(op, i, col_base + col0, fx_terms8_from_counts(v, rec_n, rec_nm1));
+            emit8_fx(op, i, col_base + col0, fx_terms8_from_counts(v, rec_n, rec_nm1, op.fx_table, op.fx_table_ld));
         else
             emit8<F>(op, i, col_base + col0, terms8_from_counts(v, cen, rec_n, rec_nm1));
     }
@@ -914,7 +926,7 @@ emit_counts_kernel(const uint32_t* __restrict__ counts, int64_t cnt_ld, const in
             if constexpr (F != OpFmt::FX) cen[c] = s >= 0 ? __ldg(center_snp + s) : 0.5;  // the fixed point needs none
         }
         if constexpr (F == OpFmt::FX)
-            emit8_fx(op, i, col0, fx_terms8_from_counts(v, rec_n, rec_nm1));
+            emit8_fx(op, i, col0, fx_terms8_from_counts(v, rec_n, rec_nm1, op.fx_table, op.fx_table_ld));
         else
             emit8<F>(op, i, col0, terms8_from_counts(v, cen, rec_n, rec_nm1));
     }
@@ -962,6 +974,38 @@ void launch_layout_tables(Ctx& c, const BlockInfo* blocks, const int64_t* snp_be
                           int32_t* col_snp, TileInfo* tiles, cudaStream_t s) {
     if (ld <= 0) return;
     layout_tables_kernel<<<static_cast<unsigned>((ld + 255) / 256), 256, 0, s>>>(blocks, snp_begin, n_block, ld, col_snp, tiles);
+    STPF2_CUDA(cudaGetLastError());
+    c.launches++;
+}
+
+namespace {
+// Entry n * (2 n_max + 1) + a2 of the fixed-point term table: the digit words of X and -A
+// for a population with n called alleles and doubled count a2, exactly as the emit
+// computes them (zeros when n = 0 or a2 > 2n).
+__global__ void fx_table_kernel(const double* __restrict__ rec_n, const double* __restrict__ rec_nm1, int64_t n_max,
+                                uint2* __restrict__ out) {
+    const int64_t ld = 2 * n_max + 1;
+    const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= (n_max + 1) * ld) return;
+    const int64_t n = k / ld, a2 = k - n * ld;
+    uint32_t X = 0, NA = 0;
+    if (n > 0 && a2 <= 2 * n) {
+        const double a2d = __hiloint2double(0x43300000, static_cast<int>(a2)) - 4503599627370496.0;
+        fx_terms(a2d * 0.5 * __ldg(rec_n + n), __ldg(rec_nm1 + n), X, NA);
+    }
+    out[k] = make_uint2(fx_digits(X), fx_digits(NA));
+}
+}  // namespace
+
+int64_t fx_table_entries(int64_t n_max) {
+    const int64_t e = (n_max + 1) * (2 * n_max + 1);
+    return e <= (int64_t(1) << 20) ? e : 0;  // 8 MiB at most; larger populations compute the terms
+}
+
+void launch_fx_table(Ctx& c, const double* rec_n, const double* rec_nm1, int64_t n_max, uint2* out, cudaStream_t s) {
+    const int64_t e = fx_table_entries(n_max);
+    if (e <= 0) return;
+    fx_table_kernel<<<static_cast<unsigned>((e + 255) / 256), 256, 0, s>>>(rec_n, rec_nm1, n_max, out);
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
 }

@@ -166,6 +166,7 @@ struct Plan {
     BlockLayout L;
     DevBuf sel, pop_off, pos, tiles, col_snp, rec_n, rec_nm1, canon, center, blocks, items, own_planes, repitched;
     DevBuf fold_order;  // per 64-population group, local indices largest first (null: all equal)
+    DevBuf fx_table;    // FX: the term table of every (n, a2) (OperandPlanes::fx_table)
     DevBuf row_map;     // kept SNP -> record row (empty: SNP s is record s)
     std::vector<int64_t> kept;  // the same on the host (segment uploads of host records)
     uint64_t* canon_ptr = nullptr;  // canon's storage, or a context workspace (one-shot calls)
@@ -356,9 +357,18 @@ std::unique_ptr<Plan> build_plan(Ctx& c, const stp_f2_request& r, uint64_t pitch
         p->own_planes.reserve(ob);
         planes_base = p->own_planes.ptr;
     }
-    // Padding columns must read as zero; decode only ever writes real SNP columns.
+    // Padding columns must read as zero; decode only ever writes real SNP columns. A plan
+    // cached on the context relies on that for the shared planes workspace, so building
+    // another plan there drops it.
+    if (planes_base == c.ws_misc.ptr) c.plan_cache.reset();
     STPF2_CUDA(cudaMemsetAsync(planes_base, 0, ob, s));
     bind_operand_planes(p->op, fmt, r.n_pop, p->L.ld, planes_base);
+    if (fmt == OpFmt::FX && fx_table_entries(n_max) > 0) {
+        p->fx_table.reserve(static_cast<size_t>(fx_table_entries(n_max)) * sizeof(uint2));
+        launch_fx_table(c, p->rec_n.as<double>(), p->rec_nm1.as<double>(), n_max, p->fx_table.as<uint2>(), s);
+        p->op.fx_table = p->fx_table.as<uint2>();
+        p->op.fx_table_ld = static_cast<int32_t>(2 * n_max + 1);
+    }
 
     if (r.precision == STP_PREC_FP32_SIMT) {
         const std::vector<WorkItem> items = make_work_items(p->L, r.n_pop, simt_tile());
@@ -1191,6 +1201,12 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
     auto* d_counts = reinterpret_cast<uint32_t*>(T + o_counts);
     auto* d_rn = reinterpret_cast<const double*>(T + o_rn);
     auto* d_rnm1 = reinterpret_cast<const double*>(T + o_rnm1);
+    const uint2* d_fxtab = nullptr;
+    if (fmt == OpFmt::FX && fx_table_entries(n_max) > 0) {
+        c.ws_fxtab.reserve(static_cast<size_t>(fx_table_entries(n_max)) * sizeof(uint2));
+        launch_fx_table(c, d_rn, d_rnm1, n_max, c.ws_fxtab.as<uint2>(), s);
+        d_fxtab = c.ws_fxtab.as<uint2>();
+    }
     if (any_auto)
         launch_copy_union_ploidy(c, reinterpret_cast<uint32_t*>(T + o_sel), reinterpret_cast<int32_t*>(T + o_umap),
                                  static_cast<int64_t>(sel_up.size()), d_desc_u, s);
@@ -1260,6 +1276,8 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
             const MemberOffsets& q = mo[wave[w]];
             const stp_f2_output& o = outs[p.k];
             bind_operand_planes(p.op, fmt, p.P, p.L.ld, c.ws_batch.as<uint8_t>() + io);
+            p.op.fx_table = d_fxtab;
+            p.op.fx_table_ld = static_cast<int32_t>(2 * n_max + 1);
             io += p.img_bytes;
             launch_emit_counts(c, d_counts, M, reinterpret_cast<const int32_t*>(T + q.upop), p.P, p.L.ld / kTileK,
                                reinterpret_cast<const int32_t*>(T + q.cols), d_center_u, d_rn, d_rnm1, p.op,

@@ -31,6 +31,9 @@ struct Error : std::runtime_error {
 
 inline void cuda_check(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return;
+    // A failed call also leaves its (non-sticky) error as the thread's last error: clear it,
+    // so the next launch check of this or a later call reports only its own launch.
+    (void)cudaGetLastError();
     const stp_status s = (e == cudaErrorMemoryAllocation) ? STP_DEVICE_OOM : STP_CUDA_ERROR;
     fail(s, std::string(what) + ": " + cudaGetErrorString(e));
 }
@@ -128,6 +131,7 @@ struct Ctx {
     DevBuf ws_batch, ws_union, ws_tables, ws_items;
     DevBuf ws_fstat;  // stp_fstats scratch
     DevBuf ws_vpc;    // grouped fixed-point batches: compact vpair tiles
+    DevBuf ws_fxtab;  // grouped fixed-point batches: the term table of the union's counts
     PinnedBuf pin_union, pin_tables, pin_items;
     PinnedBuf pin_stage;  // streamed extraction: the two-segment staging ring of f2 / vpair slabs
     DevBuf ws_counts;      // host-output path: packed vpair tiles of two segments
@@ -226,6 +230,11 @@ struct OperandPlanes {
     void* planes = nullptr;
     uint8_t* m_u8 = nullptr;  // FP32 form only: row-major int8 M
     uint8_t* mplanes = nullptr;  // FX only: the M tiles, (row tile, chunk) 4 KiB each
+    // FX only, optional: the digit words (fx_digits of X, of -A) of every count pair a
+    // population can reach, entry n * fx_table_ld + a2 (fx_table_kernel), read by the emit
+    // instead of computing the terms; null: computed per element.
+    const uint2* fx_table = nullptr;
+    int32_t fx_table_ld = 0;
     double scale_inv = 1.0;  // numerator scale undo (F16 planes are pre-scaled)
     int n_rt = 0;            // tiled: row tiles of 128 populations
     int64_t n_ck = 0;        // tiled: column chunks of 32
@@ -440,6 +449,11 @@ void launch_jackknife(Ctx& c, const double* x, const int32_t* block_sizes, int64
 // count slabs packed as 16-bit (wide: 32-bit) integers, and their widening on the host into
 // both halves of one P x P FP64 slab.
 size_t packed_counts_bytes(int P, int64_t nb, bool wide);
+// The fixed-point term table of OperandPlanes::fx_table for called-allele counts 0..n_max
+// (decode.cu); fx_table_entries: its size, 0 when it would exceed the cap (then the emit
+// computes the terms).
+int64_t fx_table_entries(int64_t n_max);
+void launch_fx_table(Ctx& c, const double* rec_n, const double* rec_nm1, int64_t n_max, uint2* out, cudaStream_t s);
 void launch_pack_counts(Ctx& c, const double* vp, int P, int64_t nb, bool wide, void* out, cudaStream_t s);
 void expand_counts(const void* packed, bool wide, double* S, int64_t P);
 // Fills the lower tiles of a symmetric P x P column-major slab whose upper T x T tiles are in

@@ -63,3 +63,19 @@ def test_changed_arrays_at_the_same_address_rebuild(ctx, panel):
     # A different precision is a different plan.
     got = ctx.extract_blocks(rec, p.n_ind, sel, po, bid, p.n_block, precision="split_f16")
     assert _same(got, _fresh(rec, p, sel, po, bid, p.n_block, precision="split_f16"))
+
+
+def test_cached_plan_survives_another_plan_in_its_workspace(ctx, panel):
+    """A streamed extraction of another request builds its plan in the same operand-plane
+    workspace (other block padding, other populations); the next repeat of the cached request
+    must rebuild rather than read stale padding columns: equal to a fresh context, bit for bit."""
+    p = panel
+    sel, po = p.selection()
+    rec = p.records_numpy()
+    want = _fresh(rec, p, sel, po, p.block_id, p.n_block, precision="fixed_i8")
+    ctx.extract_blocks(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision="fixed_i8")  # cached
+    sel2, po2 = p.selection(list(range(0, p.n_pop, 2)))
+    bid2 = (np.arange(p.n_snp) // 777).astype(np.int32)  # other padding
+    ctx.extract_streamed(rec, p.n_ind, sel2, po2, bid2, int(bid2[-1]) + 1, lambda *a: None, precision="fixed_i8")
+    got = ctx.extract_blocks(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision="fixed_i8")
+    assert _same(got, want)
