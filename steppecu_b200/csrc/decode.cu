@@ -239,11 +239,16 @@ __device__ __forceinline__ FxTerms8 fx_terms8_from_counts(const uint32_t (&v)[8]
     return t;
 }
 
-// Byte k of each of four words, in order, as one word.
-__device__ __forceinline__ uint32_t gather_byte(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, int k) {
-    const uint32_t sel = static_cast<uint32_t>(k) | (static_cast<uint32_t>(k + 4) << 4);
-    return __byte_perm(__byte_perm(w0, w1, sel), __byte_perm(w2, w3, sel), 0x5410);
+// 4 x 4 byte transpose: o[k] holds byte k of w0, w1, w2, w3 in its bytes 0..3 (eight PRMTs).
+__device__ __forceinline__ void bytes4x4(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, uint32_t (&o)[4]) {
+    const uint32_t a = __byte_perm(w0, w1, 0x5140), b = __byte_perm(w0, w1, 0x7362);  // bytes 0,1 / 2,3 of w0,w1
+    const uint32_t c = __byte_perm(w2, w3, 0x5140), d = __byte_perm(w2, w3, 0x7362);
+    o[0] = __byte_perm(a, c, 0x5410);
+    o[1] = __byte_perm(a, c, 0x7632);
+    o[2] = __byte_perm(b, d, 0x5410);
+    o[3] = __byte_perm(b, d, 0x7632);
 }
+
 
 // Writes 8 consecutive columns (starting at a multiple of 8) of one population into its
 // fixed-point operand image (nine int8 tiles, 8 bytes each) and into the separate M tiles.
@@ -251,25 +256,21 @@ __device__ __forceinline__ void emit8_fx(const OperandPlanes& op, int i, int64_t
     const int r = i % kTileRows, k = static_cast<int>(col % kTileK);
     const int64_t tile = static_cast<int64_t>(i / kTileRows) * op.n_ck + col / kTileK;
     uint8_t* img = static_cast<uint8_t*>(op.planes) + tile * kFxImageBytes + tile8_offset(r, k);
+    // Digit d of the 8 columns, per plane: two 4 x 4 byte transposes per digit word set.
+    uint32_t x0[4], x1[4], n0[4], n1[4];
+    bytes4x4(t.x[0], t.x[1], t.x[2], t.x[3], x0);
+    bytes4x4(t.x[4], t.x[5], t.x[6], t.x[7], x1);
+    bytes4x4(t.na[0], t.na[1], t.na[2], t.na[3], n0);
+    bytes4x4(t.na[4], t.na[5], t.na[6], t.na[7], n1);
 #pragma unroll
     for (int d = 0; d < 4; ++d) {
-        uint2 vx, vn;
-        vx.x = gather_byte(t.x[0], t.x[1], t.x[2], t.x[3], d);
-        vx.y = gather_byte(t.x[4], t.x[5], t.x[6], t.x[7], d);
-        vn.x = gather_byte(t.na[0], t.na[1], t.na[2], t.na[3], d);
-        vn.y = gather_byte(t.na[4], t.na[5], t.na[6], t.na[7], d);
-        *reinterpret_cast<uint2*>(img + d * kTile8Bytes) = vx;
-        *reinterpret_cast<uint2*>(img + (4 + d) * kTile8Bytes) = vn;
+        *reinterpret_cast<uint2*>(img + d * kTile8Bytes) = make_uint2(x0[d], x1[d]);
+        *reinterpret_cast<uint2*>(img + (4 + d) * kTile8Bytes) = make_uint2(n0[d], n1[d]);
     }
-    uint2 mv;
-    mv.x = 0;
-    mv.y = 0;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        const uint32_t b = ((t.mbits >> c) & 1u) ? uint32_t(kFxM) : 0u;
-        if (c < 4) mv.x |= b << (8 * c);
-        else mv.y |= b << (8 * (c - 4));
-    }
+    // M = 64 in byte c where column c is called: bit c of each nibble spread to bit 8c.
+    static_assert(kFxM == 64, "M is 1 << 6");
+    const uint32_t lo = t.mbits & 0xFu, hi = (t.mbits >> 4) & 0xFu;
+    const uint2 mv = make_uint2(((lo * 0x00204081u) & 0x01010101u) << 6, ((hi * 0x00204081u) & 0x01010101u) << 6);
     *reinterpret_cast<uint2*>(op.mplanes + tile * kTile8Bytes + tile8_offset(r, k)) = mv;
 }
 
