@@ -424,10 +424,10 @@ transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t
             const int64_t rem = n_ind - r0;
             if (rem <= 0) break;
             const int nv = static_cast<int>(rem < 16 ? rem : 16);
-            uint64_t out[16];
-#pragma unroll
-            for (int m = 0; m < 16; ++m) out[m] = 0;
             const uint32_t* base = srec + sub * kTileCols * kRowStride + sub * 8 + wl;
+            // y[rg][j]: the 4 x 4 block of SNPs 4rg.. x samples 4j.., transposed so that byte
+            // 3 - m holds sample 4j + m's four codes.
+            uint32_t y[kTileCols / 4][4];
 #pragma unroll
             for (int rg = 0; rg < kTileCols / 4; ++rg) {
                 uint32_t rw[4];
@@ -438,11 +438,18 @@ transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t
                     const uint32_t sel = static_cast<uint32_t>(j) | (static_cast<uint32_t>(j + 4) << 4);
                     const uint32_t a = __byte_perm(rw[0], rw[1], sel);
                     const uint32_t b = __byte_perm(rw[2], rw[3], sel);
-                    const uint32_t y = transpose4x4_2bit(__byte_perm(a, b, 0x0145));
-#pragma unroll
-                    for (int m = 0; m < 4; ++m)
-                        out[4 * j + m] |= static_cast<uint64_t>((y >> (8 * (3 - m))) & 0xFFu) << (8 * rg);
+                    y[rg][j] = transpose4x4_2bit(__byte_perm(a, b, 0x0145));
                 }
+            }
+            // Sample 4j + m's 32 SNPs: byte 3 - m of y[0..7][j], by 4 x 4 byte transposes.
+            uint64_t out[16];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                uint32_t lo[4], hi[4];
+                bytes4x4(y[0][j], y[1][j], y[2][j], y[3][j], lo);
+                bytes4x4(y[4][j], y[5][j], y[6][j], y[7][j], hi);
+#pragma unroll
+                for (int m = 0; m < 4; ++m) out[4 * j + m] = (static_cast<uint64_t>(hi[3 - m]) << 32) | lo[3 - m];
             }
             int32_t g[16];
             if (nv == 16) {
