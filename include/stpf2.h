@@ -345,8 +345,10 @@ stp_status stp_f2_jackknife(stp_ctx* ctx, const double* x, const int32_t* block_
 /* ---- plans: device-resident repeated extraction --------------------------------------- */
 
 /* Builds everything a request needs once (operand buffers, block layout, work list,
- * tensor maps, ploidy) so stp_plan_run only launches kernels. The request's genotype
- * records must be on the device; the plan keeps no reference to host arrays. */
+ * ploidy) so stp_plan_run only launches kernels. The request's genotype records must be on
+ * the device; the plan keeps no reference to host arrays. A plan uses its context's stream
+ * and workspaces: destroy every plan of a context before the context (stp_destroy does
+ * not free them). */
 stp_plan* stp_plan_create(stp_ctx* ctx, const stp_f2_request* req, stp_status* status);
 /* Enqueues decode + contraction on `stream` (a cudaStream_t, NULL = the context stream);
  * d_f2/d_vpair are device buffers of P*P*n_block doubles. Asynchronous. */

@@ -10,6 +10,7 @@ device the calls raise, as the reference does.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -91,6 +92,7 @@ class Context:
         if not self._h:
             raise L.StpError(st.value, L.lib().stp_last_error().decode())
         self.device = device
+        self._plans = weakref.WeakSet()  # live plans, closed before the context
         from steppecu_b200.autotune import load_mask
 
         mask = load_mask()  # the measured tile-class table, when one is committed
@@ -98,7 +100,11 @@ class Context:
             self.set_tile_classes(mask)
 
     def close(self):
+        """Destroys the context, after every plan still open on it (a plan uses the
+        context's stream and workspaces, so the C API frees plans first)."""
         if getattr(self, "_h", None):
+            for plan in list(getattr(self, "_plans", ())):
+                plan.close()
             L.lib().stp_destroy(self._h)
             self._h = None
 
@@ -471,10 +477,13 @@ class Plan:
 
     def __init__(self, ctx: Context, req: L.F2Request):
         st = C.c_int(0)
+        if not ctx._h:
+            raise ValueError("the context is closed")
         self._ctx = ctx
         self._h = L.lib().stp_plan_create(ctx._h, C.byref(req), C.byref(st))
         if not self._h:
             raise L.StpError(st.value, L.lib().stp_last_error().decode())
+        ctx._plans.add(self)
         self.P = req.n_pop
         self.n_block = req.n_block
 

@@ -29,17 +29,18 @@
 // 7e-10 on T; a block mean over K SNPs averages independent roundings (~1e-10 / sqrt(K)).
 //
 // vpair_fx_kernel runs first over the same items: the exact both-present counts
-// m_i . m_j (one kind::i8 MMA per 32 SNPs on the M tiles, 64 m on both sides, so 4096 per
-// SNP; 256 SNPs per stage, a ring of four TMEM accumulators, at most 524,032
-// SNPs per accumulation) written as one compact int32 128x128 tile per item, which the f2
-// epilogue reads for its divide and its vpair stores. (The four f2
-// accumulators fill TMEM's 512 columns, so the counts cannot share the f2 kernel.)
+// m_i . m_j (kind::i8 MMAs on the M tiles, 64 m on both sides, so 4096 per SNP; two items
+// of one row tile per unit where the next column tile follows; 128 SNPs per stage, a ring
+// of two 256-column TMEM accumulators, at most 524,032 SNPs per accumulation) written as
+// one compact int32 128x128 tile per item, which the f2 epilogue reads for its divide and
+// its vpair stores. (The four f2 accumulators fill TMEM's 512 columns, so the counts
+// cannot share the f2 kernel.)
 //
 //   f2_fx_kernel:   warp 0 producer (a 32 KiB image and a 4 KiB M copy per stage side, no
 //                   tensor maps, no multicast), warp 1 TMEM owner + single-thread MMA issuer, warps 2-17
 //                   epilogue (four per TMEM lane quarter, 32 tile columns each).
-//   vpair_fx_kernel: warp 0 producer (32 KiB per stage side), warp 1 issuer, warps 2-9
-//                   epilogue (two per lane quarter, 64 columns each).
+//   vpair_fx_kernel: warp 0 producer (16 KiB of A and of each column tile per stage),
+//                   warp 1 issuer, warps 2-9 epilogue (two per lane quarter, one item each).
 // Every wait is bounded (FxTuning::timeout_ns); on expiry the kernel raises an error flag
 // the host turns into STP_DEVICE_TIMEOUT, lets its copies and MMAs finish, frees TMEM and
 // returns.
@@ -73,18 +74,19 @@ constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kCtlBytes = 256;
 
 // ---- vpair kernel constants ----
-constexpr int kVpChunks = 8;  // 32-SNP chunks per stage
-constexpr uint32_t kVpSide = kVpChunks * static_cast<uint32_t>(kTile8Bytes);  // 32 KiB
-constexpr uint32_t kVpStageBytes = 2 * kVpSide;
-constexpr int kVpStages = 3;
-constexpr int kVpAcc = 4;  // TMEM ring of 128-column accumulators
+constexpr int kVpChunks = 4;  // 32-SNP chunks per stage
+constexpr uint32_t kVpASide = kVpChunks * static_cast<uint32_t>(kTile8Bytes);  // 16 KiB
+constexpr uint32_t kVpStageBytes = 3 * kVpASide;  // A, then the two column tiles
+constexpr int kVpStages = 4;
+constexpr int kVpAcc = 2;  // TMEM ring of 256-column accumulators
+constexpr uint32_t kVpAccCols = 2 * kTile;
 constexpr int kVpEpiWarps = 8;
 constexpr int kVpThreads = 32 * (2 + kVpEpiWarps);  // 320
-constexpr int kVpCols = 4 * kTile / kVpEpiWarps;   // 64
 // 32-SNP chunks per accumulation: M = 64 on both sides adds 4096 per both-present SNP, so
 // an int32 accumulator holds 524,032 SNPs (a multiple of the stage's eight chunks).
 constexpr int kVpPartChunks = 16376;
 static_assert(4096ll * 32 * kVpPartChunks < (1ll << 31) && kVpPartChunks % kVpChunks == 0, "vpair part");
+static_assert(kVpStages >= kStages && kVpAcc * kVpAccCols <= 512, "barrier and TMEM slots");
 
 struct FxArgs {
     const uint8_t* images;   // (row tile t, chunk c) image at (t * n_ck + c) * kFxImageBytes
@@ -100,7 +102,10 @@ struct FxArgs {
     const double* rcp;  // rcp[k] = 1/k, k = 0..rcp_max (rcp[0] = 0)
     int rcp_max;
     int* err;
-    int* next_item;  // work-item counter, zero at launch
+    int* next_item;  // work-item (f2) or unit (vpair) counter, zero at launch
+    const int32_t* units;  // vpair units: first item of each, as an index past unit_base
+    int n_units;
+    int unit_base;
     int b_base;      // block id whose slab starts the output buffers
     uint32_t idesc;
     unsigned long long timeout_ns;
@@ -279,11 +284,11 @@ __device__ void fx_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t t
                 // N = 128 + n on two adjacent B planes fills two adjacent weights at once
                 // (columns 0..n-1 from the first plane, 128.. from the second): 12 MMAs per
                 // stage for the 18 digit products, A kept in the collector buffer across the
-                // two MMAs of one shape that share it.
+                // two MMAs that share it (X3, X2 and M: nine A reads per stage).
                 mma_i8_c<C::kFill>(V3, dA(3), dB(0), id2, f);     // X3 [X0;X1] -> V3,V4
                 mma_i8_c<C::kLastUse>(V5, dA(3), dB(2), id2, f);  // X3 [X2;X3] -> V5,V6
-                mma_i8(V3, dA(2), dB(1), id2, 1u);                // X2 [X1;X2] -> V3,V4
-                mma_i8(V5, dA(2), dB(3), id, 1u);                 // X2 X3      -> V5
+                mma_i8_c<C::kFill>(V3, dA(2), dB(1), id, 1u);     // X2 X1      -> V3
+                mma_i8_c<C::kLastUse>(V4, dA(2), dB(2), id2, 1u); // X2 [X2;X3] -> V4,V5
                 mma_i8(V3, dA(1), dB(2), id2, 1u);                // X1 [X2;X3] -> V3,V4
                 mma_i8(V3, dA(0), dB(3), id, 1u);                 // X0 X3      -> V3
                 // M(i) E_w(j) on the stacked E planes, and E_w(i) M(j): tiles 4..7 are
@@ -554,17 +559,68 @@ f2_fx_kernel(const __grid_constant__ FxArgs a) {
 constexpr size_t kFxSmemBytes = kStages * kStageBytes + kCtlBytes + 1024;
 
 // ============================== vpair kernel ==============================================
+//
+// A unit is one work item, or two when the second is the next column tile of the first's
+// row (vpair_pairs_with): the A tile is copied once for both, and per 32-SNP chunk two MMAs
+// share it from the collector buffer, one per column tile, into the two 128-column halves
+// of one accumulator. A stage holds A, then the first column tile's chunks, then the
+// second's, each region one bulk copy of consecutive chunks (a partial side: one copy of
+// its valid 8-row groups per chunk). A diagonal unit reads A from the first B region. A
+// paired unit's row tile and first column tile are whole (a later column tile exists), so
+// only its second column tile can be a partial side.
+
+// The unit's second item, or -1.
+__device__ __forceinline__ int vp_second(const FxArgs& a, int it) {
+    return it + 1 < a.n_items && vpair_pairs_with(a.items[it], a.items[it + 1]) ? it + 1 : -1;
+}
+
+// Units in list order from the vpair counter, the next one claimed while this one streams
+// (u_next: the claim made one unit earlier); the ring carries the unit's first item.
+__device__ __forceinline__ int take_unit(const FxArgs& a, FxCtl* ctl, uint32_t gi, int& u_next, bool& ok) {
+    const int slot = static_cast<int>(gi % kItemRing);
+    ok = waitb(&ctl->item_empty[slot], ((gi / kItemRing) & 1u) ^ 1u, ctl, a);
+    if (!ok) return -1;
+    const int u = u_next;
+    const int it = u < a.n_units ? __ldg(a.units + u) - a.unit_base : -1;
+    *reinterpret_cast<volatile int*>(&ctl->item_idx[slot]) = it;
+    mbar_arrive(&ctl->item_full[slot]);
+    if (it >= 0) u_next = atomicAdd(a.next_item, 1);
+    return it;
+}
+
+// MMA shape for column tile t: its populations rounded up to 16.
+template <bool kGrouped>
+__device__ __forceinline__ uint32_t vp_idesc(const FxArgs& a, const BlockInfo& bi, int t) {
+    const int P = kGrouped ? a.groups[bi.grp].P : a.P;
+    const int cols = min(kTile, P - t * kTile);
+    const uint32_t n = static_cast<uint32_t>((cols + 15) & ~15);
+    return (a.idesc & ~(0x3Fu << 17)) | ((n >> 3) << 17);
+}
+
+// Bytes per chunk of a region with g valid 8-row groups (0: a region not copied).
+__device__ __forceinline__ uint32_t chunk_bytes(uint32_t g) { return g == 16 ? 4096u : g * 256u; }
+
+// n consecutive 4 KiB chunks of one M tile into a stage region: one copy when whole, the
+// valid groups of each chunk when partial, nothing when g = 0.
+__device__ __forceinline__ void vp_copy_region(uint8_t* dst, const uint8_t* src, uint32_t g, int n,
+                                               unsigned long long* bar) {
+    if (g == 16) bulk_load(dst, src, static_cast<uint32_t>(n) * 4096u, bar);
+    else
+        for (int j = 0; j < n && g != 0; ++j) bulk_load(dst + j * 4096, src + j * 4096, g * 256u, bar);
+}
 
 template <bool kGrouped>
 __device__ void vp_producer(const FxArgs& a, uint8_t* smem, FxCtl* ctl) {
     uint32_t g = 0;
+    int u_next = atomicAdd(a.next_item, 1);
     for (uint32_t gi = 0;; ++gi) {
         bool ok = true;
-        const int it = take_item(a, ctl, gi, ok);
+        const int it = take_unit(a, ctl, gi, u_next, ok);
         if (!ok) goto abort;
         if (it < 0) break;
         {
             const WorkItem w = a.items[it];
+            const bool pair = vp_second(a, it) >= 0;
             const BlockInfo bi = a.blocks[w.blk];
             const int nch = stages_of(bi.k, kStageK);
             const bool diag = w.ti == w.tj;
@@ -574,31 +630,24 @@ __device__ void vp_producer(const FxArgs& a, uint8_t* smem, FxCtl* ctl) {
                 mt = a.groups[bi.grp].mplanes;
                 n_ck = a.groups[bi.grp].n_ck;
             }
-            // The M tiles of up to eight consecutive chunks: one copy per side, or per chunk the
-            // valid 8-row groups of a partial side (feed_groups).
+            // Per chunk: the valid 8-row groups of a partial side (feed_groups), else 4 KiB.
             const int P = kGrouped ? a.groups[bi.grp].P : a.P;
-            const uint32_t gA = feed_groups(a, min(kTile, P - w.ti * kTile));
+            const uint32_t gA = diag ? 0u : feed_groups(a, min(kTile, P - w.ti * kTile));
             const uint32_t gB = feed_groups(a, min(kTile, P - w.tj * kTile));
+            const uint32_t gF = pair ? feed_groups(a, min(kTile, P - (w.tj + 1) * kTile)) : 0u;
             for (int c0 = 0; c0 < nch; c0 += kVpChunks, ++g) {
                 const int n = min(kVpChunks, nch - c0);
                 const int slot = static_cast<int>(g % kVpStages);
                 if (!waitb(&ctl->empty[slot], ((g / kVpStages) & 1u) ^ 1u, ctl, a)) goto abort;
-                uint8_t* sb = smem + slot * kVpStageBytes;
-                const uint32_t bA = static_cast<uint32_t>(n) * (gA == 16 ? 4096u : gA * 256u);
-                const uint32_t bB = static_cast<uint32_t>(n) * (gB == 16 ? 4096u : gB * 256u);
-                mbar_expect_tx(&ctl->full[slot], diag ? bA : bA + bB);
+                uint8_t* sa = smem + slot * kVpStageBytes;
+                unsigned long long* bar = &ctl->full[slot];
+                mbar_expect_tx(bar, static_cast<uint32_t>(n) * (chunk_bytes(gA) + chunk_bytes(gB) + chunk_bytes(gF)));
                 const int64_t chunk = bi.col / kStageK + c0;
                 const uint8_t* si = mt + (static_cast<int64_t>(w.ti) * n_ck + chunk) * kTile8Bytes;
                 const uint8_t* sj = mt + (static_cast<int64_t>(w.tj) * n_ck + chunk) * kTile8Bytes;
-                if (gA == 16) bulk_load(sb, si, bA, &ctl->full[slot]);
-                else
-                    for (int j = 0; j < n; ++j) bulk_load(sb + j * 4096, si + j * 4096, gA * 256u, &ctl->full[slot]);
-                if (!diag) {
-                    if (gB == 16) bulk_load(sb + kVpSide, sj, bB, &ctl->full[slot]);
-                    else
-                        for (int j = 0; j < n; ++j)
-                            bulk_load(sb + kVpSide + j * 4096, sj + j * 4096, gB * 256u, &ctl->full[slot]);
-                }
+                vp_copy_region(sa, si, gA, n, bar);
+                vp_copy_region(sa + kVpASide, sj, gB, n, bar);
+                vp_copy_region(sa + 2 * kVpASide, sj + n_ck * kTile8Bytes, gF, n, bar);
             }
         }
     }
@@ -618,7 +667,9 @@ __device__ void vp_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t t
         const BlockInfo bi = a.blocks[w.blk];
         const int nch = stages_of(bi.k, kStageK);
         if (nch == 0) continue;
-        const uint32_t id = idesc_for<kGrouped>(a, w, bi);
+        const bool pair = vp_second(a, it) >= 0;
+        const uint32_t id = vp_idesc<kGrouped>(a, bi, w.tj);
+        const uint32_t idf = pair ? vp_idesc<kGrouped>(a, bi, w.tj + 1) : 0u;
         const bool diag = w.ti == w.tj;
         // One accumulator per part of at most kVpPartChunks chunks (the int32 bound).
         for (int p0 = 0; p0 < nch; p0 += kVpPartChunks) {
@@ -626,17 +677,25 @@ __device__ void vp_issuer(const FxArgs& a, uint8_t* smem, FxCtl* ctl, uint32_t t
             const int b = static_cast<int>(n_acc % kVpAcc);
             if (!waitb(&ctl->acc_empty[b], ((n_acc / kVpAcc) & 1u) ^ 1u, ctl, a)) goto done;
             tc_fence_after();
-            const uint32_t d = tmem + static_cast<uint32_t>(b) * 128u;
+            const uint32_t d = tmem + static_cast<uint32_t>(b) * kVpAccCols;
             for (int c0 = p0; c0 < p1; c0 += kVpChunks, ++g) {
                 const int slot = static_cast<int>(g % kVpStages);
                 if (!waitb(&ctl->full[slot], (g / kVpStages) & 1u, ctl, a)) goto done;
                 tc_fence_after();
                 const uint32_t sa = smem_u32(smem + slot * kVpStageBytes);
-                const uint32_t sb = diag ? sa : sa + kVpSide;
+                const uint32_t sb = sa + kVpASide;
                 const int n = min(kVpChunks, nch - c0);
-                for (int j = 0; j < n; ++j)
-                    mma_i8(d, smem_desc(sa + static_cast<uint32_t>(j) * 4096u, 256, 6),
-                           smem_desc(sb + static_cast<uint32_t>(j) * 4096u, 256, 6), id, (c0 + j) > p0 ? 1u : 0u);
+                for (int j = 0; j < n; ++j) {
+                    const uint32_t bj = sb + static_cast<uint32_t>(j) * 4096u;
+                    const uint64_t dA = smem_desc(diag ? bj : sa + static_cast<uint32_t>(j) * 4096u, 256, 6);
+                    const uint32_t f = (c0 + j) > p0 ? 1u : 0u;
+                    if (pair) {
+                        mma_i8_c<CollectorA::kFill>(d, dA, smem_desc(bj, 256, 6), id, f);
+                        mma_i8_c<CollectorA::kLastUse>(d + kTile, dA, smem_desc(bj + kVpASide, 256, 6), idf, f);
+                    } else {
+                        mma_i8(d, dA, smem_desc(bj, 256, 6), id, f);
+                    }
+                }
                 mma_commit(&ctl->empty[slot]);
             }
             mma_commit(&ctl->acc_full[b]);
@@ -648,9 +707,11 @@ done:
     waitb(&ctl->drain, 0u, ctl, a, false);
 }
 
+// Warp (quarter q, half h): TMEM lanes 32q.., columns 128h.. of the accumulator, i.e. the
+// unit's item h (a single unit's h = 1 warps only take part in the barriers).
 __device__ void vp_epilogue(const FxArgs& a, FxCtl* ctl, uint32_t tmem, int warp, int lane) {
     const int q = warp & 3;
-    const int h = (warp - 2) >> 2;  // column half
+    const int h = (warp - 2) >> 2;
     const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
     uint32_t n_acc = 0;
     for (uint32_t gi = 0;; ++gi) {
@@ -660,7 +721,8 @@ __device__ void vp_epilogue(const FxArgs& a, FxCtl* ctl, uint32_t tmem, int warp
         if (it < 0) return;
         const int nch = stages_of(a.blocks[a.items[it].blk].k, kStageK);
         if (nch == 0) continue;  // the f2 kernel writes zeros
-        int32_t* dst = a.vpc + static_cast<int64_t>(it) * kVpTileInts + (h * kVpCols) * kTile + q * 32 + lane;
+        const int mine = h == 0 ? it : vp_second(a, it);
+        int32_t* dst = a.vpc + static_cast<int64_t>(mine) * kVpTileInts + q * 32 + lane;
         for (int p0 = 0; p0 < nch; p0 += kVpPartChunks) {
             const int b = static_cast<int>(n_acc % kVpAcc);
             bool ok = true;
@@ -668,19 +730,21 @@ __device__ void vp_epilogue(const FxArgs& a, FxCtl* ctl, uint32_t tmem, int warp
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) return;
             tc_fence_after();
+            if (mine >= 0) {
+#pragma unroll 1
+                for (int c32 = 0; c32 < kTile / 32; ++c32) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem + lane_addr + static_cast<uint32_t>(b) * kVpAccCols +
+                                  static_cast<uint32_t>(h * kTile + c32 * 32),
+                              v);
+                    tmem_wait_ld();
+                    // M = 64 on both sides: each both-present SNP adds 4096.
 #pragma unroll
-            for (int half = 0; half < kVpCols / 32; ++half) {
-                uint32_t v[32];
-                tmem_ld32(tmem + lane_addr + static_cast<uint32_t>(b) * 128u +
-                              static_cast<uint32_t>(h * kVpCols + half * 32),
-                          v);
-                tmem_wait_ld();
-                // M = 64 on both sides: each both-present SNP adds 4096.
-#pragma unroll
-                for (int c = 0; c < 32; ++c) {
-                    const int32_t cnt = static_cast<int32_t>(v[c]) >> 12;
-                    int32_t* o = dst + (half * 32 + c) * kTile;
-                    *o = p0 == 0 ? cnt : *o + cnt;
+                    for (int c = 0; c < 32; ++c) {
+                        const int32_t cnt = static_cast<int32_t>(v[c]) >> 12;
+                        int32_t* o = dst + (c32 * 32 + c) * kTile;
+                        *o = p0 == 0 ? cnt : *o + cnt;
+                    }
                 }
             }
             tc_fence_before();
@@ -757,6 +821,9 @@ void launch_fx(Ctx& c, const FxLaunch& L, cudaStream_t s) {
     a.n_ck = L.n_ck;
     a.items = L.items;
     a.n_items = L.n_items;
+    a.units = L.units;
+    a.n_units = L.n_units;
+    a.unit_base = L.unit_base;
     a.blocks = L.blocks;
     a.P = L.P;
     a.f2 = L.f2;
@@ -774,12 +841,14 @@ void launch_fx(Ctx& c, const FxLaunch& L, cudaStream_t s) {
     a.grp_done = L.grp_done;
     a.grp_ns = L.grp_ns;
     a.grp_items = L.grp_items;
+    if (!L.units || L.n_units <= 0) fail(STP_RUNTIME_ERROR, "fixed-point contraction without vpair units");
     const int grid = std::min(c.sm_count, L.n_items);
-    // Two work-item counters: one per kernel.
+    // Two work counters: vpair units, then f2 items.
     STPF2_CUDA(cudaMemsetAsync(L.counters, 0, 2 * sizeof(int), s));
     a.next_item = L.counters;
-    if (L.groups) vpair_fx_kernel<true><<<grid, kVpThreads, kVpSmemBytes, s>>>(a);
-    else vpair_fx_kernel<false><<<grid, kVpThreads, kVpSmemBytes, s>>>(a);
+    const int vp_grid = std::min(c.sm_count, L.n_units);
+    if (L.groups) vpair_fx_kernel<true><<<vp_grid, kVpThreads, kVpSmemBytes, s>>>(a);
+    else vpair_fx_kernel<false><<<vp_grid, kVpThreads, kVpSmemBytes, s>>>(a);
     STPF2_CUDA(cudaGetLastError());
     c.launches++;
     a.next_item = L.counters + 1;

@@ -530,8 +530,11 @@ struct UmmaPlan {
     int64_t n_ck = 0;
     DevBuf items, blocks, err, rcp, block_items, counter;
     DevBuf vpc;  // FX: compact vpair tiles, one per item of the largest launch
+    DevBuf units, block_units;  // FX: vpair units of items and of block_items
     std::vector<int> block_item_off;  // per block: its tile pairs in block_items
+    std::vector<int> block_unit_off;  // per block: its vpair units in block_units
     int n_items = 0;
+    int n_units = 0;
     int rcp_max = 0;
     int P = 0;
     OpFmt fmt = OpFmt::BF16;
@@ -576,6 +579,22 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
     p->rcp_max = max_k;
     p->rcp.reserve(rcp.size() * sizeof(double));
     STPF2_CUDA(cudaMemcpyAsync(p->rcp.ptr, rcp.data(), rcp.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    std::vector<int32_t> units, block_units;
+    if (op.fmt == OpFmt::FX) {
+        units = make_vpair_units(items);
+        block_units = make_vpair_units(by_block);
+        p->n_units = static_cast<int>(units.size());
+        // Units never span two blocks, so each block's units are a run of block_units.
+        p->block_unit_off.assign(L.blocks.size() + 1, 0);
+        for (int32_t u : block_units) p->block_unit_off[static_cast<size_t>(by_block[u].blk) + 1]++;
+        for (size_t b = 0; b < L.blocks.size(); ++b) p->block_unit_off[b + 1] += p->block_unit_off[b];
+        p->units.reserve(std::max<size_t>(units.size() * sizeof(int32_t), 16));
+        p->block_units.reserve(std::max<size_t>(block_units.size() * sizeof(int32_t), 16));
+        STPF2_CUDA(cudaMemcpyAsync(p->units.ptr, units.data(), units.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                   c.stream));
+        STPF2_CUDA(cudaMemcpyAsync(p->block_units.ptr, block_units.data(), block_units.size() * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, c.stream));
+    }
     STPF2_CUDA(cudaStreamSynchronize(c.stream));  // the host tables above go out of scope
 
     if (op.n_rt <= 0 || op.n_ck <= 0) fail(STP_INVALID_ARGUMENT, "tensor-core contraction needs tiled planes");
@@ -594,14 +613,16 @@ UmmaPlan* umma_plan_create(Ctx& c, const OperandPlanes& op, const BlockLayout& L
 void umma_plan_destroy(UmmaPlan* p) { delete p; }
 
 void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, double* f2, double* vpair,
-                       cudaStream_t s, int b_base = 0);
+                       cudaStream_t s, int b_base = 0, int b0 = -1, int b1 = -1);
 
 void launch_f2_umma(Ctx& c, UmmaPlan* p, double* f2, double* vpair, cudaStream_t s, bool per_block) {
     if (!p || p->n_items <= 0) return;
     if (per_block) {  // comparison form: one launch per jackknife block
         for (size_t b = 0; b + 1 < p->block_item_off.size(); ++b) {
             const int n = p->block_item_off[b + 1] - p->block_item_off[b];
-            if (n > 0) launch_umma_items(c, p, p->block_items.as<WorkItem>() + p->block_item_off[b], n, f2, vpair, s);
+            if (n > 0)
+                launch_umma_items(c, p, p->block_items.as<WorkItem>() + p->block_item_off[b], n, f2, vpair, s, 0,
+                                  static_cast<int>(b), static_cast<int>(b) + 1);
         }
         return;
     }
@@ -614,11 +635,13 @@ void launch_f2_umma_blocks(Ctx& c, UmmaPlan* p, int b0, int b1, double* f2, doub
     const int n = p->block_item_off[static_cast<size_t>(b1)] - p->block_item_off[static_cast<size_t>(b0)];
     if (n > 0)
         launch_umma_items(c, p, p->block_items.as<WorkItem>() + p->block_item_off[static_cast<size_t>(b0)], n, f2, vpair, s,
-                          rebase ? b0 : 0);
+                          rebase ? b0 : 0, b0, b1);
 }
 
+// b0 < 0: items is the whole costliest-first list; otherwise the block_items of blocks
+// b0..b1-1.
 void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, double* f2, double* vpair,
-                       cudaStream_t s, int b_base) {
+                       cudaStream_t s, int b_base, int b0, int b1) {
     if (p->fmt == OpFmt::FX) {
         FxLaunch L;
         L.images = p->images;
@@ -626,6 +649,15 @@ void launch_umma_items(Ctx& c, UmmaPlan* p, const WorkItem* items, int n_items, 
         L.n_ck = p->n_ck;
         L.items = items;
         L.n_items = n_items;
+        if (b0 < 0) {
+            L.units = p->units.as<int32_t>();
+            L.n_units = p->n_units;
+        } else {
+            const int u0 = p->block_unit_off[static_cast<size_t>(b0)], u1 = p->block_unit_off[static_cast<size_t>(b1)];
+            L.units = p->block_units.as<int32_t>() + u0;
+            L.n_units = u1 - u0;
+            L.unit_base = p->block_item_off[static_cast<size_t>(b0)];
+        }
         L.blocks = p->blocks.as<BlockInfo>();
         L.P = p->P;
         L.f2 = f2;
@@ -722,12 +754,14 @@ void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stage
     const size_t o_info = pk.add(info.size() * sizeof(GroupInfo));
     const size_t o_rcp = pk.add(rcp.size() * sizeof(double));
     const size_t o_nitems = pk.add(n_items.size() * sizeof(int));
+    const bool fx = fmt == OpFmt::FX;
+    const std::vector<int32_t> units = fx ? make_vpair_units(items) : std::vector<int32_t>();
+    const size_t o_units = pk.add(units.size() * sizeof(int32_t));
     const size_t staged = pk.end;
     const size_t o_done = pk.add(static_cast<size_t>(G) * sizeof(int));
     const size_t o_ns = pk.add(static_cast<size_t>(G) * sizeof(unsigned long long));
     const size_t o_err = pk.add(16);
     const size_t o_counter = pk.add(16);
-    const bool fx = fmt == OpFmt::FX;
     if (fx) c.ws_vpc.reserve(fx_vpc_bytes(static_cast<int>(items.size())));
     c.pin_items.reserve(staged);
     c.ws_items.reserve(pk.end);
@@ -737,6 +771,7 @@ void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stage
     std::memcpy(h + o_info, info.data(), info.size() * sizeof(GroupInfo));
     std::memcpy(h + o_rcp, rcp.data(), rcp.size() * sizeof(double));
     std::memcpy(h + o_nitems, n_items.data(), n_items.size() * sizeof(int));
+    if (!units.empty()) std::memcpy(h + o_units, units.data(), units.size() * sizeof(int32_t));
     uint8_t* d = c.ws_items.as<uint8_t>();
     STPF2_CUDA(cudaMemcpyAsync(d, h, staged, cudaMemcpyHostToDevice, s));
     STPF2_CUDA(cudaMemsetAsync(d + staged, 0, pk.end - staged, s));
@@ -751,6 +786,8 @@ void launch_f2_umma_grouped(Ctx& c, OpFmt fmt, double scale_inv, int chunk_stage
         L.vpair = info[ord[0]].vpair;
         L.items = reinterpret_cast<const WorkItem*>(d + o_items);
         L.n_items = static_cast<int>(items.size());
+        L.units = reinterpret_cast<const int32_t*>(d + o_units);
+        L.n_units = static_cast<int>(units.size());
         L.blocks = reinterpret_cast<const BlockInfo*>(d + o_blocks);
         L.vpc = c.ws_vpc.as<int32_t>();
         L.rcp = reinterpret_cast<const double*>(d + o_rcp);

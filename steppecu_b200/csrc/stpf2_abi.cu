@@ -123,6 +123,16 @@ std::vector<WorkItem> make_work_items(const BlockLayout& L, int P, int tile) {
     return items;
 }
 
+std::vector<int32_t> make_vpair_units(const std::vector<WorkItem>& items) {
+    std::vector<int32_t> u;
+    u.reserve(items.size());
+    for (size_t k = 0; k < items.size(); ++k) {
+        u.push_back(static_cast<int32_t>(k));
+        if (k + 1 < items.size() && vpair_pairs_with(items[k], items[k + 1])) ++k;
+    }
+    return u;
+}
+
 size_t operand_plane_bytes(OpFmt f, int P, int64_t ld) {
     if (f == OpFmt::F32) {
         const size_t pl = static_cast<size_t>(P) * static_cast<size_t>(ld);

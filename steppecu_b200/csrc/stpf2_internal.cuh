@@ -193,6 +193,15 @@ struct WorkItem {
 // Tile pairs of every block, costliest (largest k) first.
 std::vector<WorkItem> make_work_items(const BlockLayout& L, int P, int tile);
 
+// The fixed-point vpair kernel counts two items in one unit when the second is the next
+// column tile of the first's row tile in the same block (one MMA on the stacked B tiles).
+__host__ __device__ inline bool vpair_pairs_with(const WorkItem& x, const WorkItem& y) {
+    return y.blk == x.blk && y.ti == x.ti && y.tj == x.tj + 1;
+}
+// Its units over an item list: the index of each unit's first item, greedily left to right
+// (item k takes item k + 1 when vpair_pairs_with holds), the rule the kernel re-applies.
+std::vector<int32_t> make_vpair_units(const std::vector<WorkItem>& items);
+
 // ---- operand planes --------------------------------------------------------------------
 
 // Operand formats the decode/feeder kernels emit, one per contraction arithmetic.
@@ -401,6 +410,9 @@ struct FxLaunch {
     int64_t n_ck = 0;
     const WorkItem* items = nullptr;
     int n_items = 0;
+    const int32_t* units = nullptr;  // vpair units: first items, as indices past unit_base
+    int n_units = 0;
+    int unit_base = 0;
     const BlockInfo* blocks = nullptr;
     int P = 0;
     double* f2 = nullptr;

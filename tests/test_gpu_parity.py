@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import oracle
+import steppecu_b200 as sb
 from steppecu_b200 import F2Tensor, StpError, extract_f2, read_f2, synth
 from steppecu_b200.synth import write_eigenstrat
 
@@ -282,6 +283,26 @@ def test_plan_device_resident_matches_one_shot(ctx, c1):
     one = ctx.extract_blocks(p.records_numpy(), p.n_ind, sel, po, p.block_id, p.n_block, precision=MODES[-1])
     assert np.array_equal(f2.cpu().numpy(), one.f2) and np.array_equal(vp.cpu().numpy(), one.vpair)
     assert plan.launches >= 2
+
+
+def test_closing_the_context_closes_its_plans(c1):
+    """A plan still open when its context closes is destroyed first (it uses the context's
+    stream and workspaces); running it afterwards is refused on the host, and so is a new
+    plan on the closed context."""
+    import torch
+
+    p, sel, po, _, _ = c1
+    rec = torch.as_tensor(p.records_numpy()).cuda()
+    c = sb.Context(0)
+    plan = c.plan(rec, p.n_ind, sel, po, p.block_id, p.n_block, precision="fixed_i8")
+    c.close()
+    assert plan._h is None
+    f2 = torch.zeros(p.n_pop ** 2 * p.n_block, dtype=torch.float64, device="cuda")
+    with pytest.raises(StpError, match="invalid_argument"):
+        plan.run(rec, f2, torch.zeros_like(f2))
+    del plan
+    with pytest.raises(ValueError, match="closed"):
+        c.plan(rec, p.n_ind, sel, po, p.block_id, p.n_block)
 
 
 @pytest.mark.parametrize("mode", [TC_DEFAULT, "fixed_i8"])
