@@ -317,7 +317,11 @@ constexpr int kSliceWords = 64;                      // 1024 samples per staged 
 constexpr int kSliceBytes = kSliceWords * 4;
 constexpr int kRowStride = kSliceWords + 4;          // words per staged record row (16-byte rows)
 constexpr int kStagedWords = 4 * kTileCols * kRowStride + 32;
-constexpr size_t kTransSmemBytes = 2 * kStagedWords * sizeof(uint32_t);
+constexpr int kQuadRows = 4 * kTileCols;  // record rows of a quad
+// Two staging buffers, then the quad's row offsets (int64 each).
+constexpr size_t kTransSmemBytes = 2 * kStagedWords * sizeof(uint32_t) + kQuadRows * sizeof(int64_t);
+static_assert((2 * kStagedWords * sizeof(uint32_t)) % 8 == 0, "row table alignment");
+static_assert(kTransThreads >= kQuadRows && (kQuadRows * (kSliceBytes / 16)) % kTransThreads == 0, "staging split");
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
@@ -331,38 +335,50 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
                  : "memory");
 }
 
+// Byte offset of each of the quad's 128 record rows (row sub*32 + r: SNP r of tile 4q+sub,
+// through the row map when rows are kept), or -1 for a row past its tile's SNPs or past the
+// last tile. Computed once per CTA; every slice's staging reads it.
+__device__ __forceinline__ void quad_rows(int64_t* rows, uint64_t pitch, const TileInfo* __restrict__ tiles,
+                                          int64_t n_tiles, int64_t q, const int32_t* __restrict__ row_map) {
+    const int row = threadIdx.x;
+    if (row >= kQuadRows) return;
+    const int sub = row / kTileCols, r = row % kTileCols;
+    const int64_t t = 4 * q + sub;
+    int64_t off = -1;
+    if (t < n_tiles) {
+        const TileInfo ti = tiles[t];
+        if (r < ti.nvalid) {
+            const int64_t snp = static_cast<int64_t>(ti.snp0) + r;
+            off = static_cast<int64_t>(row_map ? __ldg(row_map + snp) : snp) * static_cast<int64_t>(pitch);
+        }
+    }
+    rows[row] = off;
+}
+
 // Stages slice `slice` of the quad's 128 records into buf: row (sub, r) at word
 // (sub*32 + r)*kRowStride + sub*8 (the sub*8 skew keeps the threads of one warp on
-// distinct banks when they read it back); bytes past the record, rows past the tile's
-// SNPs and tiles past the last hold code 3 (missing). kVec16: records and pitch are
-// 16-byte aligned (16-byte copies); otherwise 4-byte aligned (4-byte copies, so a host
-// panel keeps its own pitch on the device).
+// distinct banks when they read it back); bytes past the record and rows without a record
+// (rows[row] < 0) hold code 3 (missing). Thread t copies 16-byte column t % 16 of rows
+// t / 16 + 16 i. kVec16: records and pitch are 16-byte aligned (16-byte copies); otherwise
+// 4-byte aligned (4-byte copies, so a host panel keeps its own pitch on the device).
 template <bool kVec16>
 __device__ __forceinline__ void stage_slice(uint32_t* buf, const uint8_t* __restrict__ records, uint64_t pitch,
-                                            const TileInfo* __restrict__ tiles, int64_t n_tiles, int64_t q,
-                                            int64_t slice, const int32_t* __restrict__ row_map) {
-    const uint64_t byte0 = static_cast<uint64_t>(slice) * kSliceBytes;
-    for (int c = threadIdx.x; c < 4 * kTileCols * (kSliceBytes / 16); c += blockDim.x) {
-        const int row = c / (kSliceBytes / 16), k = c % (kSliceBytes / 16);
-        const int sub = row / kTileCols, r = row % kTileCols;
-        const int64_t t = 4 * q + sub;
-        uint32_t* d = buf + (sub * kTileCols + r) * kRowStride + sub * 8 + k * 4;
-        const uint64_t b = byte0 + static_cast<uint64_t>(k) * 16;
-        const uint8_t* src = nullptr;
-        if (t < n_tiles) {
-            const TileInfo ti = tiles[t];
-            if (r < ti.nvalid) {
-                const int64_t snp = static_cast<int64_t>(ti.snp0) + r;  // kept SNP -> its record row
-                src = records + static_cast<int64_t>(row_map ? __ldg(row_map + snp) : snp) * pitch;
-            }
-        }
+                                            const int64_t* rows, int64_t slice) {
+    constexpr int kCols16 = kSliceBytes / 16;
+    const int k = threadIdx.x % kCols16;
+    const uint64_t b = static_cast<uint64_t>(slice) * kSliceBytes + static_cast<uint64_t>(k) * 16;
+#pragma unroll
+    for (int i = 0; i < kQuadRows * kCols16 / kTransThreads; ++i) {
+        const int row = threadIdx.x / kCols16 + i * (kTransThreads / kCols16);
+        uint32_t* d = buf + row * kRowStride + (row / kTileCols) * 8 + k * 4;
+        const int64_t off = rows[row];
         if constexpr (kVec16) {
-            if (src && b < pitch) cp_async16(d, src + b);
+            if (off >= 0 && b < pitch) cp_async16(d, records + off + b);
             else *reinterpret_cast<uint4*>(d) = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
         } else {
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
-                if (src && b + 4 * w < pitch) cp_async4(d + w, src + b + 4 * w);
+                if (off >= 0 && b + 4 * w < pitch) cp_async4(d + w, records + off + b + 4 * w);
                 else d[w] = 0xFFFFFFFFu;
             }
         }
@@ -386,12 +402,14 @@ transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t
     extern __shared__ __align__(16) uint32_t srec_all[];
     const int64_t q = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    stage_slice<kVec16>(srec_all, records, pitch, tiles, n_tiles, q, 0, row_map);
+    int64_t* rows = reinterpret_cast<int64_t*>(srec_all + 2 * kStagedWords);
+    quad_rows(rows, pitch, tiles, n_tiles, q, row_map);
+    __syncthreads();
+    stage_slice<kVec16>(srec_all, records, pitch, rows, 0);
     for (int64_t slice = 0; slice < n_slices; ++slice) {
         uint32_t* srec = srec_all + (slice & 1) * kStagedWords;
         if (slice + 1 < n_slices) {
-            stage_slice<kVec16>(srec_all + ((slice + 1) & 1) * kStagedWords, records, pitch, tiles, n_tiles, q, slice + 1,
-                                row_map);
+            stage_slice<kVec16>(srec_all + ((slice + 1) & 1) * kStagedWords, records, pitch, rows, slice + 1);
             asm volatile("cp.async.wait_group 1;" ::: "memory");
         } else {
             asm volatile("cp.async.wait_group 0;" ::: "memory");
