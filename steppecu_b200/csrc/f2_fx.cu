@@ -83,7 +83,7 @@ constexpr uint32_t kVpAccCols = 2 * kTile;
 constexpr int kVpEpiWarps = 8;
 constexpr int kVpThreads = 32 * (2 + kVpEpiWarps);  // 320
 // 32-SNP chunks per accumulation: M = 64 on both sides adds 4096 per both-present SNP, so
-// an int32 accumulator holds 524,032 SNPs (a multiple of the stage's eight chunks).
+// an int32 accumulator holds 524,032 SNPs (a whole number of stages).
 constexpr int kVpPartChunks = 16376;
 static_assert(4096ll * 32 * kVpPartChunks < (1ll << 31) && kVpPartChunks % kVpChunks == 0, "vpair part");
 static_assert(kVpStages >= kStages && kVpAcc * kVpAccCols <= 512, "barrier and TMEM slots");
