@@ -408,13 +408,12 @@ transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t
     stage_slice<kVec16>(srec_all, records, pitch, rows, 0);
     for (int64_t slice = 0; slice < n_slices; ++slice) {
         uint32_t* srec = srec_all + (slice & 1) * kStagedWords;
-        if (slice + 1 < n_slices) {
-            stage_slice<kVec16>(srec_all + ((slice + 1) & 1) * kStagedWords, records, pitch, rows, slice + 1);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-        }
+        // One barrier per slice: after it every thread's copies of this slice have landed and
+        // every thread is done with the previous slice, whose buffer the next slice refills.
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
         __syncthreads();
+        if (slice + 1 < n_slices)
+            stage_slice<kVec16>(srec_all + ((slice + 1) & 1) * kStagedWords, records, pitch, rows, slice + 1);
 
         if (slice == 0 && warp < 4) {
             const int sub = warp;
@@ -484,7 +483,6 @@ transpose_pa_kernel(const uint8_t* __restrict__ records, uint64_t pitch, int64_t
             for (int m = 0; m < 16; ++m)
                 if (g[m] >= 0) canon[(q * n_sel + g[m]) * 4 + sub] = out[m];
         }
-        __syncthreads();  // this buffer is restaged two slices later
     }
 }
 
