@@ -770,6 +770,9 @@ def main():
         threads = args.cpu_threads or (os.cpu_count() or 1)
         u, t, kind, desc, sample = cpu_sample(args.workload, threads, gen_device=dev, keep=True)
         cpu = {"value": u / t, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc}
+        if threads > 1:  # the same implementation on one core: one block of the same model
+            u1, t1, _, desc1 = cpu_sample(args.workload, 1, seed_rank=1, gen_device=dev)
+            cpu["single_core"] = {"value": u1 / t1, "unit": UNIT, "cores": 1, "sample": desc1}
         modes = [args.precision] + [m for m in ("fixed_i8", "split_f16", "split_f16_fine", "split_bf16", "fp32")
                                     if m != args.precision]
         precision = {"against": f"{kind} CPU f2 on the cpu_baseline sample", **precision_report(ctx, sample, modes)}
