@@ -927,8 +927,8 @@ namespace {
 // the tile image. The terms are the decode's (terms8_from_counts).
 template <OpFmt F>
 __global__ void __launch_bounds__(256)
-emit_counts_kernel(const uint32_t* __restrict__ counts, int64_t cnt_ld, const int32_t* __restrict__ upop, int P,
-                   int64_t n_tiles, const int32_t* __restrict__ col_snp, const double* __restrict__ center_snp,
+emit_counts_kernel(const uint32_t* __restrict__ counts, int64_t cnt_ld, bool vec, const int32_t* __restrict__ upop,
+                   int P, int64_t n_tiles, const int32_t* __restrict__ col_snp, const double* __restrict__ center_snp,
                    const double* __restrict__ rec_n, const double* __restrict__ rec_nm1, OperandPlanes op) {
     const int lane = threadIdx.x & 31;
     const int r = lane & 7, chunk = lane >> 3;
@@ -941,13 +941,43 @@ emit_counts_kernel(const uint32_t* __restrict__ counts, int64_t cnt_ld, const in
         if (i >= P) continue;
         const uint32_t* row = counts + static_cast<int64_t>(__ldg(upop + i)) * cnt_ld;
         const int64_t col0 = t * kTileCols + 8 * chunk;
+        // The chunk's eight SNPs (col_snp rows are 32-byte aligned, col0 a multiple of 8).
+        const int4 ca = __ldg(reinterpret_cast<const int4*>(col_snp + col0));
+        const int4 cb = __ldg(reinterpret_cast<const int4*>(col_snp + col0) + 1);
+        const int32_t sc[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
         uint32_t v[8];
-        double cen[8];
+        if (vec && sc[0] >= 0 && sc[7] == sc[0] + 7) {
+            // Eight consecutive SNPs (a chunk inside one block): three aligned 16-byte loads
+            // from the word s0 rounds down to, then the eight words from offset s0 & 3.
+            const uint4* rp = reinterpret_cast<const uint4*>(row + (sc[0] & ~3));
+            const uint4 w0 = __ldg(rp), w1 = __ldg(rp + 1), w2 = __ldg(rp + 2);
+            const uint32_t w[12] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x, w2.y, w2.z, w2.w};
+            switch (sc[0] & 3) {
+                case 0:
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int32_t s = __ldg(col_snp + col0 + c);
-            v[c] = s >= 0 ? __ldg(row + s) : 0u;
-            if constexpr (F != OpFmt::FX) cen[c] = s >= 0 ? __ldg(center_snp + s) : 0.5;  // the fixed point needs none
+                    for (int c = 0; c < 8; ++c) v[c] = w[c];
+                    break;
+                case 1:
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) v[c] = w[c + 1];
+                    break;
+                case 2:
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) v[c] = w[c + 2];
+                    break;
+                default:
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) v[c] = w[c + 3];
+                    break;
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) v[c] = sc[c] >= 0 ? __ldg(row + sc[c]) : 0u;
+        }
+        double cen[8];
+        if constexpr (F != OpFmt::FX) {  // the fixed point needs no centre
+#pragma unroll
+            for (int c = 0; c < 8; ++c) cen[c] = sc[c] >= 0 ? __ldg(center_snp + sc[c]) : 0.5;
         }
         if constexpr (F == OpFmt::FX)
             emit8_fx(op, i, col0, fx_terms8_from_counts(v, rec_n, rec_nm1, op.fx_table, op.fx_table_ld));
@@ -1034,18 +1064,20 @@ void launch_fx_table(Ctx& c, const double* rec_n, const double* rec_nm1, int64_t
     c.launches++;
 }
 
-void launch_emit_counts(Ctx& c, const uint32_t* counts, int64_t cnt_ld, const int32_t* upop, int P, int64_t n_tiles,
+void launch_emit_counts(Ctx& c, const uint32_t* counts, int64_t cnt_ld, int64_t n_snp, const int32_t* upop, int P, int64_t n_tiles,
                         const int32_t* col_snp, const double* center_snp, const double* rec_n, const double* rec_nm1,
                         const OperandPlanes& op, cudaStream_t s) {
     if (P <= 0 || n_tiles <= 0) return;
     const int64_t units = (P + 7) / 8 * n_tiles;
     const int64_t cap = static_cast<int64_t>(c.sm_count) * 16;  // 16 CTAs of 8 warps per SM, grid-stride beyond
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((units + 7) / 8, cap)));
+    if (reinterpret_cast<uintptr_t>(col_snp) % 32 != 0) fail(STP_RUNTIME_ERROR, "emission: column map not 32-byte aligned");
+    const bool vec = cnt_ld % 4 == 0 && cnt_ld >= n_snp + 4 && reinterpret_cast<uintptr_t>(counts) % 16 == 0;
     switch (op.fmt) {
-        case OpFmt::F32: emit_counts_kernel<OpFmt::F32><<<grid, 256, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
-        case OpFmt::BF16: emit_counts_kernel<OpFmt::BF16><<<grid, 256, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
-        case OpFmt::F16: emit_counts_kernel<OpFmt::F16><<<grid, 256, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
-        case OpFmt::FX: emit_counts_kernel<OpFmt::FX><<<grid, 256, 0, s>>>(counts, cnt_ld, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
+        case OpFmt::F32: emit_counts_kernel<OpFmt::F32><<<grid, 256, 0, s>>>(counts, cnt_ld, vec, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
+        case OpFmt::BF16: emit_counts_kernel<OpFmt::BF16><<<grid, 256, 0, s>>>(counts, cnt_ld, vec, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
+        case OpFmt::F16: emit_counts_kernel<OpFmt::F16><<<grid, 256, 0, s>>>(counts, cnt_ld, vec, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
+        case OpFmt::FX: emit_counts_kernel<OpFmt::FX><<<grid, 256, 0, s>>>(counts, cnt_ld, vec, upop, P, n_tiles, col_snp, center_snp, rec_n, rec_nm1, op); break;
     }
     STPF2_CUDA(cudaGetLastError());
     c.launches++;

@@ -1190,7 +1190,10 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
         mo[m].cols = pb.add(static_cast<size_t>(mem[m].L.ld) * 4);
         mo[m].tiles = pb.add(static_cast<size_t>(mem[m].L.ld / kTileK) * sizeof(TileInfo));
     }
-    const size_t o_counts = pb.add(static_cast<size_t>(UP) * static_cast<size_t>(M) * 4);
+    // Rows of the union's counts, padded to a multiple of 4 words plus 4 (the emission reads
+    // eight consecutive SNPs as three aligned 16-byte loads, up to 4 words past the last).
+    const int64_t cnt_ld = (M + 3) / 4 * 4 + 4;
+    const size_t o_counts = pb.add(static_cast<size_t>(UP) * static_cast<size_t>(cnt_ld) * 4);
     c.pin_tables.reserve(staged_b);
     c.ws_tables.reserve(pb.end);
     {
@@ -1236,7 +1239,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
         a.umap = reinterpret_cast<const int32_t*>(T + o_umap);
         a.center_snp = d_center_u;
         a.cnt_packed = d_counts;
-        a.cnt_ld = M;
+        a.cnt_ld = cnt_ld;
         launch_decode_canon(c, a, s);
     }
     for (size_t m = 0; m < mem.size(); ++m)
@@ -1289,7 +1292,7 @@ void extract_batch_grouped(Ctx& c, const stp_f2_request* reqs, stp_f2_output* ou
             p.op.fx_table = d_fxtab;
             p.op.fx_table_ld = static_cast<int32_t>(2 * n_max + 1);
             io += p.img_bytes;
-            launch_emit_counts(c, d_counts, M, reinterpret_cast<const int32_t*>(T + q.upop), p.P, p.L.ld / kTileK,
+            launch_emit_counts(c, d_counts, cnt_ld, M, reinterpret_cast<const int32_t*>(T + q.upop), p.P, p.L.ld / kTileK,
                                reinterpret_cast<const int32_t*>(T + q.cols), d_center_u, d_rn, d_rnm1, p.op,
                                fork.next());
             double* f2 = o.f2;

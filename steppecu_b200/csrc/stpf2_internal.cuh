@@ -394,7 +394,9 @@ void launch_layout_tables(Ctx& c, const BlockInfo* blocks, const int64_t* snp_be
                           int32_t* col_snp, TileInfo* tiles, cudaStream_t s);
 // Operand images of one request (P populations, n_tiles padded tiles) from packed
 // per-population counts: population i reads counts row upop[i], column c SNP col_snp[c].
-void launch_emit_counts(Ctx& c, const uint32_t* counts, int64_t cnt_ld, const int32_t* upop, int P, int64_t n_tiles,
+// counts: rows of cnt_ld words over n_snp SNPs; rows 16-byte aligned with cnt_ld >= n_snp + 4
+// let eight consecutive SNPs load as three 16-byte vectors.
+void launch_emit_counts(Ctx& c, const uint32_t* counts, int64_t cnt_ld, int64_t n_snp, const int32_t* upop, int P, int64_t n_tiles,
                         const int32_t* col_snp, const double* center_snp, const double* rec_n, const double* rec_nm1,
                         const OperandPlanes& op, cudaStream_t s);
 // Entries of desc marked 3 (ploidy to be detected) take the ploidy bits of union sample
