@@ -581,7 +581,7 @@ __device__ __forceinline__ Terms8 terms8_from_counts(const uint32_t (&v)[8], con
 }
 
 template <OpFmt F, bool kUnion>
-__global__ void __launch_bounds__(kDecThreads2, 4)
+__global__ void __launch_bounds__(kDecThreads2, 5)
 decode_canon_kernel(const uint64_t* __restrict__ canon, int64_t n_tiles, int64_t n_sel,
                     const uint32_t* __restrict__ sel, const int32_t* __restrict__ pop_off, int P,
                     const double* __restrict__ center, const double* __restrict__ rec_n,
